@@ -1,0 +1,286 @@
+"""ORACLE — test infrastructure only.
+
+Python access to the two CPU checkers of the kriging path:
+
+* ``restated``: oracle/hpgl_oracle.cpp, this repository's CPU restatement
+  of the reference algorithm (built by oracle/build_oracle.sh);
+* ``reference``: the reference's own kriging sources compiled by
+  oracle/build_ref.sh into oracle/_ref/libhpgl_ref.so (present only where
+  the reference checkout was available when it was built), reached through
+  the reference's C ABI (api.h:218-277) and a dump driver.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module.
+"""
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libhpgl_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhpgl_ref.so")
+
+KINDS = {"ok": 0, "sk": 1, "lvm": 2, "ik": 3, "median_ik": 4}
+
+
+class OracleParams(C.Structure):
+    _fields_ = [("cov_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radii", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("marginal_prob", C.c_double)]
+
+
+class HpglShape(C.Structure):
+    _fields_ = [("data", C.c_int * 3), ("strides", C.c_int * 3)]
+
+
+class HpglOkParams(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int)]
+
+
+class HpglSkParams(C.Structure):
+    _fields_ = HpglOkParams._fields_ + [("automatic_mean", C.c_ubyte), ("mean", C.c_double)]
+
+
+class HpglIkParams(C.Structure):
+    _fields_ = HpglOkParams._fields_ + [("marginal_prob", C.c_double)]
+
+
+class HpglMedianIkParams(C.Structure):
+    _fields_ = HpglOkParams._fields_ + [("marginal_probs", C.c_double * 2)]
+
+
+class HpglContArray(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("mask", C.POINTER(C.c_ubyte)), ("shape", HpglShape)]
+
+
+class HpglIndArray(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("mask", C.POINTER(C.c_ubyte)), ("shape", HpglShape),
+                ("indicator_count", C.c_int)]
+
+
+_lib = None
+_ref = None
+
+
+def build_restated():
+    subprocess.run(["bash", os.path.join(HERE, "build_oracle.sh")], check=True, capture_output=True)
+
+
+def restated():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build_restated()
+        _lib = C.CDLL(ORACLE_SO)
+        _lib.oracle_krige.restype = C.c_int
+    return _lib
+
+
+def reference_available():
+    return os.path.exists(REF_SO)
+
+
+def reference():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(REF_SO)
+        _ref.hpgl_get_last_exception_message.restype = C.c_char_p
+        _ref.ref_template.restype = C.c_int
+    return _ref
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def oracle_params(p):
+    o = OracleParams()
+    o.cov_type = p["cov_type"]
+    o.ranges[:] = p["ranges"]
+    o.angles[:] = p["angles"]
+    o.sill = p["sill"]
+    o.nugget = p["nugget"]
+    o.radii[:] = p["radii"]
+    o.max_neighbours = p["max_neighbours"]
+    o.marginal_prob = p.get("marginal_prob", 0.0)
+    return o
+
+
+def run(job, dumps=True, node_list=None, threads=0, sk_auto_mean=False, median_marginal1=None,
+        kind=None):
+    """Run the restated oracle on a job dict (see hpgl_b200.workloads).
+    Returns a dict of numpy arrays: out (values or codes), out_mask and, with
+    ``dumps``, per system slot: variance, status, nb_count, nb_index,
+    weights, probs, via_template."""
+    lib = restated()
+    kind = kind or job["kind"]
+    nx, ny, nz = job["shape"]
+    size = nx * ny * nz
+    params = job["params"]
+    K = len(params) if kind == "ik" else 1
+    parr = (OracleParams * K)(*[oracle_params(p) for p in params[:K]])
+    cont = kind in ("ok", "sk", "lvm")
+    values = np.ascontiguousarray(job["values"], dtype=np.float32) if cont else None
+    codes = None if cont else np.ascontiguousarray(job["codes"], dtype=np.uint8)
+    mask = np.ascontiguousarray(job["mask"], dtype=np.uint8)
+    mean = np.ascontiguousarray(job["mean"], dtype=np.float32) if kind == "lvm" else None
+    out = (values.copy() if cont else codes.copy())
+    out_mask = mask.copy()
+    slots = size * K
+    cap = max(p["max_neighbours"] for p in params[:K])
+    res = {}
+    if dumps:
+        res["variance"] = np.full(slots, np.nan)
+        res["status"] = np.full(slots, -2, dtype=np.int8)
+        res["nb_count"] = np.full(slots, -1, dtype=np.int32)
+        res["nb_index"] = np.full(slots * cap, -1, dtype=np.int32)
+        res["weights"] = np.zeros(slots * cap)
+        res["probs"] = np.zeros(slots, dtype=np.float32)
+        res["via_template"] = np.zeros(slots, dtype=np.uint8)
+    nl = None if node_list is None else np.ascontiguousarray(node_list, dtype=np.int32)
+    err = C.create_string_buffer(512)
+    if median_marginal1 is None:
+        median_marginal1 = job.get("median_marginal1", 0.5)
+    rc = lib.oracle_krige(
+        KINDS[kind], nx, ny, nz, _ptr(values, C.c_float), _ptr(codes, C.c_ubyte), _ptr(mask, C.c_ubyte),
+        _ptr(mean, C.c_float), parr, K, C.c_double(job.get("sk_mean", 0.0)), int(sk_auto_mean),
+        C.c_double(median_marginal1),
+        _ptr(out, C.c_float) if cont else None, None if cont else _ptr(out, C.c_ubyte), _ptr(out_mask, C.c_ubyte),
+        _ptr(res.get("variance"), C.c_double), _ptr(res.get("status"), C.c_byte),
+        _ptr(res.get("nb_count"), C.c_int), _ptr(res.get("nb_index"), C.c_int),
+        _ptr(res.get("weights"), C.c_double), _ptr(res.get("probs"), C.c_float),
+        _ptr(res.get("via_template"), C.c_ubyte), cap, _ptr(nl, C.c_int), 0 if nl is None else len(nl),
+        threads, err, 512)
+    if rc != 0:
+        raise RuntimeError("oracle: " + err.value.decode())
+    res["out"] = out
+    res["out_mask"] = out_mask
+    res["cap"] = cap
+    return res
+
+
+def template(p, truncated=False):
+    lib = restated()
+    cap = (2 * p["radii"][0] + 1) * (2 * p["radii"][1] + 1) * (2 * p["radii"][2] + 1)
+    buf = np.zeros(cap * 3, dtype=np.int32)
+    n = lib.oracle_template(C.byref(oracle_params(p)), int(truncated), _ptr(buf, C.c_int), cap)
+    return buf[: 3 * n].reshape(n, 3)
+
+
+# ---- the reference itself (oracle/_ref) ------------------------------------
+
+def _shape(shape):
+    s = HpglShape()
+    s.data[:] = shape
+    s.strides[:] = (1, shape[0], shape[0] * shape[1])
+    return s
+
+
+def _ok_params(p, cls=HpglOkParams):
+    o = cls()
+    o.covariance_type = p["cov_type"]
+    o.ranges[:] = p["ranges"]
+    o.angles[:] = p["angles"]
+    o.sill = p["sill"]
+    o.nugget = p["nugget"]
+    o.radiuses[:] = p["radii"]
+    o.max_neighbours = p["max_neighbours"]
+    return o
+
+
+def ref_run(job, threads=0, kind=None, sk_auto_mean=False, median_marginal1=None):
+    """Run the compiled reference through its own C ABI; returns (out, mask)
+    starting, like geo.py does, from a clone of the input."""
+    ref = reference()
+    if threads > 0:
+        ref.hpgl_set_thread_num(int(threads))
+    kind = kind or job["kind"]
+    shape = job["shape"]
+    sh = _shape(shape)
+    p0 = job["params"][0]
+    mask = np.array(job["mask"], dtype=np.uint8)
+    if kind in ("ok", "sk", "lvm"):
+        values = np.array(job["values"], dtype=np.float32)
+        out, out_mask = values.copy(), mask.copy()
+        if kind == "ok":
+            a = HpglContArray(_ptr(values, C.c_float), _ptr(mask, C.c_ubyte), sh)
+            b = HpglContArray(_ptr(out, C.c_float), _ptr(out_mask, C.c_ubyte), sh)
+            ref.hpgl_ordinary_kriging(C.byref(a), C.byref(_ok_params(p0)), C.byref(b))
+        elif kind == "sk":
+            sp = _ok_params(p0, HpglSkParams)
+            sp.automatic_mean = int(sk_auto_mean)
+            sp.mean = job.get("sk_mean", 0.0)
+            ref.hpgl_simple_kriging(_ptr(values, C.c_float), _ptr(mask, C.c_ubyte), C.byref(sh), C.byref(sp),
+                                    _ptr(out, C.c_float), _ptr(out_mask, C.c_ubyte), C.byref(sh))
+        else:
+            mean = np.array(job["mean"], dtype=np.float32)
+            ref.hpgl_lvm_kriging(_ptr(values, C.c_float), _ptr(mask, C.c_ubyte), C.byref(sh),
+                                 _ptr(mean, C.c_float), C.byref(sh), C.byref(_ok_params(p0)),
+                                 _ptr(out, C.c_float), _ptr(out_mask, C.c_ubyte), C.byref(sh))
+        return out, out_mask
+    codes = np.array(job["codes"], dtype=np.uint8)
+    out, out_mask = codes.copy(), mask.copy()
+    K = len(job["params"])
+    if kind == "ik":
+        a = HpglIndArray(_ptr(codes, C.c_ubyte), _ptr(mask, C.c_ubyte), sh, K)
+        b = HpglIndArray(_ptr(out, C.c_ubyte), _ptr(out_mask, C.c_ubyte), sh, K)
+        ps = (HpglIkParams * K)()
+        for k, p in enumerate(job["params"]):
+            q = _ok_params(p, HpglIkParams)
+            q.marginal_prob = p["marginal_prob"]
+            ps[k] = q
+        ref.hpgl_indicator_kriging(C.byref(a), C.byref(b), ps, K)
+    else:
+        a = HpglIndArray(_ptr(codes, C.c_ubyte), _ptr(mask, C.c_ubyte), sh, 2)
+        b = HpglIndArray(_ptr(out, C.c_ubyte), _ptr(out_mask, C.c_ubyte), sh, 2)
+        q = _ok_params(p0, HpglMedianIkParams)
+        m1 = job.get("median_marginal1", 0.5) if median_marginal1 is None else median_marginal1
+        q.marginal_probs[:] = (1.0 - m1, m1)
+        ref.hpgl_median_ik(C.byref(a), C.byref(q), C.byref(b))
+    return out, out_mask
+
+
+def ref_dump(job, kind=None, category=0, marginal=None, threads=0):
+    """Per-node dumps from the reference's own classes (oracle/ref_dump.cpp)."""
+    ref = reference()
+    kind = kind or job["kind"]
+    nx, ny, nz = job["shape"]
+    size = nx * ny * nz
+    p = job["params"][category if kind == "ik" else 0]
+    cap = p["max_neighbours"]
+    res = dict(nb_count=np.full(size, -1, dtype=np.int32), nb_index=np.full(size * cap, -1, dtype=np.int32),
+               weights=np.zeros(size * cap), variance=np.full(size, np.nan),
+               status=np.full(size, -2, dtype=np.int32), estimate=np.full(size, np.nan))
+    args = [_ptr(res["nb_count"], C.c_int), _ptr(res["nb_index"], C.c_int), _ptr(res["weights"], C.c_double),
+            _ptr(res["variance"], C.c_double), _ptr(res["status"], C.c_int), _ptr(res["estimate"], C.c_double),
+            int(threads)]
+    mask = np.array(job["mask"], dtype=np.uint8)
+    if kind in ("ok", "sk", "lvm"):
+        values = np.array(job["values"], dtype=np.float32)
+        mean = np.array(job["mean"], dtype=np.float32) if kind == "lvm" else None
+        rc = ref.ref_dump_cont(KINDS[kind], nx, ny, nz, _ptr(values, C.c_float), _ptr(mask, C.c_ubyte),
+                               _ptr(mean, C.c_float), C.byref(_ok_params(p)), C.c_double(job.get("sk_mean", 0.0)),
+                               cap, *args)
+    else:
+        codes = np.array(job["codes"], dtype=np.uint8)
+        if marginal is None:
+            marginal = p["marginal_prob"] if kind == "ik" else job.get("median_marginal1", 0.5)
+        rc = ref.ref_dump_ind(KINDS[kind], nx, ny, nz, _ptr(codes, C.c_ubyte), _ptr(mask, C.c_ubyte),
+                              int(category), C.byref(_ok_params(p)), C.c_double(marginal), cap, *args)
+    if rc != 0:
+        raise RuntimeError("reference dump failed")
+    res["cap"] = cap
+    return res
+
+
+def ref_template(p):
+    ref = reference()
+    cap = (2 * p["radii"][0] + 1) * (2 * p["radii"][1] + 1) * (2 * p["radii"][2] + 1)
+    buf = np.zeros(cap * 3, dtype=np.int32)
+    n = ref.ref_template(C.byref(_ok_params(p)), _ptr(buf, C.c_int), cap)
+    return buf[: 3 * n].reshape(n, 3)
