@@ -1,0 +1,331 @@
+// extern "C" entry points of hpgl.so: the reference's kriging ABI
+// (src/geo_bsd/hpgl/api.h, api.cpp) plus this build's additions, all declared
+// in include/hpgl.h.  Every entry point catches every error and records it
+// for hpgl_get_last_exception_message / hpgl_get_last_error.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/hpgl.h"
+#include "engine.h"
+#include "plan.h"
+
+using namespace hpgl_b200;
+
+namespace {
+std::mutex g_err_mutex;
+std::string g_last_message;
+int g_last_error = 0;
+int (*g_output_handler)(char *, void *) = nullptr;
+void *g_output_param = nullptr;
+int (*g_progress_handler)(char *, int, void *) = nullptr;
+void *g_progress_param = nullptr;
+
+void set_error(int code, const std::string &msg) {
+    std::lock_guard<std::mutex> l(g_err_mutex);
+    g_last_error = code;
+    g_last_message = msg;
+}
+
+void log_line(const std::string &s) {
+    if (g_output_handler) g_output_handler((char *)s.c_str(), g_output_param);
+}
+
+template <typename F>
+int guarded(const char *where, F f) {
+    try {
+        f();
+        set_error(HPGL_OK, "");
+        return HPGL_OK;
+    } catch (const HpglError &e) {
+        set_error(e.code, std::string(where) + ": " + e.message);
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_error(HPGL_E_CAPACITY, std::string(where) + ": out of host memory");
+        return HPGL_E_CAPACITY;
+    } catch (const std::exception &e) {
+        set_error(HPGL_E_INTERNAL, std::string(where) + ": " + e.what());
+        return HPGL_E_INTERNAL;
+    } catch (...) {
+        set_error(HPGL_E_INTERNAL, std::string(where) + ": unknown error");
+        return HPGL_E_INTERNAL;
+    }
+}
+
+long long volume(const hpgl_shape_t *s) {
+    if (!s) throw HpglError{HPGL_E_INVALID, "shape is null"};
+    return (long long)s->m_data[0] * s->m_data[1] * s->m_data[2];
+}
+
+hpgl_ik_params_t from_ok(const hpgl_ok_params_t *p) {
+    if (!p) throw HpglError{HPGL_E_INVALID, "params are null"};
+    hpgl_ik_params_t q;
+    memset(&q, 0, sizeof(q));
+    q.m_covariance_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i) {
+        q.m_ranges[i] = p->m_ranges[i];
+        q.m_angles[i] = p->m_angles[i];
+        q.m_radiuses[i] = p->m_radiuses[i];
+    }
+    q.m_sill = p->m_sill;
+    q.m_nugget = p->m_nugget;
+    q.m_max_neighbours = p->m_max_neighbours;
+    return q;
+}
+
+hpgl_b200_job_t base_job(int kind, const hpgl_shape_t *shape) {
+    hpgl_b200_job_t j;
+    memset(&j, 0, sizeof(j));
+    j.kind = kind;
+    j.nx = shape->m_data[0];
+    j.ny = shape->m_data[1];
+    j.nz = shape->m_data[2];
+    j.precision = -1;
+    return j;
+}
+
+void run(const char *name, hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
+    run_job(job, res);
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %lld systems in %.3f ms (plan %.3f, device %.3f)\n", name, res.systems,
+             res.ms_total, res.ms_plan, res.ms_device);
+    log_line(buf);
+}
+
+void not_provided(const char *what) {
+    throw HpglError{HPGL_E_UNSUPPORTED, std::string(what) + " is not provided by this build (kriging path only)"};
+}
+}  // namespace
+
+extern "C" {
+
+char *hpgl_get_last_exception_message(void) {
+    std::lock_guard<std::mutex> l(g_err_mutex);
+    return (char *)g_last_message.c_str();
+}
+
+int hpgl_get_last_error(void) {
+    std::lock_guard<std::mutex> l(g_err_mutex);
+    return g_last_error;
+}
+
+void hpgl_set_output_handler(int (*handler)(char *, void *), void *param) {
+    g_output_handler = handler;
+    g_output_param = param;
+}
+
+void hpgl_set_progress_handler(int (*handler)(char *, int, void *), void *param) {
+    g_progress_handler = handler;
+    g_progress_param = param;
+}
+
+void hpgl_set_thread_num(int n_threads) { set_host_threads(n_threads); }
+int hpgl_get_thread_num(void) { return host_threads(); }
+
+void hpgl_b200_set_precision(int precision) {
+    guarded("hpgl_b200_set_precision", [&] {
+        if (precision != HPGL_PRECISION_FP64 && precision != HPGL_PRECISION_MIXED)
+            throw HpglError{HPGL_E_INVALID, "unknown precision"};
+        set_default_precision(precision);
+    });
+}
+int hpgl_b200_get_precision(void) { return default_precision(); }
+
+void hpgl_ordinary_kriging(hpgl_cont_masked_array_t *input_data, hpgl_ok_params_t *params,
+                           hpgl_cont_masked_array_t *output_data) {
+    guarded("hpgl_ordinary_kriging", [&] {
+        if (!input_data || !output_data) throw HpglError{HPGL_E_INVALID, "null array"};
+        if (volume(&input_data->m_shape) != volume(&output_data->m_shape))
+            throw HpglError{HPGL_E_INVALID, "input and output sizes differ"};
+        hpgl_ik_params_t p = from_ok(params);
+        hpgl_b200_job_t job = base_job(HPGL_KIND_OK, &input_data->m_shape);
+        job.values = input_data->m_data;
+        job.mask = input_data->m_mask;
+        job.params = &p;
+        job.n_params = 1;
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_values = output_data->m_data;
+        res.out_mask = output_data->m_mask;
+        run("Ordinary Kriging", job, res);
+    });
+}
+
+void hpgl_simple_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t *input_data_shape,
+                         hpgl_sk_params_t *params, float *output_data, unsigned char *output_mask,
+                         hpgl_shape_t *output_data_shape) {
+    guarded("hpgl_simple_kriging", [&] {
+        if (!params) throw HpglError{HPGL_E_INVALID, "params are null"};
+        if (volume(input_data_shape) != volume(output_data_shape))
+            throw HpglError{HPGL_E_INVALID, "input and output sizes differ"};
+        hpgl_ok_params_t okp;
+        okp.m_covariance_type = params->m_covariance_type;
+        for (int i = 0; i < 3; ++i) {
+            okp.m_ranges[i] = params->m_ranges[i];
+            okp.m_angles[i] = params->m_angles[i];
+            okp.m_radiuses[i] = params->m_radiuses[i];
+        }
+        okp.m_sill = params->m_sill;
+        okp.m_nugget = params->m_nugget;
+        okp.m_max_neighbours = params->m_max_neighbours;
+        hpgl_ik_params_t p = from_ok(&okp);
+        hpgl_b200_job_t job = base_job(HPGL_KIND_SK, input_data_shape);
+        job.values = input_data;
+        job.mask = input_mask;
+        job.params = &p;
+        job.n_params = 1;
+        // api.cpp:255-258: the mean is used only when not automatic.
+        job.sk_automatic_mean = params->m_automatic_mean ? 1 : 0;
+        job.sk_mean = params->m_mean;
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_values = output_data;
+        res.out_mask = output_mask;
+        run("Simple Kriging", job, res);
+    });
+}
+
+void hpgl_lvm_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t *input_data_shape, float *mean_data,
+                      hpgl_shape_t *mean_data_shape, hpgl_ok_params_t *params, float *output_data,
+                      unsigned char *output_mask, hpgl_shape_t *output_data_shape) {
+    guarded("hpgl_lvm_kriging", [&] {
+        long long n = volume(input_data_shape);
+        if (mean_data_shape && volume(mean_data_shape) != n)
+            throw HpglError{HPGL_E_INVALID, "mean cube size differs from the input size"};
+        if (output_data_shape && volume(output_data_shape) != n)
+            throw HpglError{HPGL_E_INVALID, "input and output sizes differ"};
+        hpgl_ik_params_t p = from_ok(params);
+        hpgl_b200_job_t job = base_job(HPGL_KIND_LVM, input_data_shape);
+        job.values = input_data;
+        job.mask = input_mask;
+        job.mean = mean_data;
+        job.params = &p;
+        job.n_params = 1;
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_values = output_data;
+        res.out_mask = output_mask;
+        run("LVM Kriging", job, res);
+    });
+}
+
+void hpgl_indicator_kriging(hpgl_ind_masked_array_t *in_data, hpgl_ind_masked_array_t *out_data,
+                            hpgl_ik_params_t *params, int indicator_count) {
+    guarded("hpgl_indicator_kriging", [&] {
+        if (!in_data || !out_data || !params) throw HpglError{HPGL_E_INVALID, "null argument"};
+        if (indicator_count < 1) throw HpglError{HPGL_E_INVALID, "indicator_count must be >= 1"};
+        if (volume(&in_data->m_shape) != volume(&out_data->m_shape))
+            throw HpglError{HPGL_E_INVALID, "input and output sizes differ"};
+        hpgl_b200_job_t job = base_job(HPGL_KIND_IK, &in_data->m_shape);
+        job.codes = in_data->m_data;
+        job.mask = in_data->m_mask;
+        job.params = params;
+        job.n_params = indicator_count;
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_codes = out_data->m_data;
+        res.out_mask = out_data->m_mask;
+        run("Indicator Kriging", job, res);
+    });
+}
+
+void hpgl_median_ik(hpgl_ind_masked_array_t *in_data, hpgl_median_ik_params_t *params,
+                    hpgl_ind_masked_array_t *out_data) {
+    guarded("hpgl_median_ik", [&] {
+        if (!in_data || !out_data || !params) throw HpglError{HPGL_E_INVALID, "null argument"};
+        // median_ik.cpp:35-43
+        if (volume(&in_data->m_shape) != volume(&out_data->m_shape))
+            throw HpglError{HPGL_E_INVALID, "Input property size is not equal output property size"};
+        hpgl_ok_params_t okp;
+        okp.m_covariance_type = params->m_covariance_type;
+        for (int i = 0; i < 3; ++i) {
+            okp.m_ranges[i] = params->m_ranges[i];
+            okp.m_angles[i] = params->m_angles[i];
+            okp.m_radiuses[i] = params->m_radiuses[i];
+        }
+        okp.m_sill = params->m_sill;
+        okp.m_nugget = params->m_nugget;
+        okp.m_max_neighbours = params->m_max_neighbours;
+        hpgl_ik_params_t p = from_ok(&okp);
+        hpgl_b200_job_t job = base_job(HPGL_KIND_MEDIAN_IK, &in_data->m_shape);
+        job.codes = in_data->m_data;
+        job.mask = in_data->m_mask;
+        job.params = &p;
+        job.n_params = 1;
+        job.median_marginal1 = params->m_marginal_probs[1];
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_codes = out_data->m_data;
+        res.out_mask = out_data->m_mask;
+        run("Median IK", job, res);
+    });
+}
+
+int hpgl_b200_krige(const hpgl_b200_job_t *job, hpgl_b200_result_t *result) {
+    return guarded("hpgl_b200_krige", [&] {
+        if (!job || !result) throw HpglError{HPGL_E_INVALID, "null argument"};
+        run_job(*job, *result);
+    });
+}
+
+int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl_b200_bench_t *bench) {
+    return guarded("hpgl_b200_bench", [&] {
+        if (!job || !result || !bench) throw HpglError{HPGL_E_INVALID, "null argument"};
+        if (bench->iters < 1 || bench->warmup < 0) throw HpglError{HPGL_E_INVALID, "iters must be >= 1"};
+        bench_job(*job, *result, *bench);
+    });
+}
+
+const char *hpgl_b200_version(void) { return "hpgl_b200 0.1 (sm_100a kriging path)"; }
+
+int hpgl_simple_kriging_weights(float *, float *, float *, float *, int, hpgl_cov_params_t *, float *) {
+    int rc = guarded("hpgl_simple_kriging_weights", [&] { not_provided("hpgl_simple_kriging_weights"); });
+    return rc == HPGL_OK ? 0 : -1;
+}
+
+void hpgl_read_inc_file_float(char *, float, int, float *, unsigned char *) {
+    guarded("hpgl_read_inc_file_float", [&] { not_provided("INC file reading"); });
+}
+void hpgl_read_inc_file_byte(char *, int, int, unsigned char *, unsigned char *, unsigned char *, int) {
+    guarded("hpgl_read_inc_file_byte", [&] { not_provided("INC file reading"); });
+}
+void hpgl_write_inc_file_float(char *, hpgl_cont_masked_array_t *, float, char *) {
+    guarded("hpgl_write_inc_file_float", [&] { not_provided("INC file writing"); });
+}
+void hpgl_write_inc_file_byte(char *, hpgl_ind_masked_array_t *, int, char *, unsigned char *, int) {
+    guarded("hpgl_write_inc_file_byte", [&] { not_provided("INC file writing"); });
+}
+void hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *, const char *, const char *, double) {
+    guarded("hpgl_write_gslib_cont_property", [&] { not_provided("GSLIB writing"); });
+}
+void hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *, const char *, const char *, double, unsigned char *,
+                                    int) {
+    guarded("hpgl_write_gslib_byte_property", [&] { not_provided("GSLIB writing"); });
+}
+void hpgl_sgs_simulation(hpgl_cont_masked_array_t *, hpgl_sgs_params_t *, hpgl_non_parametric_cdf_t *, double *,
+                         hpgl_ubyte_array_t *) {
+    guarded("hpgl_sgs_simulation", [&] { not_provided("sequential Gaussian simulation"); });
+}
+void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *, hpgl_sgs_params_t *, hpgl_non_parametric_cdf_t *,
+                             hpgl_float_array_t *, hpgl_ubyte_array_t *) {
+    guarded("hpgl_sgs_lvm_simulation", [&] { not_provided("sequential Gaussian simulation"); });
+}
+void hpgl_sis_simulation(hpgl_ind_masked_array_t *, hpgl_ik_params_t *, int, int, hpgl_ubyte_array_t *) {
+    guarded("hpgl_sis_simulation", [&] { not_provided("sequential indicator simulation"); });
+}
+void hpgl_sis_simulation_lvm(hpgl_ind_masked_array_t *, hpgl_ik_params_t *, hpgl_float_array_t *, int, int,
+                             hpgl_ubyte_array_t *, int) {
+    guarded("hpgl_sis_simulation_lvm", [&] { not_provided("sequential indicator simulation"); });
+}
+void hpgl_simple_cokriging_mark1(hpgl_cont_masked_array_t *, hpgl_cont_masked_array_t *, hpgl_cokriging_m1_params_t *,
+                                 hpgl_cont_masked_array_t *) {
+    guarded("hpgl_simple_cokriging_mark1", [&] { not_provided("simple cokriging"); });
+}
+void hpgl_simple_cokriging_mark2(hpgl_cont_masked_array_t *, hpgl_cont_masked_array_t *, hpgl_cokriging_m2_params_t *,
+                                 hpgl_cont_masked_array_t *) {
+    guarded("hpgl_simple_cokriging_mark2", [&] { not_provided("simple cokriging"); });
+}
+
+}  // extern "C"

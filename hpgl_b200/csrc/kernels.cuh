@@ -1,0 +1,88 @@
+// Device-side data of one kriging pass and the kernel launchers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hpgl_b200 {
+
+enum Status : int8_t { ST_SUCCESS = 0, ST_NO_NEIGHBOURS = 1, ST_SINGULAR = 2, ST_NOT_KRIGED = -1 };
+
+// Error bits raised by kernels (never expected; each names a broken
+// invariant so the host can report it instead of returning wrong results).
+enum DevError : int {
+    DERR_TABLE_RANGE = 1,      // a covariance offset fell outside the table
+    DERR_CAND_CAPACITY = 2,    // clusterizer candidates exceeded the scratch
+    DERR_SORT_STACK = 4,
+};
+
+struct DevPlan {
+    int nmax;
+    // template
+    const int4 *tmpl;        // (packed window offset, dy, dz, node delta)
+    int tmpl_len;
+    int px, nseg, wpr;
+    // covariance table
+    const double *table;
+    int Bx, By, Bz;
+    int Tx, Ty, Tz;          // truncation half extents
+    double c0;
+    // clusterizer
+    const int *bucket_start;
+    const int *bucket_nodes;
+    const uint8_t *bucket_clean;
+    double crx, cry, crz;
+    int mx, my, mz;
+    int max_candidates;
+};
+
+struct DevJob {
+    int kind;
+    int nx, ny, nz;
+    long long size;
+    const float *values;
+    const uint8_t *codes;
+    const uint8_t *mask;
+    const float *mean;
+    const uint32_t *bits;    // padded informed-bit rows
+    // categories: this pass computes probabilities of categories [k0, k1)
+    int K, k0, k1;
+    const float *pk;         // IK marginal probabilities (float) per category
+    float sk_mean_f;         // SK mean as the float the combiner sees
+    float median_m;          // median IK (float)marginal_probs[1]
+    // neighbour lists
+    int *nb;                 // [size][nmax]
+    int *nbcount;            // [size]
+    // outputs
+    float *out_values;
+    uint8_t *out_codes;
+    uint8_t *out_mask;
+    double *variance;        // optional
+    int8_t *status;          // [size] (or [size*K] for per-category IK)
+    float *probs;            // IK [size*K], median IK [size]
+    double *weights;         // optional [size][nmax]
+    int status_stride;       // 1, or K for per-category IK
+    int status_offset;       // category for per-category IK
+    // untouched nodes (ordinary kriging failures keep the caller's content)
+    int *untouched;
+    int *n_untouched;
+    // mixed precision routing
+    int *routed;
+    int *n_routed;
+    // counters
+    unsigned long long *n_fp64;
+    int *err;
+};
+
+// Launchers (stream-ordered, no synchronisation).
+void launch_build_bits(const DevJob &J, const DevPlan &P, uint32_t *bits, cudaStream_t s);
+void launch_search_template(const DevJob &J, const DevPlan &P, cudaStream_t s);
+void launch_search_cluster(const DevJob &J, const DevPlan &P, double *scratch_key, int *scratch_idx,
+                           int n_warps, cudaStream_t s);
+// precision: 0 exact FP64, 1 FP32 + FP64 refinement (routes to `routed`).
+// node_list: optional list of nodes (routed re-solve); else every node.
+void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
+                  int n_list_max, cudaStream_t s);
+void launch_ik_argmax(const DevJob &J, cudaStream_t s);
+int solve_kernel_count();
+
+}  // namespace hpgl_b200

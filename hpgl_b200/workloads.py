@@ -56,7 +56,7 @@ def gaussian_field(rng, shape, corr_range, cov="exponential"):
     spec = np.fft.rfftn(c).real
     spec[spec < 0] = 0
     noise = rng.standard_normal(shape)
-    f = np.fft.irfftn(np.sqrt(spec) * np.fft.rfftn(noise), s=shape)
+    f = np.fft.irfftn(np.sqrt(spec) * np.fft.rfftn(noise), s=shape, axes=(0, 1, 2))
     f = (f - f.mean()) / (f.std() + 1e-30)
     return f
 

@@ -1,0 +1,342 @@
+/*
+ * hpgl.h — C ABI of the B200 kriging library (hpgl_b200/hpgl.so).
+ *
+ * The first part re-declares, with identical layouts and signatures, the
+ * reference library's kriging interface (HPGL 0.9.9, src/geo_bsd/hpgl/api.h)
+ * so that the reference's ctypes layer (src/geo_bsd/hpgl_wrap.py:141-311)
+ * can load this library in place of `hpgl.so`.  Each declaration cites the
+ * reference line it replaces.  The second part adds entry points with no
+ * reference counterpart: an extended kriging call that exposes precision
+ * control and per-node side outputs (variance, status, neighbour lists,
+ * weights), error codes, and a device-resident benchmark hook.
+ *
+ * All buffers are caller-owned host memory.  Grids are Fortran ordered:
+ * index = x + nx*(y + ny*z).  Output buffers must be pre-filled by the caller
+ * with a copy of the input (the reference's Python layer does this,
+ * geo.py:232-240): nodes the algorithm leaves alone (ordinary kriging
+ * failures) keep that content.  Every call is synchronous and returns only
+ * after the results are in the caller's buffers.
+ *
+ * Errors: the reference functions return void.  Here every entry point
+ * catches all errors, records a message for hpgl_get_last_exception_message()
+ * and a code for hpgl_get_last_error() (0 = success), and returns.
+ */
+#ifndef HPGL_B200_HPGL_H
+#define HPGL_B200_HPGL_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference structs, api.h:18-146 (same field order and types) ---- */
+
+typedef struct hpgl_shape_t {          /* api.h:18-22 */
+    int m_data[3];
+    int m_strides[3];                  /* ignored, as in the reference */
+} hpgl_shape_t;
+
+typedef struct hpgl_cont_masked_array_t {   /* api.h:24-29 */
+    float *m_data;
+    unsigned char *m_mask;
+    hpgl_shape_t m_shape;
+} hpgl_cont_masked_array_t;
+
+typedef struct hpgl_ind_masked_array_t {    /* api.h:31-37 */
+    unsigned char *m_data;
+    unsigned char *m_mask;
+    hpgl_shape_t m_shape;
+    int m_indicator_count;
+} hpgl_ind_masked_array_t;
+
+typedef struct hpgl_float_array_t {         /* api.h:39-43 */
+    float *m_data;
+    hpgl_shape_t m_shape;
+} hpgl_float_array_t;
+
+typedef struct hpgl_ubyte_array_t {         /* api.h:45-49 */
+    unsigned char *m_data;
+    hpgl_shape_t m_shape;
+} hpgl_ubyte_array_t;
+
+typedef struct hpgl_ok_params_t {           /* api.h:51-60 */
+    int m_covariance_type;             /* 0 spherical, 1 exponential, 2 gaussian */
+    double m_ranges[3];
+    double m_angles[3];                /* degrees */
+    double m_sill;
+    double m_nugget;
+    int m_radiuses[3];
+    int m_max_neighbours;
+} hpgl_ok_params_t;
+
+typedef struct hpgl_sk_params_t {           /* api.h:62-73 */
+    int m_covariance_type;
+    double m_ranges[3];
+    double m_angles[3];
+    double m_sill;
+    double m_nugget;
+    int m_radiuses[3];
+    int m_max_neighbours;
+    unsigned char m_automatic_mean;
+    double m_mean;
+} hpgl_sk_params_t;
+
+typedef struct hpgl_cov_params_t {          /* api.h:75-82 */
+    int m_covariance_type;
+    double m_ranges[3];
+    double m_angles[3];
+    double m_sill;
+    double m_nugget;
+} hpgl_cov_params_t;
+
+typedef struct hpgl_sgs_params_t {          /* api.h:84-96 */
+    int m_covariance_type;
+    double m_ranges[3];
+    double m_angles[3];
+    double m_sill;
+    double m_nugget;
+    int m_radiuses[3];
+    int m_max_neighbours;
+    int m_kriging_kind;
+    long int m_seed;
+    int m_min_neighbours;
+} hpgl_sgs_params_t;
+
+typedef struct hpgl_median_ik_params_t {    /* api.h:98-108 */
+    int m_covariance_type;
+    double m_ranges[3];
+    double m_angles[3];
+    double m_sill;
+    double m_nugget;
+    int m_radiuses[3];
+    int m_max_neighbours;
+    double m_marginal_probs[2];
+} hpgl_median_ik_params_t;
+
+typedef struct hpgl_ik_params_t {           /* api.h:110-120 */
+    int m_covariance_type;
+    double m_ranges[3];
+    double m_angles[3];
+    double m_sill;
+    double m_nugget;
+    int m_radiuses[3];
+    int m_max_neighbours;
+    double m_marginal_prob;
+} hpgl_ik_params_t;
+
+typedef struct hpgl_cokriging_m1_params_t { /* api.h:122-135 */
+    int m_covariance_type;
+    double m_ranges[3];
+    double m_angles[3];
+    double m_sill;
+    double m_nugget;
+    int m_radiuses[3];
+    int m_max_neighbours;
+    double m_primary_mean;
+    double m_secondary_mean;
+    double m_secondary_variance;
+    double m_correlation_coef;
+} hpgl_cokriging_m1_params_t;
+
+typedef struct hpgl_cokriging_m2_params_t { /* api.h:137-146 */
+    hpgl_cov_params_t m_primary_cov_params;
+    hpgl_cov_params_t m_secondary_cov_params;
+    int m_radiuses[3];
+    int m_max_neighbours;
+    double m_primary_mean;
+    double m_secondary_mean;
+    double m_correlation_coef;
+} hpgl_cokriging_m2_params_t;
+
+typedef struct hpgl_non_parametric_cdf_t {  /* api.h:148-153 */
+    float *m_values;
+    float *m_probs;
+    long long m_size;
+} hpgl_non_parametric_cdf_t;
+
+/* ---- reference entry points, api.h:159-309 ---- */
+
+/* api.h:159-160.  Message of the last failed call ("" after a success). */
+char *hpgl_get_last_exception_message(void);
+
+/* api.h:162-166.  Handlers receive the library's log lines / progress. */
+void hpgl_set_output_handler(int (*handler)(char *str, void *param), void *param);
+void hpgl_set_progress_handler(int (*handler)(char *stage, int percentage, void *param), void *param);
+
+/* api.h:168-169.  Host worker threads of the library (planning steps). */
+void hpgl_set_thread_num(int n_threads);
+int hpgl_get_thread_num(void);
+
+/* api.h:218-221, implemented by api.cpp:195-231.  Ordinary kriging. */
+void hpgl_ordinary_kriging(hpgl_cont_masked_array_t *input_data, hpgl_ok_params_t *params,
+                           hpgl_cont_masked_array_t *output_data);
+
+/* api.h:223-230, api.cpp:261-288.  Simple kriging (mean given or automatic). */
+void hpgl_simple_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t *input_data_shape,
+                         hpgl_sk_params_t *params, float *output_data, unsigned char *output_mask,
+                         hpgl_shape_t *output_data_shape);
+
+/* api.h:242-251, api.cpp:344-383.  Locally varying mean kriging. */
+void hpgl_lvm_kriging(float *input_data, unsigned char *input_mask, hpgl_shape_t *input_data_shape,
+                      float *mean_data, hpgl_shape_t *mean_data_shape, hpgl_ok_params_t *params,
+                      float *output_data, unsigned char *output_mask, hpgl_shape_t *output_data_shape);
+
+/* api.h:267-272, api.cpp:385-406.  Indicator kriging, one params entry per
+   category. */
+void hpgl_indicator_kriging(hpgl_ind_masked_array_t *in_data, hpgl_ind_masked_array_t *out_data,
+                            hpgl_ik_params_t *params, int indicator_count);
+
+/* api.h:274-277, api.cpp:469-515.  Median indicator kriging (2 categories). */
+void hpgl_median_ik(hpgl_ind_masked_array_t *in_data, hpgl_median_ik_params_t *params,
+                    hpgl_ind_masked_array_t *out_data);
+
+/* api.h:232-240, api.cpp:292-342.  Simple-kriging weights of one point.
+   Not provided by this build: records an error and returns -1. */
+int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
+                                float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
+                                float *weights);
+
+/* api.h:171-215, 253-265, 279-309.  Outside the kriging path (file I/O,
+   sequential simulation, cokriging).  They exist so that the reference's
+   ctypes layer loads; each records "not provided by this build" in the
+   last-error state and returns without touching its buffers. */
+void hpgl_read_inc_file_float(char *filename, float undefined_value, int size, float *data, unsigned char *mask);
+void hpgl_read_inc_file_byte(char *filename, int undefined_value, int size, unsigned char *data,
+                             unsigned char *mask, unsigned char *values, int values_count);
+void hpgl_write_inc_file_float(char *filename, hpgl_cont_masked_array_t *arr, float undefined_value, char *name);
+void hpgl_write_inc_file_byte(char *filename, hpgl_ind_masked_array_t *arr, int undefined_value, char *name,
+                              unsigned char *values, int values_count);
+void hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *data, const char *filename, const char *name,
+                                    double undefined_value);
+void hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *data, const char *filename, const char *name,
+                                    double undefined_value, unsigned char *values, int values_count);
+void hpgl_sgs_simulation(hpgl_cont_masked_array_t *prop, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
+                         double *mean, hpgl_ubyte_array_t *simulation_mask);
+void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params,
+                             hpgl_non_parametric_cdf_t *cdf, hpgl_float_array_t *means,
+                             hpgl_ubyte_array_t *simulation_mask);
+void hpgl_sis_simulation(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, int indicator_count, int seed,
+                         hpgl_ubyte_array_t *simulation_mask);
+void hpgl_sis_simulation_lvm(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, hpgl_float_array_t *mean_data,
+                             int indicator_count, int seed, hpgl_ubyte_array_t *simulation_mask,
+                             int use_correlograms);
+void hpgl_simple_cokriging_mark1(hpgl_cont_masked_array_t *input_data, hpgl_cont_masked_array_t *secondary_data,
+                                 hpgl_cokriging_m1_params_t *params, hpgl_cont_masked_array_t *output_data);
+void hpgl_simple_cokriging_mark2(hpgl_cont_masked_array_t *primary_data, hpgl_cont_masked_array_t *secondary_data,
+                                 hpgl_cokriging_m2_params_t *params, hpgl_cont_masked_array_t *output_data);
+
+/* ---- additions (no counterpart in the reference) ---- */
+
+/* 0 after a successful call, else one of HPGL_E_*. */
+int hpgl_get_last_error(void);
+#define HPGL_OK 0
+#define HPGL_E_INVALID 1      /* bad arguments (sizes, params, null pointers) */
+#define HPGL_E_CUDA 2         /* CUDA runtime error, or no usable GPU */
+#define HPGL_E_UNSUPPORTED 3  /* outside this build (e.g. max_neighbours > 64) */
+#define HPGL_E_CAPACITY 4     /* a device capacity limit was exceeded */
+#define HPGL_E_INTERNAL 5
+
+/* Arithmetic of the per-node solve used by the reference entry points above
+   and by hpgl_b200_krige when its own field is -1.
+   HPGL_PRECISION_FP64: the reference's FP64 Cholesky in its exact operation
+   order — results bit-identical to the reference's.
+   HPGL_PRECISION_MIXED: FP32 factorisation with FP64 iterative refinement;
+   systems whose FP32 pivots fail a threshold, or whose refinement does not
+   converge, are re-solved with the FP64 path.  Masks are identical to the
+   reference's; estimates and variances agree to <= 1e-6 relative.
+   The default is HPGL_PRECISION_FP64, or the value of the environment
+   variable HPGL_B200_PRECISION ("fp64" / "mixed") at library load. */
+#define HPGL_PRECISION_FP64 0
+#define HPGL_PRECISION_MIXED 1
+void hpgl_b200_set_precision(int precision);
+int hpgl_b200_get_precision(void);
+
+/* Kriging kinds of hpgl_b200_job_t. */
+#define HPGL_KIND_OK 0
+#define HPGL_KIND_SK 1
+#define HPGL_KIND_LVM 2
+#define HPGL_KIND_IK 3
+#define HPGL_KIND_MEDIAN_IK 4
+
+/* One kriging job for hpgl_b200_krige.  `params` holds `n_params` entries
+   (one per category for IK, else 1); hpgl_ik_params_t carries every field
+   the kinds need (m_marginal_prob is used by IK only). */
+typedef struct hpgl_b200_job_t {
+    int kind;
+    int nx, ny, nz;
+    const float *values;          /* OK / SK / LVM input values */
+    const unsigned char *codes;   /* IK / median IK category codes */
+    const unsigned char *mask;    /* informed flags */
+    const float *mean;            /* LVM mean cube */
+    const hpgl_ik_params_t *params;
+    int n_params;
+    int sk_automatic_mean;        /* SK: compute the mean of informed values */
+    double sk_mean;               /* SK: mean when not automatic */
+    double median_marginal1;      /* median IK: marginal probability of code 1 */
+    int precision;                /* HPGL_PRECISION_*, or -1 for the global one */
+} hpgl_b200_job_t;
+
+/* Outputs of hpgl_b200_krige.  out_values (cont) or out_codes (IK) and
+   out_mask are required and must be pre-filled with the input (see above).
+   The rest may be NULL.  Per "system slot" = node, or node*K + k for IK with
+   categories whose parameters differ (node for IK with identical ones):
+   variance     double   kriging variance (-1 when the solve failed)
+   status       int8     0 solved, 1 no neighbours, 2 singular, -1 not kriged
+   nb_count     int32    neighbour count
+   nb_index     int32    neighbour node indices, nb_stride per slot
+   weights      double   kriging weights, nb_stride per slot
+   probs        float    IK: probability per node*K + k; median IK: per node
+   nb_stride must be >= max_neighbours when nb_index or weights is given. */
+typedef struct hpgl_b200_result_t {
+    float *out_values;
+    unsigned char *out_codes;
+    unsigned char *out_mask;
+    double *variance;
+    signed char *status;
+    int *nb_count;
+    int *nb_index;
+    double *weights;
+    float *probs;
+    int nb_stride;
+    /* filled by the call */
+    long long systems;            /* kriging systems attempted */
+    long long systems_fp64;       /* of those, solved by the FP64 path */
+    long long failures;           /* no neighbours + singular */
+    double ms_plan;               /* host planning (template, tables, buckets) */
+    double ms_h2d;
+    double ms_device;             /* device work, CUDA events */
+    double ms_d2h;
+    double ms_total;              /* wall time of the call */
+} hpgl_b200_result_t;
+
+/* Runs one job on the GPU.  Returns 0 or an HPGL_E_* code (message via
+   hpgl_get_last_exception_message). */
+int hpgl_b200_krige(const hpgl_b200_job_t *job, hpgl_b200_result_t *result);
+
+/* Device-resident timing of one job: uploads it once, runs `warmup`
+   untimed and `iters` timed passes of the device pipeline (search, build,
+   solve, estimate) with a write of `flush_bytes` between passes to flush L2,
+   and reports per-pass milliseconds in ms_per_iter[iters] (CUDA events on the
+   launching stream), the dominant kernel's average launch milliseconds and
+   the number of kernel launches per pass.  The job's outputs of the last
+   pass are written like hpgl_b200_krige's. */
+typedef struct hpgl_b200_bench_t {
+    int iters;
+    int warmup;
+    long long flush_bytes;
+    double *ms_per_iter;
+    double ms_top_kernel;         /* average duration of the top kernel */
+    char top_kernel[64];
+    int launches_per_iter;
+    long long systems;
+    long long systems_fp64;
+    double ms_plan;
+} hpgl_b200_bench_t;
+int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl_b200_bench_t *bench);
+
+/* Library build and device description, e.g. for logs. */
+const char *hpgl_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPGL_B200_HPGL_H */
