@@ -1,0 +1,277 @@
+"""Benchmark of the kriging path on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): simple kriging of the 256x256x64 synthetic cube, 1 %
+informed cells from an FFT Gaussian field, exponential variogram (40,20,8)
+azimuth 30, sill 1, nugget 0.05, radii (80,40,16), 32 neighbours, SK mean 0
+(hpgl_b200.workloads.sk_ok_256x256x64) — every uninformed node kriged once.
+Metric: kriged nodes/s.
+
+* ``value``: FP32 factorisation + FP64 refinement, device-resident (inputs
+  in HBM before the timed region; each step re-runs search, covariance
+  build, solve and estimate), CUDA events on the library's stream, 256 MiB
+  written between steps to flush L2; whole job = all ranks' nodes / max rank
+  time.  ``fp64`` holds the same for the bit-exact FP64 path and
+  ``mixed_vs_fp64`` their ratio.
+* ``e2e``: the same metric through the public C ABI (hpgl_b200_krige) from
+  host buffers: planning, host->device copies, device work and device->host
+  copies of the estimate and mask inside each timed call.
+* ``cpu_baseline``: the reference's own kriging (compiled from its sources by
+  oracle/build_ref.sh) on a node sample of the same job, all host threads.
+* ``--impl reference``: that reference CPU path as the timed arm.
+
+Multi-GPU: the path has no exchange step; N ranks (torchrun, one per GPU)
+each krige their own copy of the job ("replicas only", weak scaling).
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "kriged nodes/s"
+WORKLOAD = "sk_256x256x64_exp(40,20,8)_az30_r(80,40,16)_n32_1pct"
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_flops(nb_counts, rhs):
+    """Per-system work of the path: F(N) = 2/3 N^3 (Cholesky) + 2 R N^2
+    (triangular solves) + 4N (combine, variance), plus 20 flop for each of the
+    N(N+1)/2 + N covariance entries; summed over the kriged systems."""
+    n = nb_counts.astype(np.float64)
+    f = 2.0 / 3.0 * n ** 3 + 2.0 * rhs * n ** 2 + 4.0 * n + 20.0 * (n * (n + 1) / 2.0 + n)
+    return float(f.sum())
+
+
+def cpu_reference(job, steps, warmup, sample_nodes, threads):
+    """The reference's own per-node kriging (oracle/_ref) on a node sample;
+    falls back to the oracle restatement when the reference library is not
+    present.  Returns (nodes/s per step list, kind, sample description)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(7)
+    un = np.nonzero(job["mask"] == 0)[0]
+    sample = np.sort(rng.choice(un, min(sample_nodes, len(un)), replace=False)).astype(np.int32)
+    use_ref = O.reference_available()
+    rates = []
+    for it in range(warmup + steps):
+        t = time.perf_counter()
+        if use_ref:
+            O.ref_sample(job, sample, threads=threads)
+        else:
+            O.run(job, node_list=sample, dumps=False, threads=threads)
+        dt = time.perf_counter() - t
+        if it >= warmup:
+            rates.append(len(sample) / dt)
+    kind = "reference" if use_ref else "port"
+    desc = ("%d uniformly sampled uninformed nodes of the same job per step (lookup construction included), "
+            "%d OpenMP threads" % (len(sample), threads))
+    return rates, kind, desc
+
+
+def run_reference_arm(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from hpgl_b200 import workloads as W
+    job = W.sk_ok_256x256x64()
+    threads = os.cpu_count() or 1
+    rates, kind, desc = cpu_reference(job, args.steps, args.warmup, 200000, threads)
+    v = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "nodes/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * 200000 / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": threads, "kind": kind, "sample": desc},
+        "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=200000)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local = _dist()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from hpgl_b200 import build
+    from hpgl_b200 import native as N
+    from hpgl_b200 import workloads as W
+    if not os.path.exists(N.LIB_PATH):
+        build.build()
+    job = W.sk_ok_256x256x64()
+    size = int(np.prod(job["shape"]))
+    kriged = int((job["mask"] == 0).sum())
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # Untimed run of each path first (library warm-up, neighbour counts).
+    dump = N.krige(job, precision="fp64", dumps=True)
+    nbc = dump["nb_count"][dump["status"] >= 0]
+    flops = algorithmic_flops(nbc, rhs=1)
+    del dump
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    ms_mixed, info_m = N.bench(job, precision="mixed", iters=args.steps, warmup=args.warmup)
+    clk = clocks.stop()
+    barrier()
+    ms_fp64, info_f = N.bench(job, precision="fp64", iters=args.steps, warmup=args.warmup)
+    barrier()
+    t_mixed = max_over_ranks(float(ms_mixed.sum()))
+    t_fp64 = max_over_ranks(float(ms_fp64.sum()))
+    value = world * kriged * args.steps / (t_mixed / 1000.0)
+    fp64_value = world * kriged * args.steps / (t_fp64 / 1000.0)
+
+    # End to end through the public API from host buffers.
+    for _ in range(1):
+        N.krige(job, precision="mixed")
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        r = N.krige(job, precision="mixed")
+        e2e_ms.append(r["ms_total"])
+    t_e2e = max_over_ranks(float(np.sum(e2e_ms)))
+    e2e_value = world * kriged * args.steps / (t_e2e / 1000.0)
+    h2d = size * 4 + size * 1
+    d2h = size * 4 + size * 1
+
+    # Roofline of the dominant kernel (the solve): algorithmic flops per
+    # launch / CUDA-event duration; FP32 CUDA-core peak (nominal: 148 SMs x
+    # 128 FP32 lanes x 2 flop x 1.965 GHz).
+    peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
+    achieved = flops / (info_m["ms_top_kernel"] / 1000.0) / 1e12
+    roofline = {"kernel": info_m["top_kernel"], "bound": "fp32", "achieved": achieved, "peak": peak_fp32,
+                "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": None,
+                "peak_source": "nominal FP32 CUDA-core peak (MEASURED_PEAKS.json has HBM and bf16 tensor only)",
+                "ms_per_launch": info_m["ms_top_kernel"], "flop_per_launch": flops}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rates, kind, desc = cpu_reference(job, 2, 1, args.cpu_sample, threads)
+        cpu = {"value": float(np.median(rates)), "unit": "nodes/s", "cores": threads, "kind": kind,
+               "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": list(job["shape"]), "kriged_nodes_per_step": kriged,
+                       "precision": "fp32 factorisation + fp64 refinement, fp64 re-solve of routed systems",
+                       "l2": "256 MiB written between steps", "parallelism": "replicas%d" % world},
+            "fp64": {"value": fp64_value, "ms_per_step": t_fp64 / args.steps,
+                     "top_kernel_ms": info_f["ms_top_kernel"]},
+            "mixed_vs_fp64": value / fp64_value,
+            "routed_to_fp64": info_m["systems_fp64"] / max(1, info_m["systems"]),
+            "e2e": {"value": e2e_value, "unit": "nodes/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": t_e2e / args.steps},
+            "roofline": roofline,
+            "clocks": clk,
+            "gpu_launches": info_m["launches"] * args.steps,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -284,3 +284,21 @@ def ref_template(p):
     buf = np.zeros(cap * 3, dtype=np.int32)
     n = ref.ref_template(C.byref(_ok_params(p)), _ptr(buf, C.c_int), cap)
     return buf[: 3 * n].reshape(n, 3)
+
+
+def ref_sample(job, node_list, threads=0, kind=None):
+    """The reference's own per-node kriging on `node_list` (OK or SK);
+    returns the estimates (NaN where the system failed)."""
+    ref = reference()
+    kind = kind or job["kind"]
+    nx, ny, nz = job["shape"]
+    values = np.array(job["values"], dtype=np.float32)
+    mask = np.array(job["mask"], dtype=np.uint8)
+    nl = np.ascontiguousarray(node_list, dtype=np.int32)
+    out = np.zeros(len(nl), dtype=np.float32)
+    rc = ref.ref_sample_cont(KINDS[kind], nx, ny, nz, _ptr(values, C.c_float), _ptr(mask, C.c_ubyte),
+                             C.byref(_ok_params(job["params"][0])), C.c_double(job.get("sk_mean", 0.0)),
+                             _ptr(nl, C.c_int), len(nl), int(threads), _ptr(out, C.c_float))
+    if rc != 0:
+        raise RuntimeError("reference sample failed")
+    return out

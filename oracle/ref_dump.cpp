@@ -203,3 +203,56 @@ int ref_template(const hpgl_ok_params_t *p, int *out_xyz, int cap) {
     return (int)v.size();
 }
 }
+
+extern "C" {
+// Times nothing itself: runs the reference's per-node kriging
+// (kriging_interpolation, kriging_interpolation.h:228-265, with the lookup
+// and covariance objects its drivers build) on the nodes of `node_list`, in
+// an OpenMP loop like cont_kriging's (cont_kriging.h:392-429).  The lookup
+// construction (template sort, clusterizer fill) runs first and is included.
+// kind: 0 OK, 1 SK.  Estimates go to out[i] (NaN on failure).  Returns 0.
+int ref_sample_cont(int kind, int nx, int ny, int nz, float *values, unsigned char *mask, const hpgl_ok_params_t *p,
+                    double sk_mean, const int *node_list, int n_nodes, int threads, float *out) {
+    try {
+        if (threads > 0) omp_set_num_threads(threads);
+        sugarbox_grid_t grid;
+        grid.init(nx, ny, nz);
+        int size = nx * ny * nz;
+        cont_property_array_t prop(values, mask, size);
+        ok_params_t params;
+        fill_ok_params(p, params);
+        is_informed_predicate_t<cont_property_array_t> pred(prop);
+        if (kind == 0) {
+            cov_model_t cov(params);
+            indexed_neighbour_lookup_t<sugarbox_grid_t, cov_model_t> nl(&grid, &cov, params);
+            for (node_index_t n = 0; n < size; ++n)
+                if (prop.is_informed(n)) nl.add_node(n);
+            no_mean_t mp;
+            ok_weight_calculator_t wc;
+#pragma omp parallel for
+            for (int i = 0; i < n_nodes; ++i) {
+                cont_value_t v;
+                ki_result_t r = kriging_interpolation(prop, pred, node_list[i], cov, mp, nl, wc, v);
+                out[i] = r == KI_SUCCESS ? v : NAN;
+            }
+        } else {
+            precalculated_covariances_t cov(cov_model_t(params), params.m_radiuses);
+            indexed_neighbour_lookup_t<sugarbox_grid_t, precalculated_covariances_t> nl(&grid, &cov, params);
+            for (node_index_t n = 0; n < size; ++n)
+                if (prop.is_informed(n)) nl.add_node(n);
+            single_mean_t mp(sk_mean);
+            sk_weight_calculator_t wc;
+#pragma omp parallel for
+            for (int i = 0; i < n_nodes; ++i) {
+                cont_value_t v;
+                ki_result_t r = kriging_interpolation(prop, pred, node_list[i], cov, mp, nl, wc, v);
+                out[i] = r == KI_SUCCESS ? v : NAN;
+            }
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "ref_sample_cont: %s\n", e.what());
+        return 1;
+    }
+}
+}
