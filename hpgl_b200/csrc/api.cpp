@@ -280,8 +280,11 @@ int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl
 
 const char *hpgl_b200_version(void) { return "hpgl_b200 0.1 (sm_100a kriging path)"; }
 
-int hpgl_simple_kriging_weights(float *, float *, float *, float *, int, hpgl_cov_params_t *, float *) {
-    int rc = guarded("hpgl_simple_kriging_weights", [&] { not_provided("hpgl_simple_kriging_weights"); });
+int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y, float *neighbours_z,
+                                int neighbours_count, hpgl_cov_params_t *params, float *weights) {
+    int rc = guarded("hpgl_simple_kriging_weights", [&] {
+        sk_weights_alloc(center_coords, neighbours_x, neighbours_y, neighbours_z, neighbours_count, params, weights);
+    });
     return rc == HPGL_OK ? 0 : -1;
 }
 

@@ -214,3 +214,37 @@ def bench(job, precision="mixed", iters=5, warmup=3, flush_bytes=256 << 20, kind
                 systems=b.systems, systems_fp64=b.systems_fp64, ms_plan=b.ms_plan, out=p.out,
                 out_mask=p.out_mask)
     return ms, info
+
+
+class HpglCovParams(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double)]
+
+
+def cov_struct(p):
+    cp = HpglCovParams()
+    cp.covariance_type = p["cov_type"]
+    cp.ranges[:] = p["ranges"]
+    cp.angles[:] = p["angles"]
+    cp.sill = p["sill"]
+    cp.nugget = p["nugget"]
+    return cp
+
+
+def sk_weights(center, xs, ys, zs, p, entry="hpgl_simple_kriging_weights"):
+    """Simple-kriging weights of one point through the C ABI entry `entry`
+    (the reference's signature).  Returns float32 weights; raises HpglError."""
+    L = lib()
+    fn = getattr(L, entry)
+    n = len(xs)
+    c = (C.c_float * 3)(*[float(v) for v in center])
+    x = np.ascontiguousarray(xs, dtype=np.float32)
+    y = np.ascontiguousarray(ys, dtype=np.float32)
+    z = np.ascontiguousarray(zs, dtype=np.float32)
+    w = np.zeros(n, dtype=np.float32)
+    cp = cov_struct(p)
+    rc = fn(c, _ptr(x, C.c_float), _ptr(y, C.c_float), _ptr(z, C.c_float), n, C.byref(cp), _ptr(w, C.c_float))
+    if rc != 0:
+        code, msg = last_error()
+        raise HpglError(code, msg)
+    return w

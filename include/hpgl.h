@@ -189,8 +189,10 @@ void hpgl_indicator_kriging(hpgl_ind_masked_array_t *in_data, hpgl_ind_masked_ar
 void hpgl_median_ik(hpgl_ind_masked_array_t *in_data, hpgl_median_ik_params_t *params,
                     hpgl_ind_masked_array_t *out_data);
 
-/* api.h:232-240, api.cpp:292-342.  Simple-kriging weights of one point.
-   Not provided by this build: records an error and returns -1. */
+/* api.h:232-240, api.cpp:292-342.  Simple-kriging weights of one point
+   from explicit neighbour coordinates, computed on the GPU.  Returns 0, or
+   -1 with the last-error state set (singular system, bad arguments, more
+   than 1024 neighbours).  With neighbours_count == 0 nothing is written. */
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y,
                                 float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                 float *weights);

@@ -630,3 +630,44 @@ int oracle_template(const oracle_params_t *p, int truncated, int *out_xyz, int c
     return n;
 }
 }
+
+extern "C" {
+// Simple-kriging weights of one point from explicit coordinates:
+// hpgl_simple_kriging_weights (api.cpp:292-342) over simple_kriging_weights
+// (simple_kriging.cpp:15-35): float coordinates widened to double, the
+// untruncated model on real-valued offsets, sk_kriging_weights_3
+// (my_kriging_weights.h:26-129).  Returns 0, or 1 when the system is not
+// positive definite (the reference then reads past an emptied vector).
+int oracle_sk_weights(const float *center, const float *xs, const float *ys, const float *zs, int n,
+                      const oracle_params_t *p, float *weights) {
+    try {
+        cov_model model(*p);
+        if (n <= 0) return 0;
+        double c[3] = {center[0], center[1], center[2]};
+        std::vector<double> pts(3 * (size_t)n);
+        for (int i = 0; i < n; ++i) {
+            pts[3 * i] = xs[i];
+            pts[3 * i + 1] = ys[i];
+            pts[3 * i + 2] = zs[i];
+        }
+        std::vector<double> A((size_t)n * n), b(n);
+        for (int i = 0; i < n; ++i) {
+            for (int j = i; j < n; ++j) {
+                A[(size_t)i * n + j] = model(pts[3 * i] - pts[3 * j], pts[3 * i + 1] - pts[3 * j + 1],
+                                             pts[3 * i + 2] - pts[3 * j + 2]);
+                A[(size_t)j * n + i] = A[(size_t)i * n + j];
+            }
+            b[i] = model(pts[3 * i] - c[0], pts[3 * i + 1] - c[1], pts[3 * i + 2] - c[2]);
+        }
+        if (n > 64) return 2;
+        int info = oracle_dpotf2_upper(n, A.data(), n);
+        std::vector<double> w(b);
+        oracle_dpotrs_upper(n, 1, A.data(), n, w.data(), n);
+        if (info != 0) return 1;
+        for (int i = 0; i < n; ++i) weights[i] = (float)w[i];
+        return 0;
+    } catch (const std::exception &) {
+        return 3;
+    }
+}
+}

@@ -302,3 +302,41 @@ def ref_sample(job, node_list, threads=0, kind=None):
     if rc != 0:
         raise RuntimeError("reference sample failed")
     return out
+
+
+def sk_weights(center, xs, ys, zs, p):
+    """Restated hpgl_simple_kriging_weights; returns (status, float32 weights)."""
+    lib = restated()
+    n = len(xs)
+    c = np.ascontiguousarray(center, dtype=np.float32)
+    x = np.ascontiguousarray(xs, dtype=np.float32)
+    y = np.ascontiguousarray(ys, dtype=np.float32)
+    z = np.ascontiguousarray(zs, dtype=np.float32)
+    w = np.zeros(n, dtype=np.float32)
+    rc = lib.oracle_sk_weights(_ptr(c, C.c_float), _ptr(x, C.c_float), _ptr(y, C.c_float), _ptr(z, C.c_float), n,
+                               C.byref(oracle_params(p)), _ptr(w, C.c_float))
+    return rc, w
+
+
+def ref_sk_weights(center, xs, ys, zs, p):
+    """The compiled reference's hpgl_simple_kriging_weights (float32 weights)."""
+    ref = reference()
+
+    class CovParams(C.Structure):
+        _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                    ("sill", C.c_double), ("nugget", C.c_double)]
+    cp = CovParams()
+    cp.covariance_type = p["cov_type"]
+    cp.ranges[:] = p["ranges"]
+    cp.angles[:] = p["angles"]
+    cp.sill = p["sill"]
+    cp.nugget = p["nugget"]
+    n = len(xs)
+    c = (C.c_float * 3)(*center)
+    x = np.ascontiguousarray(xs, dtype=np.float32)
+    y = np.ascontiguousarray(ys, dtype=np.float32)
+    z = np.ascontiguousarray(zs, dtype=np.float32)
+    w = np.zeros(n, dtype=np.float32)
+    ref.hpgl_simple_kriging_weights(c, _ptr(x, C.c_float), _ptr(y, C.c_float), _ptr(z, C.c_float), n, C.byref(cp),
+                                    _ptr(w, C.c_float))
+    return w
