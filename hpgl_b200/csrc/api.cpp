@@ -288,6 +288,15 @@ int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float
     return rc == HPGL_OK ? 0 : -1;
 }
 
+int hpgl_b200_simple_kriging_weights_static(float *center_coords, float *neighbours_x, float *neighbours_y,
+                                            float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
+                                            float *weights) {
+    int rc = guarded("hpgl_b200_simple_kriging_weights_static", [&] {
+        sk_weights_static(center_coords, neighbours_x, neighbours_y, neighbours_z, neighbours_count, params, weights);
+    });
+    return rc == HPGL_OK ? 0 : -1;
+}
+
 void hpgl_read_inc_file_float(char *, float, int, float *, unsigned char *) {
     guarded("hpgl_read_inc_file_float", [&] { not_provided("INC file reading"); });
 }

@@ -23,6 +23,10 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
 void sk_weights_alloc(const float *center, const float *xs, const float *ys, const float *zs, int n,
                       const hpgl_cov_params_t *p, float *weights);
 
+// The same without any device allocation (static scratch, sk_weights.cu).
+void sk_weights_static(const float *center, const float *xs, const float *ys, const float *zs, int n,
+                       const hpgl_cov_params_t *p, float *weights);
+
 int default_precision();
 void set_default_precision(int p);
 

@@ -203,4 +203,71 @@ void sk_weights_alloc(const float *center, const float *xs, const float *ys, con
     WCHECK(cudaFree(scratch));
 }
 
+// ---- the same kernel without any device allocation -------------------------
+//
+// hpgl_b200_simple_kriging_weights_static (include/hpgl.h) serves callers that
+// must not allocate device memory: cudaMalloc/cudaFree synchronise the whole
+// device (stalling the caller's other streams), and a host application that
+// has reserved the GPU's memory for its own pool leaves nothing to allocate.
+// Its scratch is this file-scope array: every GPU that loads the library
+// holds it until the process exits.  Every call shares it and leaves the last
+// call's contents behind; k_sk_weights writes each word of its layout before
+// reading it (coordinates by the host copy, then A, b, x and the status word
+// by the kernel), so nothing needs clearing between calls.  Calls that
+// overlapped on the GPU would race on the array; this library serialises its
+// own calls with a lock.
+constexpr int STATIC_WEIGHTS_MAX = HPGL_B200_STATIC_WEIGHTS_MAX;
+constexpr size_t STATIC_WEIGHTS_BYTES = (WeightsScratchLayout::bytes(STATIC_WEIGHTS_MAX) + 255) / 256 * 256;
+static __device__ __align__(256) unsigned char g_weights_scratch[STATIC_WEIGHTS_BYTES];
+
+static std::mutex g_static_mutex;
+static void *g_static_addr[256];
+
+// Device address of g_weights_scratch on the current device.  In host code
+// the array's name is only a stand-in, never a device address, so the real
+// address is looked up once per device (first call on that device, with it
+// current) and cached.
+static double *static_scratch() {
+    int dev = 0;
+    WCHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) throw HpglError{HPGL_E_UNSUPPORTED, "device ordinal above 255"};
+    if (!g_static_addr[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_weights_scratch);
+        if (e != cudaSuccess || !ptr)
+            throw HpglError{HPGL_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
+        g_static_addr[dev] = ptr;
+    }
+    return (double *)g_static_addr[dev];
+}
+
+void sk_weights_static(const float *center, const float *xs, const float *ys, const float *zs, int n,
+                       const hpgl_cov_params_t *p, float *weights) {
+    check_inputs(center, xs, ys, zs, n, p, weights);
+    if (n > STATIC_WEIGHTS_MAX)
+        throw HpglError{HPGL_E_CAPACITY, "neighbours_count above the static scratch limit of " +
+                                             std::to_string(STATIC_WEIGHTS_MAX)};
+    const CovDev cov = make_cov(p);
+    if (n == 0) return;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    double *scratch = static_scratch();
+    double coords[3 * STATIC_WEIGHTS_MAX + 3];
+    for (int i = 0; i < n; ++i) {
+        coords[3 * i] = xs[i];
+        coords[3 * i + 1] = ys[i];
+        coords[3 * i + 2] = zs[i];
+    }
+    for (int i = 0; i < 3; ++i) coords[3 * n + i] = center[i];
+    WCHECK(cudaMemcpy(scratch, coords, (3 * (size_t)n + 3) * sizeof(double), cudaMemcpyHostToDevice));
+    k_sk_weights<<<1, 32>>>(cov, n, scratch);
+    WCHECK(cudaGetLastError());
+    double x[STATIC_WEIGHTS_MAX + 1];
+    const double *dx = scratch + 3 * (size_t)n + 3 + (size_t)n * n + n;
+    WCHECK(cudaMemcpy(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost));
+    int status = 0;
+    WCHECK(cudaMemcpy(&status, dx + n, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) throw HpglError{HPGL_E_INVALID, "kriging system is not positive definite"};
+    for (int i = 0; i < n; ++i) weights[i] = (float)x[i];
+}
+
 }  // namespace hpgl_b200

@@ -335,6 +335,25 @@ typedef struct hpgl_b200_bench_t {
 } hpgl_b200_bench_t;
 int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl_b200_bench_t *bench);
 
+/* No counterpart in the reference.  hpgl_simple_kriging_weights for callers
+   that cannot allocate device memory: cudaMalloc and cudaFree synchronise
+   the whole device, stalling the caller's other GPU work, and a host
+   application that has reserved the GPU's memory for its own pool leaves
+   nothing to allocate.  Same arguments, results and error convention as
+   hpgl_simple_kriging_weights; it calls no cudaMalloc, cudaFree or other
+   allocating routine.  Its scratch is a fixed device array inside the
+   library, present on every GPU that loads it until the process exits, sized
+   for at most HPGL_B200_STATIC_WEIGHTS_MAX neighbours: larger counts return
+   -1 with HPGL_E_CAPACITY.  The first call on a device looks up the array's
+   device address (make that first call before any stream capture).  All
+   calls share the array and it keeps the last call's contents; the library
+   serialises its own calls, and calls that overlapped on the GPU would race
+   on it. */
+#define HPGL_B200_STATIC_WEIGHTS_MAX 256
+int hpgl_b200_simple_kriging_weights_static(float *center_coords, float *neighbours_x, float *neighbours_y,
+                                            float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
+                                            float *weights);
+
 /* Library build and device description, e.g. for logs. */
 const char *hpgl_b200_version(void);
 
