@@ -1,0 +1,69 @@
+// Device helpers shared by the kernel files.
+#pragma once
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace hpgl_b200 {
+
+#define FULL_MASK 0xffffffffu
+
+__device__ __forceinline__ bool is_cont(int kind) { return kind <= 2; }
+
+// Covariance of offset v (grid steps) from the plan's table.  Truncated kinds
+// read 0 beyond the search radii (precalculated_covariance.h:60-75,
+// covariance_field.h:144-153); the table box covers every offset the search
+// can produce, anything else is a broken invariant.
+// For truncated kinds T = min(radii, B) and every |v| <= n-1 <= B, so the
+// table covers all in-radius offsets; for ordinary kriging T = B covers
+// every offset the search produces (an offset beyond it raises an error bit).
+__device__ __forceinline__ bool cov_in_range(const DevPlan &P, int vx, int vy, int vz) {
+    return (unsigned)(vx + P.Tx) <= (unsigned)(2 * P.Tx) && (unsigned)(vy + P.Ty) <= (unsigned)(2 * P.Ty) &&
+           (unsigned)(vz + P.Tz) <= (unsigned)(2 * P.Tz);
+}
+
+// lin = vz*syx + vy*sx + vx, the table offset of v relative to its centre.
+__device__ __forceinline__ double cov_lin(const DevPlan &P, int vx, int vy, int vz, int lin, int *err) {
+    if (!cov_in_range(P, vx, vy, vz)) {
+        if (!P.truncated) atomicOr(err, DERR_TABLE_RANGE);
+        return 0.0;
+    }
+    return __ldg(P.table + (P.center + lin));
+}
+
+__device__ __forceinline__ double cov_at(const DevPlan &P, int vx, int vy, int vz, int *err) {
+    return cov_lin(P, vx, vy, vz, vz * P.syx + vy * P.sx + vx, err);
+}
+
+// Node coordinates, sugarbox_grid.cpp:70-74.
+__device__ __forceinline__ void node_xyz(int idx, int nx, int ny, int &x, int &y, int &z) {
+    x = idx % nx;
+    y = idx % (nx * ny) / nx;
+    z = idx / (nx * ny);
+}
+
+// A node takes the template walk when any of its 27 neighbouring clusterizer
+// boxes overflowed (sugarbox_indexed_neighbour_lookup.h:68-71).
+__device__ __forceinline__ bool node_clean(const DevPlan &P, int x, int y, int z) {
+    int cx = (int)(x / P.crx), cy = (int)(y / P.cry), cz = (int)(z / P.crz);
+    return P.bucket_clean[((long long)cz * P.my + cy) * P.mx + cx] != 0;
+}
+
+__device__ __forceinline__ bool node_needs_kriging(const DevJob &J, int node) {
+    return is_cont(J.kind) ? J.mask[node] == 0 : true;
+}
+
+// Correctly rounded quotient a / b from y = RN(1/b): q = RN(a*y) is within
+// one ulp of a/b, r = a - b*q is exact in one fused multiply-add, and
+// RN(q + r*y) is the correctly rounded quotient (Markstein's theorem, IBM J.
+// Res. Dev. 34(1), 1990, for round-to-nearest binary arithmetic away from
+// overflow and the subnormal range).  Bit-identical to __ddiv_rn on the
+// kriging systems' magnitudes; tests/test_division.py checks it against
+// __ddiv_rn on the GPU.
+__device__ __forceinline__ double div_by_rcp(double a, double b, double y) {
+    const double q = __dmul_rn(a, y);
+    const double r = __fma_rn(-q, b, a);
+    return __fma_rn(r, y, q);
+}
+
+}  // namespace hpgl_b200

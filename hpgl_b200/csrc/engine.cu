@@ -232,9 +232,13 @@ static void upload_plan(Group &g, cudaStream_t s) {
     d.Bx = P.B[0];
     d.By = P.B[1];
     d.Bz = P.B[2];
-    d.Tx = P.truncated ? P.trunc[0] : INT_MAX;
-    d.Ty = P.truncated ? P.trunc[1] : INT_MAX;
-    d.Tz = P.truncated ? P.trunc[2] : INT_MAX;
+    d.Tx = std::min(P.trunc[0], P.B[0]);
+    d.Ty = std::min(P.trunc[1], P.B[1]);
+    d.Tz = std::min(P.trunc[2], P.B[2]);
+    d.sx = 2 * P.B[0] + 1;
+    d.syx = d.sx * (2 * P.B[1] + 1);
+    d.center = P.B[2] * d.syx + P.B[1] * d.sx + P.B[0];
+    d.truncated = P.truncated ? 1 : 0;
     d.c0 = P.c0;
     d.bucket_start = B.bucket_start.p;
     d.bucket_nodes = B.bucket_nodes.p;

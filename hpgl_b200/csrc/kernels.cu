@@ -5,30 +5,15 @@
 //   k_solve<NMAX,MODE> covariance build + Cholesky solve + estimate/variance
 //   k_ik_argmax        most probable category
 // Paths cited are relative to the reference's src/geo_bsd/hpgl/.
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 
+#include "device_common.cuh"
 #include "introsort.h"
 #include "kernels.cuh"
 
 namespace hpgl_b200 {
-
-#define FULL_MASK 0xffffffffu
-
-__device__ __forceinline__ bool is_cont(int kind) { return kind <= 2; }
-
-// Covariance of offset v (grid steps) from the plan's table.  Truncated kinds
-// read 0 beyond the search radii (precalculated_covariance.h:60-75,
-// covariance_field.h:144-153); the table box covers every offset the search
-// can produce, anything else is a broken invariant.
-__device__ __forceinline__ double cov_at(const DevPlan &P, int vx, int vy, int vz, int *err) {
-    if (abs(vx) > P.Tx || abs(vy) > P.Ty || abs(vz) > P.Tz) return 0.0;
-    if (abs(vx) > P.Bx || abs(vy) > P.By || abs(vz) > P.Bz) {
-        atomicOr(err, DERR_TABLE_RANGE);
-        return 0.0;
-    }
-    return __ldg(&P.table[((long long)(vz + P.Bz) * (2 * P.By + 1) + (vy + P.By)) * (2 * P.Bx + 1) + (vx + P.Bx)]);
-}
 
 // ---------------------------------------------------------------------------
 // informed-bit rows: bit j of word w of row (z*ny + y) is padded x = 32w + j,
@@ -48,76 +33,75 @@ __global__ void k_build_bits(DevJob J, DevPlan P, uint32_t *bits) {
     bits[t] = word;
 }
 
-// Node coordinates, sugarbox_grid.cpp:70-74.
-__device__ __forceinline__ void node_xyz(int idx, int nx, int ny, int &x, int &y, int &z) {
-    x = idx % nx;
-    y = idx % (nx * ny) / nx;
-    z = idx / (nx * ny);
-}
-
-// A node takes the template walk when any of its 27 neighbouring clusterizer
-// boxes overflowed (sugarbox_indexed_neighbour_lookup.h:68-71).
-__device__ __forceinline__ bool node_clean(const DevPlan &P, int x, int y, int z) {
-    int cx = (int)(x / P.crx), cy = (int)(y / P.cry), cz = (int)(z / P.crz);
-    return P.bucket_clean[((long long)cz * P.my + cy) * P.mx + cx] != 0;
-}
-
-__device__ __forceinline__ bool node_needs_kriging(const DevJob &J, int node) {
-    return is_cont(J.kind) ? J.mask[node] == 0 : true;
-}
-
 // ---------------------------------------------------------------------------
-// Template search (neighbour_lookup_t::find, sugarbox_neighbour_lookup.h:35-61):
-// each thread owns a 32-node x-segment of one grid row and walks the sorted
-// template once for all 32 nodes.  For template offset (dx,dy,dz) the
-// informed flags of the 32 target cells are one funnel-shifted 32-bit window
-// of the padded bit row (y+dy, z+dz), so a step costs two word loads and a
-// few integer ops; out-of-grid cells are 0 bits (padding / skipped rows),
-// matching is_informed(-1) == false.  Hits are appended per node in template
-// order until the node holds max_neighbours.
-__global__ void __launch_bounds__(128) k_search_template(DevJob J, DevPlan P) {
-    __shared__ uint8_t cnt_sm[128 * 33];
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    long long total = (long long)P.nseg * J.ny * J.nz;
-    if (t >= total) return;
-    const int seg = (int)(t % P.nseg);
-    const long long row = t / P.nseg;
-    const int y = (int)(row % J.ny), z = (int)(row / J.ny);
-    const int x0 = seg * 32;
-    const int base = (int)(row * J.nx) + x0;
-    uint8_t *cnt = cnt_sm + threadIdx.x * 33;
-    uint32_t active = 0;
-    for (int b = 0; b < 32; ++b) {
-        cnt[b] = 0;
-        int x = x0 + b;
-        if (x < J.nx && node_needs_kriging(J, base + b) && !node_clean(P, x, y, z)) active |= 1u << b;
+// Template search (neighbour_lookup_t::find, sugarbox_neighbour_lookup.h:35-61).
+// One warp per 32-node x-segment of a grid row walks the sorted template 32
+// entries at a time: lane t loads entry base+t and forms the 32-bit window of
+// informed flags of the segment's 32 target cells at that offset (one
+// funnel shift of two words of bit row (y+dy, z+dz); out-of-grid cells are 0
+// bits, matching is_informed(-1) == false).  A 32x32 bit transpose across
+// the lanes turns the windows into, for node b (lane b), the mask of chunk
+// entries that hit it; lane b appends them in template order until it holds
+// max_neighbours.  Nodes that do not take the template path (clean
+// clusterizer neighbourhoods) or need no kriging never become active.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+    const uint32_t lo_masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int st = 0; st < 5; ++st) {
+        const int j = 16 >> st;
+        const uint32_t m = lo_masks[st];
+        const uint32_t y = __shfl_xor_sync(FULL_MASK, x, j);
+        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y & m) << j));
     }
-    const int nmax = P.nmax;
-    uint32_t rem = active;
-    const uint32_t *bits = J.bits;
-    for (int ti = 0; ti < P.tmpl_len && rem; ++ti) {
-        const int4 e = __ldg(&P.tmpl[ti]);
-        const int yy = y + e.y, zz = z + e.z;
-        if ((unsigned)yy >= (unsigned)J.ny || (unsigned)zz >= (unsigned)J.nz) continue;
-        const uint32_t *rp = bits + ((long long)zz * J.ny + yy) * P.wpr + seg + (e.x >> 5);
-        const uint32_t w = __funnelshift_r(__ldg(rp), __ldg(rp + 1), e.x & 31);
-        uint32_t hits = w & rem;
-        while (hits) {
-            const int b = __ffs(hits) - 1;
-            hits &= hits - 1;
-            const int node = base + b;
-            int c = cnt[b];
-            J.nb[(long long)node * nmax + c] = node + e.w;
-            ++c;
-            cnt[b] = (uint8_t)c;
-            if (c == nmax) rem &= ~(1u << b);
+    return x;
+}
+
+__global__ void __launch_bounds__(256) k_search_template(DevJob J, DevPlan P) {
+    __shared__ int delta_sm[8][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long total = (long long)P.nseg * J.ny * J.nz;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    int *dsm = delta_sm[wib];
+    for (long long segi = (long long)blockIdx.x * (blockDim.x >> 5) + wib; segi < total; segi += nwarps) {
+        const int seg = (int)(segi % P.nseg);
+        const long long row = segi / P.nseg;
+        const int y = (int)(row % J.ny), z = (int)(row / J.ny);
+        const int x0 = seg * 32;
+        const int base = (int)(row * J.nx) + x0;
+        const int node = base + lane;
+        const bool act = x0 + lane < J.nx && node_needs_kriging(J, node) && !node_clean(P, x0 + lane, y, z);
+        uint32_t active = __ballot_sync(FULL_MASK, act);
+        if (!active) continue;
+        const int nmax = P.nmax;
+        int cnt = 0;
+        int *out = J.nb + (long long)node * nmax;
+        const uint32_t *bits = J.bits;
+        for (int tb = 0; tb < P.tmpl_len && active; tb += 32) {
+            const int t = tb + lane;
+            uint32_t w = 0;
+            int delta = 0;
+            if (t < P.tmpl_len) {
+                const int4 e = __ldg(&P.tmpl[t]);
+                delta = e.w;
+                const int yy = y + e.y, zz = z + e.z;
+                if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
+                    const uint32_t *rp = bits + ((long long)zz * J.ny + yy) * P.wpr + seg + (e.x >> 5);
+                    w = __funnelshift_r(__ldg(rp), __ldg(rp + 1), e.x & 31);
+                }
+            }
+            w &= active;
+            dsm[lane] = delta;
+            uint32_t hits = transpose32(w, lane);
+            __syncwarp();
+            while (hits && cnt < nmax) {
+                const int tt = __ffs(hits) - 1;
+                hits &= hits - 1;
+                out[cnt++] = node + dsm[tt];
+            }
+            __syncwarp();
+            active = __ballot_sync(FULL_MASK, act && cnt < nmax);
         }
-    }
-    uint32_t a = active;
-    while (a) {
-        const int b = __ffs(a) - 1;
-        a &= a - 1;
-        J.nbcount[base + b] = cnt[b];
+        if (act) J.nbcount[node] = cnt;
     }
 }
 
@@ -787,8 +771,11 @@ void launch_build_bits(const DevJob &J, const DevPlan &P, uint32_t *bits, cudaSt
 }
 
 void launch_search_template(const DevJob &J, const DevPlan &P, cudaStream_t s) {
-    long long n = (long long)P.nseg * J.ny * J.nz;
-    k_search_template<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(J, P);
+    const long long segs = (long long)P.nseg * J.ny * J.nz;
+    long long blocks = (segs + 7) / 8;
+    const long long cap = (long long)sm_count() * 8;  // 8 blocks of 8 warps per SM
+    if (blocks > cap) blocks = cap;
+    k_search_template<<<(unsigned)std::max<long long>(1, blocks), 256, 0, s>>>(J, P);
 }
 
 void launch_search_cluster(const DevJob &J, const DevPlan &P, double *sk, int *si, int n_warps, cudaStream_t s) {
@@ -818,6 +805,10 @@ void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *n
                   int n_list_max, cudaStream_t s) {
     long long n_max = node_list ? (long long)n_list_max : J.size;
     if (n_max <= 0) return;
+    if (P.nmax <= 32) {
+        launch_solve32(J, P, precision, node_list, n_list, n_max, s);
+        return;
+    }
     if (P.nmax <= 32) {
         if (precision == 0) launch_solve_t<32, 0>(J, P, node_list, n_list, n_max, s);
         else launch_solve_t<32, 1>(J, P, node_list, n_list, n_max, s);

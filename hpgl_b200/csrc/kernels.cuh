@@ -24,7 +24,10 @@ struct DevPlan {
     // covariance table
     const double *table;
     int Bx, By, Bz;
-    int Tx, Ty, Tz;          // truncation half extents
+    int Tx, Ty, Tz;          // half extents read from the table (beyond: 0)
+    int sx, syx;             // table strides (x, then y*x)
+    int center;              // table index of offset 0
+    int truncated;           // beyond T is the model's 0 (else a broken invariant)
     double c0;
     // clusterizer
     const int *bucket_start;
@@ -83,6 +86,9 @@ void launch_search_cluster(const DevJob &J, const DevPlan &P, double *scratch_ke
 void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                   int n_list_max, cudaStream_t s);
 void launch_ik_argmax(const DevJob &J, cudaStream_t s);
+// solve32.cu: register-resident solves for max_neighbours <= 32
+void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
+                    long long n_max, cudaStream_t s);
 int solve_kernel_count();
 
 }  // namespace hpgl_b200

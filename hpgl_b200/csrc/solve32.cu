@@ -1,0 +1,541 @@
+// Register-resident per-node solves for systems of at most 32 neighbours
+// (one warp per system, persistent over the grid's nodes).
+//
+//   k_solve_exact32  FP64 in the reference's exact operation order
+//                    (my_kriging_weights.h:26-255 over LAPACK DPOTF2/DPOTRS):
+//                    lane k holds column k of the system in registers; the
+//                    finished part of column j is broadcast through shared
+//                    memory as 16-byte pairs for the dot products of step j.
+//   k_solve_mixed32  FP32 Gauss-Jordan inverse of the (unit-diagonal scaled)
+//                    system, lane r holding row r, every solve a parallel
+//                    matrix-vector product; FP64 residuals against the exact
+//                    FP64 system refine the solution.  Systems whose FP32
+//                    pivots fall below 1e-3 (the FP64 factorisation cannot
+//                    fail above that), or whose refinement stalls, are routed
+//                    to the exact kernel.
+//
+// Both start from the same system: neighbour offsets from the search lists
+// and covariances gathered from the plan's table (my_kriging_weights.h:49-58,
+// 156-165), padded to 32x32 with the identity.
+#include "device_common.cuh"
+
+namespace hpgl_b200 {
+
+namespace {
+
+constexpr int N32 = 32;
+constexpr int WARPS32 = 4;
+constexpr float MIXED_PIVOT_MIN = 1e-3f;  // on the unit-diagonal scaled system
+constexpr double MIXED_ACCEPT_1 = 1e-7;   // |d| / |x| after the first correction
+constexpr double MIXED_ACCEPT_N = 1e-7;   // after later corrections
+constexpr int MIXED_MAX_CORR = 3;
+
+struct SysSmem {
+    double A[N32 * 34];     // exact: in-place factor (column k at k*34); mixed: full system (LD 33)
+    double vd[N32];         // double vector broadcast
+    float vf[2][N32];       // float vector broadcast
+    float row[2][N32];      // mixed: pivot row broadcast (double buffered)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
+    return v;
+}
+
+// Per-node prologue shared by both kernels.  Returns n (neighbour count) and
+// fills the lane's neighbour data; the system itself is built separately.
+struct NodeData {
+    int n;
+    float dv;   // cont: value - mean of row `lane` (float, combiner.h:18-22)
+    int code;   // IK: category code of row `lane`
+    double b;   // b_lane = C(x_lane - x0)
+    int ox, oy, oz, lin;  // offset of neighbour `lane` from the node, and its table offset
+};
+
+__device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane) {
+    NodeData d;
+    d.n = J.nbcount[node];
+    int x0, y0, z0;
+    node_xyz(node, J.nx, J.ny, x0, y0, z0);
+    d.dv = 0.f;
+    d.code = -1;
+    d.b = 0.0;
+    int ox = 0, oy = 0, oz = 0;
+    if (lane < d.n) {
+        const int cell = J.nb[(long long)node * P.nmax + lane];
+        int qx, qy, qz;
+        node_xyz(cell, J.nx, J.ny, qx, qy, qz);
+        ox = qx - x0;
+        oy = qy - y0;
+        oz = qz - z0;
+        if (is_cont(J.kind)) {
+            const float m = J.kind == 1 ? J.sk_mean_f : (J.kind == 2 ? J.mean[cell] : 0.f);
+            d.dv = __fsub_rn(J.values[cell], m);
+        } else {
+            d.code = J.codes[cell];
+        }
+        d.b = cov_at(P, ox, oy, oz, J.err);
+    }
+    d.ox = ox;
+    d.oy = oy;
+    d.oz = oz;
+    d.lin = oz * P.syx + oy * P.sx + ox;
+    return d;
+}
+
+// A(lane, k) for one column k <= ... : C(x_lane - x_k) (my_kriging_weights.h:53,
+// 160), the identity beyond n.
+__device__ __forceinline__ double pair_cov(const DevJob &J, const DevPlan &P, const NodeData &d, int k, int lane) {
+    const int kx = __shfl_sync(FULL_MASK, d.ox, k), ky = __shfl_sync(FULL_MASK, d.oy, k);
+    const int kz = __shfl_sync(FULL_MASK, d.oz, k), kl = __shfl_sync(FULL_MASK, d.lin, k);
+    if (k >= d.n || lane >= d.n) return lane == k ? 1.0 : 0.0;
+    return cov_lin(P, d.ox - kx, d.oy - ky, d.oz - kz, d.lin - kl, J.err);
+}
+
+// Upper triangle A(i,k), i <= k < n, into S.A at k*LD + i (and the mirror
+// when FULL), identity padding beyond n.
+template <int LD, bool FULL>
+__device__ __forceinline__ void build_system(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeData &d,
+                                             int lane) {
+#pragma unroll 4
+    for (int k = 0; k < N32; ++k) {
+        const int kx = __shfl_sync(FULL_MASK, d.ox, k), ky = __shfl_sync(FULL_MASK, d.oy, k);
+        const int kz = __shfl_sync(FULL_MASK, d.oz, k), kl = __shfl_sync(FULL_MASK, d.lin, k);
+        if (lane <= k) {
+            double v;
+            if (k < d.n) v = cov_lin(P, d.ox - kx, d.oy - ky, d.oz - kz, d.lin - kl, J.err);
+            else v = lane == k ? 1.0 : 0.0;
+            S.A[k * LD + lane] = v;
+            if (FULL) S.A[lane * LD + k] = v;
+        }
+    }
+    __syncwarp();
+}
+
+// Outputs of one solved (or failed) system: weights w (row `lane`), status.
+__device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P, int node, int lane, const NodeData &d,
+                                              int status, double w, double variance) {
+    const long long slot = (long long)node * J.status_stride + J.status_offset;
+    const bool success = status == ST_SUCCESS;
+    const int n = d.n;
+    if (J.weights && n > 0 && lane < n) J.weights[slot * P.nmax + lane] = w;
+    if (J.variance && lane == 0) J.variance[slot] = success ? variance : -1.0;
+    if (lane == 0) J.status[slot] = (int8_t)status;
+    if (is_cont(J.kind)) {
+        if (success) {
+            // combine (combiner.h:9-24): float sum in neighbour order.
+            const float term = __double2float_rn(__dmul_rn(w, (double)d.dv));
+            float res = J.kind == 1 ? J.sk_mean_f : (J.kind == 2 ? J.mean[node] : 0.f);
+            for (int i = 0; i < n; ++i) res = __fadd_rn(res, __shfl_sync(FULL_MASK, term, i));
+            if (lane == 0) {
+                J.out_values[node] = res;
+                J.out_mask[node] = 1;
+            }
+        } else if (lane == 0) {
+            if (J.kind == 0) {
+                const int pos = atomicAdd(J.n_untouched, 1);
+                J.untouched[pos] = node;
+            } else {
+                J.out_values[node] = J.kind == 1 ? J.sk_mean_f : J.mean[node];
+                J.out_mask[node] = 1;
+            }
+        }
+    } else if (J.kind == 3) {
+        int best = 0;
+        double best_p = 0;
+        for (int k = J.k0; k < J.k1; ++k) {
+            const float pk = J.pk[k];
+            float prob = pk;
+            if (success) {
+                const float term = __double2float_rn(__dmul_rn(w, (double)__fsub_rn(d.code == k ? 1.f : 0.f, pk)));
+                for (int i = 0; i < n; ++i) prob = __fadd_rn(prob, __shfl_sync(FULL_MASK, term, i));
+            }
+            if (lane == 0) J.probs[(long long)node * J.K + k] = prob;
+            if (k == J.k0 || (double)prob > best_p) {
+                best_p = prob;
+                best = k;
+            }
+        }
+        if (J.k0 == 0 && J.k1 == J.K && lane == 0) {
+            J.out_codes[node] = (uint8_t)best;
+            J.out_mask[node] = 1;
+        }
+    } else {
+        const float m = J.median_m;
+        double prob = (double)m;
+        if (success) {
+            const double term = __dmul_rn(w, (double)__fsub_rn(d.code == 1 ? 1.f : 0.f, m));
+            for (int i = 0; i < n; ++i) prob = __dadd_rn(prob, __shfl_sync(FULL_MASK, term, i));
+        }
+        if (lane == 0) {
+            J.probs[node] = (float)prob;
+            J.out_codes[node] = ((float)prob <= 0.5f) ? 0 : 1;
+            J.out_mask[node] = 1;
+        }
+    }
+}
+
+__device__ __forceinline__ bool copy_informed(const DevJob &J, int node, int lane) {
+    if (is_cont(J.kind) && J.mask[node]) {
+        if (lane == 0) {
+            J.out_values[node] = J.values[node];
+            J.out_mask[node] = 1;
+            J.status[(long long)node * J.status_stride + J.status_offset] = ST_NOT_KRIGED;
+        }
+        return true;
+    }
+    return false;
+}
+
+// Sequential sums of the reference (SumSK, SumOnes, variance) over rows.
+__device__ __forceinline__ double seq_sum(double v, int n) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s = __dadd_rn(s, __shfl_sync(FULL_MASK, v, i));
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Exact FP64 path.
+
+// IEEE square root and reciprocal (one lane per factorisation step).
+__device__ __noinline__ double dsqrt_rn(double a) { return __dsqrt_rn(a); }
+__device__ __noinline__ double drcp_rn(double a) { return __drcp_rn(a); }
+
+// Solves and writes the outputs of one system.  Lane k gathers column k of
+// the upper triangle straight into registers.
+__device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane,
+                                             const NodeData &d) {
+    constexpr int LD = 34;
+    const int n = d.n;
+    const bool ordinary = J.kind == 0;
+    double c[N32];
+#pragma unroll
+    for (int i = 0; i < N32; ++i) {
+        // A(i, lane) = C(x_i - x_lane) for i <= lane (my_kriging_weights.h:53)
+        const int ix = __shfl_sync(FULL_MASK, d.ox, i), iy = __shfl_sync(FULL_MASK, d.oy, i);
+        const int iz = __shfl_sync(FULL_MASK, d.oz, i), il = __shfl_sync(FULL_MASK, d.lin, i);
+        c[i] = 0.0;
+        if (i <= lane && lane < n) c[i] = cov_lin(P, ix - d.ox, iy - d.oy, iz - d.oz, il - d.lin, J.err);
+    }
+    // DPOTF2 'U': column j, ajj = a_jj - sum_{i<j} a_ij^2; a_jk += -sum a_ij a_ik;
+    // a_jk *= 1/ajj.  Finished entries U(j,k) go to S.A (column k at k*34)
+    // for the broadcasts and for the transposed reads of the back substitution.
+    int info = 0;
+    double my_rcp = 0.0;  // RN(1/U(lane,lane))
+#pragma unroll
+    for (int j = 0; j < N32; ++j) {
+        if (j >= n) break;
+        double t = 0.0;
+        const double2 *cj = reinterpret_cast<const double2 *>(S.A + j * LD);
+#pragma unroll
+        for (int q = 0; q < (j + 1) / 2; ++q) {
+            const double2 u = cj[q];
+            t = __dadd_rn(t, __dmul_rn(c[2 * q], u.x));
+            if (2 * q + 1 < j) t = __dadd_rn(t, __dmul_rn(c[2 * q + 1], u.y));
+        }
+        int fail = 0;
+        double rinv = 0.0;
+        if (lane == j) {
+            double ajj = __dsub_rn(c[j], t);
+            if (!(ajj > 0.0)) {
+                fail = 1;
+            } else {
+                ajj = dsqrt_rn(ajj);
+                rinv = drcp_rn(ajj);
+            }
+            c[j] = ajj;
+            S.A[j * LD + j] = ajj;
+            my_rcp = rinv;
+        }
+        fail = __shfl_sync(FULL_MASK, fail, j);
+        if (fail) {
+            info = j + 1;
+            break;
+        }
+        rinv = __shfl_sync(FULL_MASK, rinv, j);
+        if (lane > j) {
+            double v = c[j];
+            if (j > 0) v = __dadd_rn(v, -t);
+            v = __dmul_rn(rinv, v);
+            c[j] = v;
+            S.A[lane * LD + j] = v;
+        }
+        __syncwarp();
+    }
+    double w = 0.0;
+    int status = ST_SUCCESS;
+    if (info != 0) {
+        status = ST_SINGULAR;
+    } else {
+        // DPOTRS 'U': U^T y = b (dot form, k ascending), then U x = y (column form).
+        double xa = d.b, xb = 1.0;
+#pragma unroll
+        for (int i = 0; i < N32; ++i) {
+            if (i >= n) break;
+            double ya = 0.0, yb = 0.0;
+            if (lane == i) {
+                ya = div_by_rcp(xa, c[i], my_rcp);
+                xa = ya;
+                if (ordinary) {
+                    yb = div_by_rcp(xb, c[i], my_rcp);
+                    xb = yb;
+                }
+            }
+            ya = __shfl_sync(FULL_MASK, ya, i);
+            if (ordinary) yb = __shfl_sync(FULL_MASK, yb, i);
+            if (lane > i) {
+                xa = __dsub_rn(xa, __dmul_rn(c[i], ya));
+                if (ordinary) xb = __dsub_rn(xb, __dmul_rn(c[i], yb));
+            }
+        }
+        __syncwarp();
+        for (int k = n - 1; k >= 0; --k) {
+            double va = __shfl_sync(FULL_MASK, xa, k);
+            double vb = ordinary ? __shfl_sync(FULL_MASK, xb, k) : 0.0;
+            const bool nza = va != 0.0, nzb = vb != 0.0;
+            if (lane == k) {
+                const double ukk = S.A[k * LD + k];
+                if (nza) xa = div_by_rcp(xa, ukk, my_rcp);
+                if (ordinary && nzb) xb = div_by_rcp(xb, ukk, my_rcp);
+            }
+            va = __shfl_sync(FULL_MASK, xa, k);
+            if (ordinary) vb = __shfl_sync(FULL_MASK, xb, k);
+            if (lane < k) {
+                const double u = S.A[k * LD + lane];
+                if (nza) xa = __dsub_rn(xa, __dmul_rn(va, u));
+                if (ordinary && nzb) xb = __dsub_rn(xb, __dmul_rn(vb, u));
+            }
+        }
+        if (ordinary) {
+            const double ssk = seq_sum(lane < n ? xa : 0.0, n);
+            const double son = seq_sum(lane < n ? xb : 0.0, n);
+            const double mu = __ddiv_rn(__dsub_rn(ssk, 1.0), son);
+            w = __dsub_rn(xa, __dmul_rn(mu, xb));
+        } else {
+            w = xa;
+        }
+    }
+    double variance = -1.0;
+    if (J.variance && status == ST_SUCCESS) {
+        double v = P.c0;
+        const double p = __dmul_rn(w, d.b);
+        for (int i = 0; i < n; ++i) v = __dsub_rn(v, __shfl_sync(FULL_MASK, p, i));
+        if (ordinary) v = __dsub_rn(v, __shfl_sync(FULL_MASK, w, n - 1));
+        variance = v;
+    }
+    write_outputs(J, P, node, lane, d, status, w, variance);
+}
+
+__global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPlan P, const int *list, const int *n_list) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    const long long count = list ? (long long)*n_list : J.size;
+    unsigned long long solved = 0;
+    for (long long it = (long long)blockIdx.x * WARPS32 + warp; it < count; it += (long long)gridDim.x * WARPS32) {
+        const int node = list ? list[it] : (int)it;
+        if (copy_informed(J, node, lane)) continue;
+        const NodeData d = load_node(J, P, S, node, lane);
+        if (d.n <= 0) {
+            write_outputs(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
+            continue;
+        }
+        exact_system(J, P, S, node, lane, d);
+        ++solved;
+        __syncwarp();
+    }
+    if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed path.
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// y = M v (row `lane` of M packed in m2), v broadcast through shared memory.
+__device__ __forceinline__ float apply_inverse(const float2 (&m2)[N32 / 2], float v, float *buf, int lane) {
+    buf[lane] = v;
+    __syncwarp();
+    float2 acc = f2(0.f, 0.f);
+    const float4 *b4 = reinterpret_cast<const float4 *>(buf);
+#pragma unroll
+    for (int q = 0; q < N32 / 4; ++q) {
+        const float4 u = b4[q];
+        acc = __ffma2_rn(m2[2 * q], f2(u.x, u.y), acc);
+        acc = __ffma2_rn(m2[2 * q + 1], f2(u.z, u.w), acc);
+    }
+    __syncwarp();
+    return acc.x + acc.y;
+}
+
+// r = b - A x in FP64 (row `lane`; S.A holds the full symmetric system, LD 33).
+__device__ __forceinline__ double residual(const SysSmem &S, double *vd, double x, double b, int lane) {
+    vd[lane] = x;
+    __syncwarp();
+    double acc = 0.0;
+    const double2 *x2 = reinterpret_cast<const double2 *>(vd);
+#pragma unroll
+    for (int q = 0; q < N32 / 2; ++q) {
+        const double2 u = x2[q];
+        acc = fma(S.A[(2 * q) * 33 + lane], u.x, acc);
+        acc = fma(S.A[(2 * q + 1) * 33 + lane], u.y, acc);
+    }
+    __syncwarp();
+    return b - acc;
+}
+
+template <int P_>
+__device__ __forceinline__ float get2(const float2 (&m2)[N32 / 2]) {
+    return (P_ & 1) ? m2[P_ / 2].y : m2[P_ / 2].x;
+}
+
+__global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPlan P) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    const bool ordinary = J.kind == 0;
+    const double inv_c0 = 1.0 / P.c0;
+    for (long long it = (long long)blockIdx.x * WARPS32 + warp; it < J.size; it += (long long)gridDim.x * WARPS32) {
+        const int node = (int)it;
+        if (copy_informed(J, node, lane)) continue;
+        const NodeData d = load_node(J, P, S, node, lane);
+        if (d.n <= 0) {
+            write_outputs(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
+            continue;
+        }
+        const int n = d.n;
+        build_system<33, true>(J, P, S, d, lane);
+        // Row `lane` of the unit-diagonal system A / C(0) (identity padding).
+        float2 m2[N32 / 2];
+#pragma unroll
+        for (int q = 0; q < N32 / 2; ++q)
+            m2[q] = f2((float)(S.A[(2 * q) * 33 + lane] * inv_c0), (float)(S.A[(2 * q + 1) * 33 + lane] * inv_c0));
+        // Symmetric Gauss-Jordan sweeps (the sweep operator): the matrix stays
+        // symmetric, so row p is column p and every lane publishes its own
+        // element of it; after all sweeps m holds -(A/C(0))^-1.  The pivot
+        // lane's own row update (scaling by 1/pivot) is folded into the same
+        // fused multiply-add as every other lane's elimination.
+        bool low = false;
+#pragma unroll
+        for (int p = 0; p < N32; ++p) {
+            float *rb = S.row[p & 1];
+            const float mp = (p & 1) ? m2[p / 2].y : m2[p / 2].x;
+            rb[lane] = mp;
+            __syncwarp();
+            const float piv = rb[p];
+            low |= !(piv > MIXED_PIVOT_MIN);
+            const float dinv = __frcp_rn(piv);
+            const float isp = lane == p ? 1.f : 0.f;
+            const float g = (mp - isp) * dinv;
+            const float2 ng = f2(-g, -g);
+            const float4 *r4 = reinterpret_cast<const float4 *>(rb);
+#pragma unroll
+            for (int q = 0; q < N32 / 4; ++q) {
+                const float4 u = r4[q];
+                m2[2 * q] = __ffma2_rn(ng, f2(u.x, u.y), m2[2 * q]);
+                m2[2 * q + 1] = __ffma2_rn(ng, f2(u.z, u.w), m2[2 * q + 1]);
+            }
+            if (p & 1) m2[p / 2].y = g - isp;
+            else m2[p / 2].x = g - isp;
+        }
+        if (__any_sync(FULL_MASK, low)) {
+            if (lane == 0) {
+                const int pos = atomicAdd(J.n_routed, 1);
+                J.routed[pos] = node;
+            }
+            __syncwarp();
+            continue;
+        }
+        // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
+        // refined with FP64 residuals.
+        const double sc = -inv_c0;
+        double xa = (double)apply_inverse(m2, (float)d.b, S.vf[0], lane) * sc;
+        double xb = ordinary ? (double)apply_inverse(m2, lane < n ? 1.f : 0.f, S.vf[1], lane) * sc : 0.0;
+        const double ba = d.b, bb = lane < n ? 1.0 : 0.0;
+        bool converged = false;
+        for (int corr = 0; corr < MIXED_MAX_CORR; ++corr) {
+            const double ra = residual(S, S.vd, xa, ba, lane);
+            const double da = (double)apply_inverse(m2, (float)ra, S.vf[0], lane) * sc;
+            xa += da;
+            double dmax = fabs(da), xmax = fabs(xa);
+            if (ordinary) {
+                const double rbv = residual(S, S.vd, xb, bb, lane);
+                const double db = (double)apply_inverse(m2, (float)rbv, S.vf[1], lane) * sc;
+                xb += db;
+                dmax = fmax(dmax, fabs(db));
+                xmax = fmax(xmax, fabs(xb));
+            }
+            dmax = warp_max(dmax);
+            xmax = warp_max(xmax);
+            if (dmax <= (corr == 0 ? MIXED_ACCEPT_1 : MIXED_ACCEPT_N) * xmax) {
+                converged = true;
+                break;
+            }
+        }
+        if (!converged) {
+            if (lane == 0) {
+                const int pos = atomicAdd(J.n_routed, 1);
+                J.routed[pos] = node;
+            }
+            __syncwarp();
+            continue;
+        }
+        if (lane >= n) {
+            xa = 0.0;
+            xb = 0.0;
+        }
+        double w;
+        if (ordinary) {
+            const double mu = (warp_sum(xa) - 1.0) / warp_sum(xb);
+            w = xa - mu * xb;
+        } else {
+            w = xa;
+        }
+        double variance = -1.0;
+        if (J.variance) {
+            variance = P.c0 - warp_sum(w * d.b);
+            if (ordinary) variance -= __shfl_sync(FULL_MASK, w, n - 1);
+        }
+        write_outputs(J, P, node, lane, d, ST_SUCCESS, w, variance);
+        __syncwarp();
+    }
+}
+
+constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
+
+int grid_for(const void *fn, int threads) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM32);
+    int per_sm = 0, dev = 0, sms = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, SMEM32);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (per_sm < 1 ? 1 : per_sm) * sms;
+}
+
+}  // namespace
+
+void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
+                    long long n_max, cudaStream_t s) {
+    if (n_max <= 0) return;
+    if (precision == 0 || node_list) {
+        static int grid = 0;
+        if (!grid) grid = grid_for((const void *)k_solve_exact32, WARPS32 * 32);
+        long long blocks = (n_max + WARPS32 - 1) / WARPS32;
+        if (blocks > grid) blocks = grid;
+        k_solve_exact32<<<(unsigned)blocks, WARPS32 * 32, SMEM32, s>>>(J, P, node_list, n_list);
+    } else {
+        static int grid = 0;
+        if (!grid) grid = grid_for((const void *)k_solve_mixed32, WARPS32 * 32);
+        long long blocks = (n_max + WARPS32 - 1) / WARPS32;
+        if (blocks > grid) blocks = grid;
+        k_solve_mixed32<<<(unsigned)blocks, WARPS32 * 32, SMEM32, s>>>(J, P);
+    }
+}
+
+}  // namespace hpgl_b200
