@@ -278,6 +278,50 @@ int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl
     });
 }
 
+hpgl_b200_server_t *hpgl_b200_server_create(const hpgl_b200_server_config_t *config) {
+    void *h = nullptr;
+    guarded("hpgl_b200_server_create", [&] {
+        if (!config) throw HpglError{HPGL_E_INVALID, "config is null"};
+        h = server_create(*config);
+    });
+    return (hpgl_b200_server_t *)h;
+}
+
+long long hpgl_b200_server_submit(hpgl_b200_server_t *server, const hpgl_b200_job_t *job,
+                                  hpgl_b200_result_t *result) {
+    long long t = -1;
+    int rc = guarded("hpgl_b200_server_submit", [&] {
+        if (!server || !job) throw HpglError{HPGL_E_INVALID, "null argument"};
+        t = server_submit(server, *job, result);
+    });
+    return rc == HPGL_OK ? t : -(long long)rc;
+}
+
+int hpgl_b200_server_wait(hpgl_b200_server_t *server, long long ticket, int timeout_ms) {
+    int code = -1;
+    std::string msg;
+    int rc = guarded("hpgl_b200_server_wait", [&] {
+        if (!server) throw HpglError{HPGL_E_INVALID, "null server"};
+        code = server_wait(server, ticket, timeout_ms, msg);
+    });
+    if (rc != HPGL_OK) return rc;
+    if (code > 0) set_error(code, "hpgl_b200_server job " + std::to_string(ticket) + ": " + msg);
+    return code;
+}
+
+int hpgl_b200_server_stats(hpgl_b200_server_t *server, hpgl_b200_server_stats_t *stats) {
+    return guarded("hpgl_b200_server_stats", [&] {
+        if (!server || !stats) throw HpglError{HPGL_E_INVALID, "null argument"};
+        server_stats(server, *stats);
+    });
+}
+
+void hpgl_b200_server_destroy(hpgl_b200_server_t *server) {
+    guarded("hpgl_b200_server_destroy", [&] {
+        if (server) server_destroy(server);
+    });
+}
+
 const char *hpgl_b200_version(void) { return "hpgl_b200 0.1 (sm_100a kriging path)"; }
 
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y, float *neighbours_z,

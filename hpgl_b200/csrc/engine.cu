@@ -1,14 +1,24 @@
-// Job execution on the GPU.  One CUDA stream, device buffers cached and grown
-// across calls; every call is synchronous at the C ABI.
+// Job execution on the GPU.
+//
+// Every job gets one device arena holding its inputs, plan (template,
+// covariance table, clusterizer buckets, informed-bit rows), neighbour lists,
+// scratch and outputs.  The synchronous C-ABI calls run on one stream with a
+// cached, grow-only arena; the server (server section below) runs several jobs
+// at once, each on its own stream with an arena from the stream-ordered pool
+// (cudaMallocAsync), admitted against an HBM budget.
 #include <algorithm>
 #include <chrono>
 #include <climits>
-#include <functional>
+#include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
+#include <thread>
 
 #include "engine.h"
 #include "kernels.cuh"
@@ -31,25 +41,30 @@ static int g_precision = env_precision();
 int default_precision() { return g_precision; }
 void set_default_precision(int p) { g_precision = p; }
 
-template <typename T>
-struct DBuf {
-    T *p = nullptr;
-    size_t cap = 0;
-    void ensure(size_t n) {
-        if (n == 0) n = 1;
-        if (n <= cap) return;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        CUDA_CHECK(cudaMalloc(&p, n * sizeof(T)));
-        cap = n;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
+static double ms_since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
+static void ensure_device() {
+    static const cudaError_t probe = [] {
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e == cudaSuccess && n == 0) e = cudaErrorNoDevice;
+        return e;
+    }();
+    if (probe != cudaSuccess)
+        throw HpglError{HPGL_E_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(probe)};
+}
+
+static int sm_count_host() {
+    static const int n = [] {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        return sms > 0 ? sms : 148;
+    }();
+    return n;
+}
 
 struct Counters {
     int n_untouched;
@@ -59,73 +74,39 @@ struct Counters {
     unsigned long long n_fp64;
 };
 
-struct PlanBuffers {
-    DBuf<int4> tmpl;
-    DBuf<double> table;
-    DBuf<int> bucket_start, bucket_nodes;
-    DBuf<uint8_t> bucket_clean;
-    DBuf<uint32_t> bits;
-    ~PlanBuffers() {
-        tmpl.release();
-        table.release();
-        bucket_start.release();
-        bucket_nodes.release();
-        bucket_clean.release();
-        bits.release();
-    }
-};
-
-struct Context {
-    cudaStream_t stream = nullptr;
-    DBuf<float> values, mean, out_values, probs, pk;
-    DBuf<uint8_t> codes, mask, out_codes, out_mask;
-    DBuf<int8_t> status;
-    DBuf<double> variance, weights, skey;
-    DBuf<int> nb, nbcount, untouched, routed, sidx;
-    DBuf<Counters> counters;
-    DBuf<char> flush;
-};
-
-static std::mutex g_mutex;
-
-static Context &ctx() {
-    static Context *c = nullptr;
-    if (!c) {
-        int n = 0;
-        cudaError_t e = cudaGetDeviceCount(&n);
-        if (e != cudaSuccess || n == 0)
-            throw HpglError{HPGL_E_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e)};
-        auto *nc = new Context();
-        CUDA_CHECK(cudaStreamCreateWithFlags(&nc->stream, cudaStreamNonBlocking));
-        c = nc;
-    }
-    return *c;
-}
-
-static double ms_since(std::chrono::steady_clock::time_point t) {
-    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
-}
-
-// ---- job state -------------------------------------------------------------
+// ---- job state ---------------------------------------------------------------
 
 struct Group {
     int k0, k1;
     Plan plan;
-    std::unique_ptr<PlanBuffers> buf;
+    std::vector<int4> tmpl_dev;  // device form of the template
     DevPlan dp;
+    // arena offsets
+    size_t o_tmpl, o_table, o_bstart, o_bnodes, o_bclean, o_bits;
+};
+
+struct Arena {
+    size_t o_values, o_codes, o_mask, o_mean, o_out_values, o_out_codes, o_out_mask, o_probs, o_pk, o_status,
+        o_variance, o_weights, o_nb, o_nbcount, o_untouched, o_routed, o_counters, o_skey, o_sidx;
+    size_t total;
+    long long cluster_warps;
 };
 
 struct JobState {
     hpgl_b200_job_t job;
     int precision;
     long long size;
-    int K;            // categories (IK), else 1
+    int K;
     bool per_category;
     int status_stride;
     std::vector<Group> groups;
     std::vector<float> pk;
     double sk_mean;
     int nmax_all;
+    bool want_variance, want_weights;
+    long long kriged;
+    Arena ar;
+    char *base = nullptr;
 };
 
 static KrigingParams to_params(const hpgl_ik_params_t &p) {
@@ -145,7 +126,17 @@ static KrigingParams to_params(const hpgl_ik_params_t &p) {
 
 static void invalid(const std::string &m) { throw HpglError{HPGL_E_INVALID, m}; }
 
-static void prepare(JobState &S, const hpgl_b200_job_t &job) {
+static void check_result(const JobState &S, const hpgl_b200_result_t &res) {
+    if (S.job.kind <= KIND_LVM && !res.out_values) invalid("out_values is null");
+    if (S.job.kind > KIND_LVM && !res.out_codes) invalid("out_codes is null");
+    if (!res.out_mask) invalid("out_mask is null");
+    if ((res.nb_index || res.weights) && res.nb_stride < S.nmax_all) invalid("nb_stride smaller than max_neighbours");
+}
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Host planning and arena layout (no device work).
+static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_result_t &res) {
     S.job = job;
     if (job.kind < 0 || job.kind > 4) invalid("unknown kriging kind");
     if (job.nx <= 0 || job.ny <= 0 || job.nz <= 0) invalid("grid dimensions must be positive");
@@ -191,6 +182,7 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job) {
     } catch (const std::invalid_argument &e) {
         throw HpglError{HPGL_E_INVALID, e.what()};
     }
+    check_result(S, res);
     // The reference keeps marginal probabilities as float (ik_params.h:41,
     // mean_provider.cpp:8-13) and hands every mean to the combiner as float.
     S.pk.resize(S.K);
@@ -198,111 +190,137 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job) {
     S.sk_mean = 0;
     if (job.kind == KIND_SK)
         S.sk_mean = job.sk_automatic_mean ? informed_mean(job.values, job.mask, S.size) : job.sk_mean;
+    S.want_variance = res.variance != nullptr;
+    S.want_weights = res.weights != nullptr;
+    S.kriged = 0;
+    if (cont) {
+        for (long long i = 0; i < S.size; ++i) S.kriged += job.mask[i] == 0;
+    } else {
+        S.kriged = S.size;
+    }
+
+    // arena layout
+    const size_t n = (size_t)S.size, slots = n * S.status_stride;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += align_up(bytes ? bytes : 1);
+        return o;
+    };
+    Arena &A = S.ar;
+    A.o_mask = take(n);
+    A.o_values = cont ? take(n * 4) : 0;
+    A.o_codes = cont ? 0 : take(n);
+    A.o_mean = job.kind == KIND_LVM ? take(n * 4) : 0;
+    A.o_out_values = cont ? take(n * 4) : 0;
+    A.o_out_codes = cont ? 0 : take(n);
+    A.o_out_mask = take(n);
+    A.o_probs = cont ? 0 : take(n * S.K * 4);
+    A.o_pk = take(S.K * 4);
+    A.o_status = take(slots);
+    A.o_variance = S.want_variance ? take(slots * 8) : 0;
+    A.o_weights = S.want_weights ? take(slots * S.nmax_all * 8) : 0;
+    A.o_nb = take(n * (size_t)S.nmax_all * 4);
+    A.o_nbcount = take(n * 4);
+    A.o_untouched = take(n * 4);
+    A.o_routed = take(n * 4);
+    A.o_counters = take(sizeof(Counters));
+    int max_cand = 1;
+    bool any_clean = false;
+    for (auto &g : S.groups) {
+        const Plan &P = g.plan;
+        g.tmpl_dev.resize(P.tmpl.size());
+        for (size_t i = 0; i < P.tmpl.size(); ++i)
+            g.tmpl_dev[i] = make_int4(P.px + P.tmpl[i].dx, P.tmpl[i].dy, P.tmpl[i].dz, P.tmpl[i].delta);
+        g.o_tmpl = take(g.tmpl_dev.size() * sizeof(int4));
+        g.o_table = take(P.table.size() * 8);
+        g.o_bstart = take(P.bucket_start.size() * 4);
+        g.o_bnodes = take(P.bucket_nodes.size() * 4);
+        g.o_bclean = take(P.bucket_clean.size());
+        g.o_bits = take(((size_t)P.wpr * P.ny * P.nz + 2) * 4);
+        if (P.any_clean) {
+            any_clean = true;
+            max_cand = std::max(max_cand, P.max_candidates);
+        }
+    }
+    A.cluster_warps = 0;
+    if (any_clean) {
+        A.cluster_warps = std::min<long long>((long long)sm_count_host() * 32, (S.size + 31) / 32 * 32);
+        A.o_skey = take((size_t)A.cluster_warps * max_cand * 8);
+        A.o_sidx = take((size_t)A.cluster_warps * max_cand * 4);
+    } else {
+        A.o_skey = A.o_sidx = 0;
+    }
+    A.total = off;
 }
 
-static void upload_plan(Group &g, cudaStream_t s) {
-    const Plan &P = g.plan;
-    g.buf.reset(new PlanBuffers());
-    PlanBuffers &B = *g.buf;
-    std::vector<int4> t(P.tmpl.size());
-    for (size_t i = 0; i < t.size(); ++i)
-        t[i] = make_int4(P.px + P.tmpl[i].dx, P.tmpl[i].dy, P.tmpl[i].dz, P.tmpl[i].delta);
-    B.tmpl.ensure(t.size());
-    B.table.ensure(P.table.size());
-    B.bucket_start.ensure(P.bucket_start.size());
-    B.bucket_nodes.ensure(P.bucket_nodes.size());
-    B.bucket_clean.ensure(P.bucket_clean.size());
-    B.bits.ensure((size_t)P.wpr * P.ny * P.nz + 2);
-    if (!t.empty()) CUDA_CHECK(cudaMemcpyAsync(B.tmpl.p, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
-    CUDA_CHECK(cudaMemcpyAsync(B.table.p, P.table.data(), P.table.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    CUDA_CHECK(cudaMemcpyAsync(B.bucket_start.p, P.bucket_start.data(), P.bucket_start.size() * sizeof(int),
-                               cudaMemcpyHostToDevice, s));
-    if (!P.bucket_nodes.empty())
-        CUDA_CHECK(cudaMemcpyAsync(B.bucket_nodes.p, P.bucket_nodes.data(), P.bucket_nodes.size() * sizeof(int),
-                                   cudaMemcpyHostToDevice, s));
-    CUDA_CHECK(cudaMemcpyAsync(B.bucket_clean.p, P.bucket_clean.data(), P.bucket_clean.size(), cudaMemcpyHostToDevice, s));
-    DevPlan &d = g.dp;
-    d.nmax = P.nmax;
-    d.tmpl = B.tmpl.p;
-    d.tmpl_len = (int)P.tmpl.size();
-    d.px = P.px;
-    d.nseg = P.nseg;
-    d.wpr = P.wpr;
-    d.table = B.table.p;
-    d.Bx = P.B[0];
-    d.By = P.B[1];
-    d.Bz = P.B[2];
-    d.Tx = std::min(P.trunc[0], P.B[0]);
-    d.Ty = std::min(P.trunc[1], P.B[1]);
-    d.Tz = std::min(P.trunc[2], P.B[2]);
-    d.sx = 2 * P.B[0] + 1;
-    d.syx = d.sx * (2 * P.B[1] + 1);
-    d.center = P.B[2] * d.syx + P.B[1] * d.sx + P.B[0];
-    d.truncated = P.truncated ? 1 : 0;
-    d.c0 = P.c0;
-    d.bucket_start = B.bucket_start.p;
-    d.bucket_nodes = B.bucket_nodes.p;
-    d.bucket_clean = B.bucket_clean.p;
-    d.crx = P.cl_r[0];
-    d.cry = P.cl_r[1];
-    d.crz = P.cl_r[2];
-    d.mx = P.mx;
-    d.my = P.my;
-    d.mz = P.mz;
-    d.max_candidates = std::max(1, P.max_candidates);
+template <typename T>
+static T *at(const JobState &S, size_t off) {
+    return reinterpret_cast<T *>(S.base + off);
 }
 
-static void upload_inputs(JobState &S, Context &C, const hpgl_b200_result_t *res) {
-    cudaStream_t s = C.stream;
+static void upload(JobState &S, cudaStream_t s) {
     const hpgl_b200_job_t &job = S.job;
     const size_t n = (size_t)S.size;
-    C.mask.ensure(n);
-    CUDA_CHECK(cudaMemcpyAsync(C.mask.p, job.mask, n, cudaMemcpyHostToDevice, s));
-    if (job.kind <= KIND_LVM) {
-        C.values.ensure(n);
-        CUDA_CHECK(cudaMemcpyAsync(C.values.p, job.values, n * sizeof(float), cudaMemcpyHostToDevice, s));
-        C.out_values.ensure(n);
-    } else {
-        C.codes.ensure(n);
-        CUDA_CHECK(cudaMemcpyAsync(C.codes.p, job.codes, n, cudaMemcpyHostToDevice, s));
-        C.out_codes.ensure(n);
-        C.probs.ensure(n * S.K);
-    }
-    if (job.kind == KIND_LVM) {
-        C.mean.ensure(n);
-        CUDA_CHECK(cudaMemcpyAsync(C.mean.p, job.mean, n * sizeof(float), cudaMemcpyHostToDevice, s));
-    }
-    C.out_mask.ensure(n);
-    C.status.ensure(n * S.status_stride);
-    C.nb.ensure(n * (size_t)S.nmax_all);
-    C.nbcount.ensure(n);
-    C.untouched.ensure(n);
-    C.routed.ensure(n);
-    C.counters.ensure(1);
-    C.pk.ensure(S.K);
-    CUDA_CHECK(cudaMemcpyAsync(C.pk.p, S.pk.data(), S.K * sizeof(float), cudaMemcpyHostToDevice, s));
-    if (res && res->variance) C.variance.ensure(n * S.status_stride);
-    if (res && res->weights) C.weights.ensure(n * S.status_stride * (size_t)S.nmax_all);
-    int max_cand = 1;
+    const Arena &A = S.ar;
+    CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_mask), job.mask, n, cudaMemcpyHostToDevice, s));
+    if (job.kind <= KIND_LVM)
+        CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_values), job.values, n * 4, cudaMemcpyHostToDevice, s));
+    else
+        CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_codes), job.codes, n, cudaMemcpyHostToDevice, s));
+    if (job.kind == KIND_LVM)
+        CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_mean), job.mean, n * 4, cudaMemcpyHostToDevice, s));
+    CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_pk), S.pk.data(), S.K * 4, cudaMemcpyHostToDevice, s));
     for (auto &g : S.groups) {
-        upload_plan(g, s);
-        if (g.plan.any_clean) max_cand = std::max(max_cand, g.plan.max_candidates);
-    }
-    // clusterizer scratch: one candidate list per resident warp
-    bool any_clean = false;
-    for (auto &g : S.groups) any_clean |= g.plan.any_clean;
-    if (any_clean) {
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        long long warps = std::min<long long>((long long)sms * 32, (S.size + 31) / 32 * 32);
-        C.skey.ensure((size_t)warps * max_cand);
-        C.sidx.ensure((size_t)warps * max_cand);
+        const Plan &P = g.plan;
+        if (!g.tmpl_dev.empty())
+            CUDA_CHECK(cudaMemcpyAsync(at<int4>(S, g.o_tmpl), g.tmpl_dev.data(), g.tmpl_dev.size() * sizeof(int4),
+                                       cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(at<double>(S, g.o_table), P.table.data(), P.table.size() * 8,
+                                   cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(at<int>(S, g.o_bstart), P.bucket_start.data(), P.bucket_start.size() * 4,
+                                   cudaMemcpyHostToDevice, s));
+        if (!P.bucket_nodes.empty())
+            CUDA_CHECK(cudaMemcpyAsync(at<int>(S, g.o_bnodes), P.bucket_nodes.data(), P.bucket_nodes.size() * 4,
+                                       cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, g.o_bclean), P.bucket_clean.data(), P.bucket_clean.size(),
+                                   cudaMemcpyHostToDevice, s));
+        DevPlan &d = g.dp;
+        d.nmax = P.nmax;
+        d.tmpl = at<int4>(S, g.o_tmpl);
+        d.tmpl_len = (int)P.tmpl.size();
+        d.px = P.px;
+        d.nseg = P.nseg;
+        d.wpr = P.wpr;
+        d.table = at<double>(S, g.o_table);
+        d.Bx = P.B[0];
+        d.By = P.B[1];
+        d.Bz = P.B[2];
+        d.Tx = std::min(P.trunc[0], P.B[0]);
+        d.Ty = std::min(P.trunc[1], P.B[1]);
+        d.Tz = std::min(P.trunc[2], P.B[2]);
+        d.sx = 2 * P.B[0] + 1;
+        d.syx = d.sx * (2 * P.B[1] + 1);
+        d.center = P.B[2] * d.syx + P.B[1] * d.sx + P.B[0];
+        d.truncated = P.truncated ? 1 : 0;
+        d.c0 = P.c0;
+        d.bucket_start = at<int>(S, g.o_bstart);
+        d.bucket_nodes = at<int>(S, g.o_bnodes);
+        d.bucket_clean = at<uint8_t>(S, g.o_bclean);
+        d.crx = P.cl_r[0];
+        d.cry = P.cl_r[1];
+        d.crz = P.cl_r[2];
+        d.mx = P.mx;
+        d.my = P.my;
+        d.mz = P.mz;
+        d.max_candidates = std::max(1, P.max_candidates);
     }
 }
 
-static DevJob make_devjob(JobState &S, Context &C, const Group &g, const hpgl_b200_result_t *res) {
+static DevJob make_devjob(const JobState &S, const Group &g) {
     const hpgl_b200_job_t &job = S.job;
+    const Arena &A = S.ar;
+    const bool cont = job.kind <= KIND_LVM;
     DevJob J;
     memset(&J, 0, sizeof(J));
     J.kind = job.kind;
@@ -310,34 +328,35 @@ static DevJob make_devjob(JobState &S, Context &C, const Group &g, const hpgl_b2
     J.ny = job.ny;
     J.nz = job.nz;
     J.size = S.size;
-    J.values = job.kind <= KIND_LVM ? C.values.p : nullptr;
-    J.codes = job.kind <= KIND_LVM ? nullptr : C.codes.p;
-    J.mask = C.mask.p;
-    J.mean = job.kind == KIND_LVM ? C.mean.p : nullptr;
-    J.bits = g.buf->bits.p;
+    J.values = cont ? at<float>(S, A.o_values) : nullptr;
+    J.codes = cont ? nullptr : at<uint8_t>(S, A.o_codes);
+    J.mask = at<uint8_t>(S, A.o_mask);
+    J.mean = job.kind == KIND_LVM ? at<float>(S, A.o_mean) : nullptr;
+    J.bits = at<uint32_t>(S, g.o_bits);
     J.K = S.K;
     J.k0 = g.k0;
     J.k1 = g.k1;
-    J.pk = C.pk.p;
+    J.pk = at<float>(S, A.o_pk);
     J.sk_mean_f = (float)S.sk_mean;
     J.median_m = (float)job.median_marginal1;
-    J.nb = C.nb.p;
-    J.nbcount = C.nbcount.p;
-    J.out_values = job.kind <= KIND_LVM ? C.out_values.p : nullptr;
-    J.out_codes = job.kind <= KIND_LVM ? nullptr : C.out_codes.p;
-    J.out_mask = C.out_mask.p;
-    J.variance = (res && res->variance) ? C.variance.p : nullptr;
-    J.status = C.status.p;
-    J.probs = job.kind <= KIND_LVM ? nullptr : C.probs.p;
-    J.weights = (res && res->weights) ? C.weights.p : nullptr;
+    J.nb = at<int>(S, A.o_nb);
+    J.nbcount = at<int>(S, A.o_nbcount);
+    J.out_values = cont ? at<float>(S, A.o_out_values) : nullptr;
+    J.out_codes = cont ? nullptr : at<uint8_t>(S, A.o_out_codes);
+    J.out_mask = at<uint8_t>(S, A.o_out_mask);
+    J.variance = S.want_variance ? at<double>(S, A.o_variance) : nullptr;
+    J.status = at<int8_t>(S, A.o_status);
+    J.probs = cont ? nullptr : at<float>(S, A.o_probs);
+    J.weights = S.want_weights ? at<double>(S, A.o_weights) : nullptr;
     J.status_stride = S.status_stride;
     J.status_offset = S.per_category ? g.k0 : 0;
-    J.untouched = C.untouched.p;
-    J.n_untouched = &C.counters.p->n_untouched;
-    J.routed = C.routed.p;
-    J.n_routed = &C.counters.p->n_routed;
-    J.n_fp64 = &C.counters.p->n_fp64;
-    J.err = &C.counters.p->err;
+    Counters *cnt = at<Counters>(S, A.o_counters);
+    J.untouched = at<int>(S, A.o_untouched);
+    J.n_untouched = &cnt->n_untouched;
+    J.routed = at<int>(S, A.o_routed);
+    J.n_routed = &cnt->n_routed;
+    J.n_fp64 = &cnt->n_fp64;
+    J.err = &cnt->err;
     return J;
 }
 
@@ -347,25 +366,21 @@ struct PassTiming {
 };
 
 // One device pass over all groups: bits, searches, solve(s), argmax.
-static void device_pass(JobState &S, Context &C, const hpgl_b200_result_t *res, PassTiming *pt,
+static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
                         const std::function<void(const Group &)> &after_group) {
-    cudaStream_t s = C.stream;
-    CUDA_CHECK(cudaMemsetAsync(C.counters.p, 0, sizeof(Counters), s));
+    const Arena &A = S.ar;
+    Counters *cnt = at<Counters>(S, A.o_counters);
+    CUDA_CHECK(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
     int launches = 0;
     for (size_t gi = 0; gi < S.groups.size(); ++gi) {
         Group &g = S.groups[gi];
-        DevJob J = make_devjob(S, C, g, res);
-        CUDA_CHECK(cudaMemsetAsync(C.nbcount.p, 0, (size_t)S.size * sizeof(int), s));
-        launch_build_bits(J, g.dp, g.buf->bits.p, s);
+        DevJob J = make_devjob(S, g);
+        CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
+        launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
         launch_search_template(J, g.dp, s);
         launches += 2;
         if (g.plan.any_clean) {
-            long long warps = C.skey.cap / g.dp.max_candidates;
-            int dev = 0, sms = 148;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            warps = std::min<long long>(warps, (long long)sms * 32);
-            launch_search_cluster(J, g.dp, C.skey.p, C.sidx.p, (int)std::max<long long>(1, warps), s);
+            launch_search_cluster(J, g.dp, at<double>(S, A.o_skey), at<int>(S, A.o_sidx), (int)A.cluster_warps, s);
             ++launches;
         }
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top0, s));
@@ -373,16 +388,16 @@ static void device_pass(JobState &S, Context &C, const hpgl_b200_result_t *res, 
         ++launches;
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top1, s));
         if (S.precision == HPGL_PRECISION_MIXED) {
-            launch_solve(J, g.dp, HPGL_PRECISION_FP64, C.routed.p, J.n_routed, (int)S.size, s);
+            launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, J.n_routed, (int)S.size, s);
             ++launches;
         }
         CUDA_CHECK(cudaGetLastError());
         if (after_group) after_group(g);
         if (S.precision == HPGL_PRECISION_MIXED && gi + 1 < S.groups.size())
-            CUDA_CHECK(cudaMemsetAsync(&C.counters.p->n_routed, 0, sizeof(int), s));
+            CUDA_CHECK(cudaMemsetAsync(&cnt->n_routed, 0, sizeof(int), s));
     }
     if (S.per_category) {
-        DevJob J = make_devjob(S, C, S.groups[0], res);
+        DevJob J = make_devjob(S, S.groups[0]);
         launch_ik_argmax(J, s);
         ++launches;
     }
@@ -390,9 +405,31 @@ static void device_pass(JobState &S, Context &C, const hpgl_b200_result_t *res, 
     if (pt) pt->launches = launches;
 }
 
-static void download(JobState &S, Context &C, hpgl_b200_result_t &res, const Counters &cnt) {
-    cudaStream_t s = C.stream;
+// Neighbour lists of the group just searched, into slot node*stride + offset.
+static void download_neighbours(const JobState &S, const Group &g, hpgl_b200_result_t &res, cudaStream_t s) {
+    const size_t n = (size_t)S.size;
+    const int off = S.per_category ? g.k0 : 0;
+    if (res.nb_count)
+        CUDA_CHECK(cudaMemcpy2DAsync(res.nb_count + off, (size_t)S.status_stride * sizeof(int),
+                                     at<int>(S, S.ar.o_nbcount), sizeof(int), sizeof(int), n, cudaMemcpyDeviceToHost,
+                                     s));
+    if (res.nb_index)
+        CUDA_CHECK(cudaMemcpy2DAsync(res.nb_index + (size_t)off * res.nb_stride,
+                                     (size_t)S.status_stride * res.nb_stride * sizeof(int), at<int>(S, S.ar.o_nb),
+                                     (size_t)g.plan.nmax * sizeof(int), (size_t)g.plan.nmax * sizeof(int), n,
+                                     cudaMemcpyDeviceToHost, s));
+}
+
+static Counters read_counters(const JobState &S, cudaStream_t s) {
+    Counters c;
+    CUDA_CHECK(cudaMemcpyAsync(&c, at<Counters>(S, S.ar.o_counters), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    return c;
+}
+
+static void download(const JobState &S, hpgl_b200_result_t &res, const Counters &cnt, cudaStream_t s) {
     const hpgl_b200_job_t &job = S.job;
+    const Arena &A = S.ar;
     const size_t n = (size_t)S.size;
     if (cnt.err)
         throw HpglError{HPGL_E_INTERNAL, "device invariant violated (error bits " + std::to_string(cnt.err) + ")"};
@@ -401,7 +438,8 @@ static void download(JobState &S, Context &C, hpgl_b200_result_t &res, const Cou
     std::vector<float> saved_v(cnt.n_untouched);
     std::vector<uint8_t> saved_m(cnt.n_untouched);
     if (cnt.n_untouched > 0) {
-        CUDA_CHECK(cudaMemcpyAsync(untouched.data(), C.untouched.p, cnt.n_untouched * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(untouched.data(), at<int>(S, A.o_untouched), cnt.n_untouched * sizeof(int),
+                                   cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
         for (int i = 0; i < cnt.n_untouched; ++i) {
             saved_v[i] = res.out_values[untouched[i]];
@@ -409,59 +447,73 @@ static void download(JobState &S, Context &C, hpgl_b200_result_t &res, const Cou
         }
     }
     if (job.kind <= KIND_LVM)
-        CUDA_CHECK(cudaMemcpyAsync(res.out_values, C.out_values.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, A.o_out_values), n * 4, cudaMemcpyDeviceToHost, s));
     else
-        CUDA_CHECK(cudaMemcpyAsync(res.out_codes, C.out_codes.p, n, cudaMemcpyDeviceToHost, s));
-    CUDA_CHECK(cudaMemcpyAsync(res.out_mask, C.out_mask.p, n, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(res.out_codes, at<uint8_t>(S, A.o_out_codes), n, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaMemcpyAsync(res.out_mask, at<uint8_t>(S, A.o_out_mask), n, cudaMemcpyDeviceToHost, s));
     const size_t slots = n * S.status_stride;
-    if (res.status) CUDA_CHECK(cudaMemcpyAsync(res.status, C.status.p, slots, cudaMemcpyDeviceToHost, s));
-    if (res.variance) CUDA_CHECK(cudaMemcpyAsync(res.variance, C.variance.p, slots * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res.status) CUDA_CHECK(cudaMemcpyAsync(res.status, at<int8_t>(S, A.o_status), slots, cudaMemcpyDeviceToHost, s));
+    if (res.variance)
+        CUDA_CHECK(cudaMemcpyAsync(res.variance, at<double>(S, A.o_variance), slots * 8, cudaMemcpyDeviceToHost, s));
     if (res.probs && job.kind >= KIND_IK)
-        CUDA_CHECK(cudaMemcpyAsync(res.probs, C.probs.p, n * (job.kind == KIND_IK ? S.K : 1) * sizeof(float),
+        CUDA_CHECK(cudaMemcpyAsync(res.probs, at<float>(S, A.o_probs), n * (job.kind == KIND_IK ? S.K : 1) * 4,
                                    cudaMemcpyDeviceToHost, s));
     if (res.weights)
-        CUDA_CHECK(cudaMemcpy2DAsync(res.weights, (size_t)res.nb_stride * sizeof(double), C.weights.p,
-                                     (size_t)S.nmax_all * sizeof(double), (size_t)S.nmax_all * sizeof(double), slots,
-                                     cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpy2DAsync(res.weights, (size_t)res.nb_stride * 8, at<double>(S, A.o_weights),
+                                     (size_t)S.nmax_all * 8, (size_t)S.nmax_all * 8, slots, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     for (int i = 0; i < cnt.n_untouched; ++i) {
         res.out_values[untouched[i]] = saved_v[i];
         res.out_mask[untouched[i]] = saved_m[i];
     }
+    res.systems = S.kriged * (long long)S.groups.size();
+    res.systems_fp64 = (long long)cnt.n_fp64;
+    res.failures = 0;
 }
 
-// Neighbour lists of the group just searched, into slot node*stride + offset.
-static void download_neighbours(JobState &S, Context &C, const Group &g, hpgl_b200_result_t &res) {
-    cudaStream_t s = C.stream;
-    const size_t n = (size_t)S.size;
-    const int off = S.per_category ? g.k0 : 0;
-    if (res.nb_count)
-        CUDA_CHECK(cudaMemcpy2DAsync(res.nb_count + off, (size_t)S.status_stride * sizeof(int), C.nbcount.p, sizeof(int),
-                                     sizeof(int), n, cudaMemcpyDeviceToHost, s));
-    if (res.nb_index)
-        CUDA_CHECK(cudaMemcpy2DAsync(res.nb_index + (size_t)off * res.nb_stride,
-                                     (size_t)S.status_stride * res.nb_stride * sizeof(int), C.nb.p,
-                                     (size_t)g.plan.nmax * sizeof(int), (size_t)g.plan.nmax * sizeof(int), n,
-                                     cudaMemcpyDeviceToHost, s));
+// ---- synchronous calls ---------------------------------------------------------
+
+struct SyncContext {
+    cudaStream_t stream = nullptr;
+    char *arena = nullptr;
+    size_t cap = 0;
+    char *flush = nullptr;
+    size_t flush_cap = 0;
+};
+
+static std::mutex g_sync_mutex;
+
+static SyncContext &sync_ctx() {
+    static SyncContext *c = nullptr;
+    if (!c) {
+        ensure_device();
+        auto *nc = new SyncContext();
+        CUDA_CHECK(cudaStreamCreateWithFlags(&nc->stream, cudaStreamNonBlocking));
+        c = nc;
+    }
+    return *c;
 }
 
-static void check_result(const JobState &S, const hpgl_b200_result_t &res) {
-    if (S.job.kind <= KIND_LVM && !res.out_values) invalid("out_values is null");
-    if (S.job.kind > KIND_LVM && !res.out_codes) invalid("out_codes is null");
-    if (!res.out_mask) invalid("out_mask is null");
-    if ((res.nb_index || res.weights) && res.nb_stride < S.nmax_all) invalid("nb_stride smaller than max_neighbours");
+static void sync_arena(SyncContext &C, size_t bytes) {
+    if (bytes <= C.cap) return;
+    if (C.arena) cudaFree(C.arena);
+    C.arena = nullptr;
+    C.cap = 0;
+    CUDA_CHECK(cudaMalloc(&C.arena, bytes));
+    C.cap = bytes;
 }
 
 void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
-    std::lock_guard<std::mutex> lock(g_mutex);
     auto t0 = std::chrono::steady_clock::now();
     JobState S;
-    prepare(S, job);
-    check_result(S, res);
+    prepare(S, job, res);
     res.ms_plan = ms_since(t0);
-    Context &C = ctx();
+    std::lock_guard<std::mutex> lock(g_sync_mutex);
+    SyncContext &C = sync_ctx();
     auto t1 = std::chrono::steady_clock::now();
-    upload_inputs(S, C, &res);
+    sync_arena(C, S.ar.total);
+    S.base = C.arena;
+    upload(S, C.stream);
     CUDA_CHECK(cudaStreamSynchronize(C.stream));
     res.ms_h2d = ms_since(t1);
     cudaEvent_t e0, e1;
@@ -469,45 +521,39 @@ void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     CUDA_CHECK(cudaEventCreate(&e1));
     CUDA_CHECK(cudaEventRecord(e0, C.stream));
     const bool want_nb = res.nb_count || res.nb_index;
-    device_pass(S, C, &res, nullptr, [&](const Group &g) {
-        if (want_nb) download_neighbours(S, C, g, res);
+    device_pass(S, C.stream, nullptr, [&](const Group &g) {
+        if (want_nb) download_neighbours(S, g, res, C.stream);
     });
     CUDA_CHECK(cudaEventRecord(e1, C.stream));
-    Counters cnt;
-    CUDA_CHECK(cudaMemcpyAsync(&cnt, C.counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, C.stream));
-    CUDA_CHECK(cudaStreamSynchronize(C.stream));
+    Counters cnt = read_counters(S, C.stream);
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     res.ms_device = ms;
     auto t2 = std::chrono::steady_clock::now();
-    download(S, C, res, cnt);
+    download(S, res, cnt, C.stream);
     res.ms_d2h = ms_since(t2);
-    // systems attempted: kriged nodes (uninformed for OK/SK/LVM, all for IK)
-    // times categories solved separately
-    long long kriged = 0;
-    if (job.kind <= KIND_LVM) {
-        for (long long i = 0; i < S.size; ++i) kriged += job.mask[i] == 0;
-    } else {
-        kriged = S.size;
-    }
-    res.systems = kriged * (long long)S.groups.size();
-    res.systems_fp64 = (long long)cnt.n_fp64;
-    res.failures = 0;
     res.ms_total = ms_since(t0);
 }
 
 void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_bench_t &bench) {
-    std::lock_guard<std::mutex> lock(g_mutex);
     auto t0 = std::chrono::steady_clock::now();
     JobState S;
-    prepare(S, job);
-    check_result(S, res);
+    prepare(S, job, res);
     bench.ms_plan = ms_since(t0);
-    Context &C = ctx();
-    upload_inputs(S, C, &res);
-    if (bench.flush_bytes > 0) C.flush.ensure((size_t)bench.flush_bytes);
+    std::lock_guard<std::mutex> lock(g_sync_mutex);
+    SyncContext &C = sync_ctx();
+    sync_arena(C, S.ar.total);
+    S.base = C.arena;
+    upload(S, C.stream);
+    if (bench.flush_bytes > (long long)C.flush_cap) {
+        if (C.flush) cudaFree(C.flush);
+        C.flush = nullptr;
+        C.flush_cap = 0;
+        CUDA_CHECK(cudaMalloc(&C.flush, (size_t)bench.flush_bytes));
+        C.flush_cap = (size_t)bench.flush_bytes;
+    }
     CUDA_CHECK(cudaStreamSynchronize(C.stream));
     PassTiming pt;
     CUDA_CHECK(cudaEventCreate(&pt.top0));
@@ -519,12 +565,11 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     Counters cnt{};
     for (int it = 0; it < bench.warmup + bench.iters; ++it) {
         if (bench.flush_bytes > 0)
-            CUDA_CHECK(cudaMemsetAsync(C.flush.p, it & 0xff, (size_t)bench.flush_bytes, C.stream));
+            CUDA_CHECK(cudaMemsetAsync(C.flush, it & 0xff, (size_t)bench.flush_bytes, C.stream));
         CUDA_CHECK(cudaEventRecord(e0, C.stream));
-        device_pass(S, C, &res, &pt, nullptr);
+        device_pass(S, C.stream, &pt, nullptr);
         CUDA_CHECK(cudaEventRecord(e1, C.stream));
-        CUDA_CHECK(cudaMemcpyAsync(&cnt, C.counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, C.stream));
-        CUDA_CHECK(cudaStreamSynchronize(C.stream));
+        cnt = read_counters(S, C.stream);
         if (it >= bench.warmup) {
             float ms = 0, tms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
@@ -534,24 +579,251 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
         }
     }
     bench.ms_top_kernel = bench.iters > 0 ? top_sum / bench.iters : 0;
-    snprintf(bench.top_kernel, sizeof(bench.top_kernel), "k_solve<%d,%d>", S.nmax_all <= 32 ? 32 : 64,
-             S.precision);
+    snprintf(bench.top_kernel, sizeof(bench.top_kernel), "%s",
+             S.nmax_all <= 32 ? (S.precision ? "k_solve_mixed32" : "k_solve_exact32")
+                              : (S.precision ? "k_solve<64,1>" : "k_solve<64,0>"));
     bench.launches_per_iter = pt.launches;
     cudaEventDestroy(pt.top0);
     cudaEventDestroy(pt.top1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    download(S, C, res, cnt);
-    long long kriged = 0;
-    if (job.kind <= KIND_LVM) {
-        for (long long i = 0; i < S.size; ++i) kriged += job.mask[i] == 0;
-    } else {
-        kriged = S.size;
+    download(S, res, cnt, C.stream);
+    bench.systems = res.systems;
+    bench.systems_fp64 = res.systems_fp64;
+}
+
+// ---- server: continuous batching ----------------------------------------------
+//
+// Each submitted job is planned on a host worker, then waits for admission:
+// a free stream slot and room in the HBM budget for its arena.  Admitted jobs
+// run concurrently, each on its own stream with an arena from the
+// stream-ordered pool, so work from jobs that arrive while others are on the
+// GPU overlaps on the device; finishing jobs return their memory and slot and
+// the next waiting job is admitted at once.  Results are exactly those of
+// hpgl_b200_krige on the same job (the kernels share nothing across jobs).
+
+struct ServerJob {
+    long long ticket;
+    hpgl_b200_job_t job;
+    std::vector<hpgl_ik_params_t> params;
+    hpgl_b200_result_t *result;
+    std::chrono::steady_clock::time_point submitted;
+    bool done = false;
+    int code = HPGL_OK;
+    std::string message;
+    double latency_ms = 0;
+};
+
+struct Server {
+    long long budget;
+    int max_inflight;
+    std::vector<cudaStream_t> streams;
+    std::vector<int> free_slots;
+    long long in_use = 0;
+    long long peak_bytes = 0;
+    int inflight = 0;
+    int peak_inflight = 0;
+    std::mutex mu;
+    std::condition_variable cv_admit;
+    std::condition_variable cv_done;
+    std::deque<std::shared_ptr<ServerJob>> queue;
+    std::vector<std::shared_ptr<ServerJob>> all;
+    std::vector<std::thread> workers;
+    bool stopping = false;
+    long long next_ticket = 0;
+    long long systems_done = 0;
+    std::chrono::steady_clock::time_point first_submit, last_done;
+    bool any_submit = false;
+    int device = 0;
+
+    void worker_loop();
+    void run_one(const std::shared_ptr<ServerJob> &sj);
+};
+
+void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
+    JobState S;
+    int slot = -1;
+    long long bytes = 0;
+    try {
+        CUDA_CHECK(cudaSetDevice(device));
+        prepare(S, sj->job, *sj->result);
+        bytes = (long long)S.ar.total;
+        if (bytes > budget)
+            throw HpglError{HPGL_E_CAPACITY, "job needs " + std::to_string(bytes) +
+                                                 " bytes of device memory, above the server's budget of " +
+                                                 std::to_string(budget)};
+        {
+            std::unique_lock<std::mutex> l(mu);
+            cv_admit.wait(l, [&] { return stopping || (!free_slots.empty() && in_use + bytes <= budget); });
+            if (stopping) throw HpglError{HPGL_E_INTERNAL, "server stopped"};
+            slot = free_slots.back();
+            free_slots.pop_back();
+            in_use += bytes;
+            peak_bytes = std::max(peak_bytes, in_use);
+            ++inflight;
+            peak_inflight = std::max(peak_inflight, inflight);
+        }
+        cudaStream_t s = streams[slot];
+        void *arena = nullptr;
+        CUDA_CHECK(cudaMallocAsync(&arena, S.ar.total, s));
+        S.base = (char *)arena;
+        try {
+            upload(S, s);
+            device_pass(S, s, nullptr, nullptr);
+            Counters cnt = read_counters(S, s);
+            download(S, *sj->result, cnt, s);
+        } catch (...) {
+            cudaFreeAsync(arena, s);
+            cudaStreamSynchronize(s);
+            throw;
+        }
+        CUDA_CHECK(cudaFreeAsync(arena, s));
+        CUDA_CHECK(cudaStreamSynchronize(s));
+    } catch (const HpglError &e) {
+        sj->code = e.code;
+        sj->message = e.message;
+    } catch (const std::exception &e) {
+        sj->code = HPGL_E_INTERNAL;
+        sj->message = e.what();
     }
-    bench.systems = kriged * (long long)S.groups.size();
-    bench.systems_fp64 = (long long)cnt.n_fp64;
-    res.systems = bench.systems;
-    res.systems_fp64 = bench.systems_fp64;
+    std::lock_guard<std::mutex> l(mu);
+    if (slot >= 0) {
+        free_slots.push_back(slot);
+        in_use -= bytes;
+        --inflight;
+    }
+    sj->done = true;
+    sj->latency_ms = ms_since(sj->submitted);
+    if (sj->code == HPGL_OK) systems_done += sj->result->systems;
+    last_done = std::chrono::steady_clock::now();
+    cv_admit.notify_all();
+    cv_done.notify_all();
+}
+
+void Server::worker_loop() {
+    while (true) {
+        std::shared_ptr<ServerJob> sj;
+        {
+            std::unique_lock<std::mutex> l(mu);
+            cv_admit.wait(l, [&] { return stopping || !queue.empty(); });
+            if (queue.empty()) return;
+            sj = queue.front();
+            queue.pop_front();
+        }
+        run_one(sj);
+    }
+}
+
+void *server_create(const hpgl_b200_server_config_t &cfg) {
+    ensure_device();
+    if (cfg.hbm_budget_bytes <= 0) invalid("hbm_budget_bytes must be positive");
+    if (cfg.max_inflight < 1 || cfg.max_inflight > 64) invalid("max_inflight must be in [1, 64]");
+    auto *sv = new Server();
+    sv->budget = cfg.hbm_budget_bytes;
+    sv->max_inflight = cfg.max_inflight;
+    cudaGetDevice(&sv->device);
+    // Keep freed arenas in the pool up to the budget, so admission does not
+    // return memory to the driver and fetch it again.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, sv->device) == cudaSuccess) {
+        unsigned long long thr = (unsigned long long)cfg.hbm_budget_bytes;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    for (int i = 0; i < cfg.max_inflight; ++i) {
+        cudaStream_t s;
+        CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        sv->streams.push_back(s);
+        sv->free_slots.push_back(i);
+    }
+    int workers = cfg.worker_threads > 0 ? cfg.worker_threads : cfg.max_inflight * 2;
+    for (int i = 0; i < workers; ++i) sv->workers.emplace_back([sv] { sv->worker_loop(); });
+    return sv;
+}
+
+long long server_submit(void *h, const hpgl_b200_job_t &job, hpgl_b200_result_t *result) {
+    auto *sv = (Server *)h;
+    if (!result) invalid("result is null");
+    if (!job.params || job.n_params < 1 || job.n_params > 255) invalid("params missing");
+    auto sj = std::make_shared<ServerJob>();
+    sj->job = job;
+    sj->params.assign(job.params, job.params + job.n_params);
+    sj->job.params = sj->params.data();
+    sj->result = result;
+    sj->submitted = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> l(sv->mu);
+    if (!sv->any_submit) {
+        sv->any_submit = true;
+        sv->first_submit = sj->submitted;
+    }
+    sj->ticket = sv->next_ticket++;
+    sv->all.push_back(sj);
+    sv->queue.push_back(sj);
+    sv->cv_admit.notify_all();
+    return sj->ticket;
+}
+
+int server_wait(void *h, long long ticket, int timeout_ms, std::string &message) {
+    auto *sv = (Server *)h;
+    std::unique_lock<std::mutex> l(sv->mu);
+    if (ticket < 0 || ticket >= (long long)sv->all.size()) invalid("unknown ticket");
+    auto sj = sv->all[ticket];
+    auto ready = [&] { return sj->done; };
+    if (timeout_ms < 0) sv->cv_done.wait(l, ready);
+    else if (!sv->cv_done.wait_for(l, std::chrono::milliseconds(timeout_ms), ready)) return -1;
+    message = sj->message;
+    return sj->code;
+}
+
+void server_stats(void *h, hpgl_b200_server_stats_t &st) {
+    auto *sv = (Server *)h;
+    std::lock_guard<std::mutex> l(sv->mu);
+    std::vector<double> lat;
+    long long failed = 0, completed = 0;
+    for (auto &sj : sv->all) {
+        if (!sj->done) continue;
+        ++completed;
+        if (sj->code != HPGL_OK) ++failed;
+        else lat.push_back(sj->latency_ms);
+    }
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double q) {
+        if (lat.empty()) return 0.0;
+        long long i = (long long)std::ceil(q * (double)lat.size()) - 1;
+        if (i < 0) i = 0;
+        if (i >= (long long)lat.size()) i = (long long)lat.size() - 1;
+        return lat[i];
+    };
+    double sum = 0;
+    for (double v : lat) sum += v;
+    st.submitted = (long long)sv->all.size();
+    st.completed = completed;
+    st.failed = failed;
+    st.systems = sv->systems_done;
+    st.p50_ms = pct(0.50);
+    st.p99_ms = pct(0.99);
+    st.mean_ms = lat.empty() ? 0 : sum / lat.size();
+    st.wall_s = sv->any_submit && completed ? std::chrono::duration<double>(sv->last_done - sv->first_submit).count()
+                                            : 0;
+    st.systems_per_s = st.wall_s > 0 ? sv->systems_done / st.wall_s : 0;
+    st.peak_inflight = sv->peak_inflight;
+    st.peak_bytes = sv->peak_bytes;
+}
+
+void server_destroy(void *h) {
+    auto *sv = (Server *)h;
+    {
+        std::unique_lock<std::mutex> l(sv->mu);
+        sv->cv_done.wait(l, [&] {
+            for (auto &sj : sv->all)
+                if (!sj->done) return false;
+            return true;
+        });
+        sv->stopping = true;
+        sv->cv_admit.notify_all();
+    }
+    for (auto &t : sv->workers) t.join();
+    for (auto s : sv->streams) cudaStreamDestroy(s);
+    delete sv;
 }
 
 }  // namespace hpgl_b200

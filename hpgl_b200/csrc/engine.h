@@ -27,6 +27,13 @@ void sk_weights_alloc(const float *center, const float *xs, const float *ys, con
 void sk_weights_static(const float *center, const float *xs, const float *ys, const float *zs, int n,
                        const hpgl_cov_params_t *p, float *weights);
 
+// Server (engine.cu); handles are Server* behind void*.
+void *server_create(const hpgl_b200_server_config_t &cfg);
+long long server_submit(void *h, const hpgl_b200_job_t &job, hpgl_b200_result_t *result);
+int server_wait(void *h, long long ticket, int timeout_ms, std::string &message);
+void server_stats(void *h, hpgl_b200_server_stats_t &st);
+void server_destroy(void *h);
+
 int default_precision();
 void set_default_precision(int p);
 

@@ -754,15 +754,14 @@ __global__ void k_ik_argmax(DevJob J) {
 }
 
 // ---------------------------------------------------------------------------
-static int g_sm_count = 0;
 static int sm_count() {
-    if (!g_sm_count) {
-        int dev = 0;
+    static const int n = [] {
+        int dev = 0, sms = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-        if (g_sm_count <= 0) g_sm_count = 148;
-    }
-    return g_sm_count;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        return sms > 0 ? sms : 148;
+    }();
+    return n;
 }
 
 void launch_build_bits(const DevJob &J, const DevPlan &P, uint32_t *bits, cudaStream_t s) {
@@ -786,14 +785,12 @@ template <int NMAX, int MODE>
 static void launch_solve_t(const DevJob &J, const DevPlan &P, const int *list, const int *n_list, long long n_max,
                            cudaStream_t s) {
     using C = SolveCfg<NMAX, MODE>;
-    static bool configured = false;
-    if (!configured) {
+    static const int per_sm = [] {
         cudaFuncSetAttribute(k_solve<NMAX, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-        configured = true;
-    }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<NMAX, MODE>, C::WARPS * 32, C::SMEM);
-    if (per_sm < 1) per_sm = 1;
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_solve<NMAX, MODE>, C::WARPS * 32, C::SMEM);
+        return v < 1 ? 1 : v;
+    }();
     long long blocks = (n_max + C::WARPS - 1) / C::WARPS;
     long long cap = (long long)sm_count() * per_sm * 8;
     if (blocks > cap) blocks = cap;

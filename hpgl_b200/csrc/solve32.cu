@@ -524,14 +524,12 @@ void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int 
                     long long n_max, cudaStream_t s) {
     if (n_max <= 0) return;
     if (precision == 0 || node_list) {
-        static int grid = 0;
-        if (!grid) grid = grid_for((const void *)k_solve_exact32, WARPS32 * 32);
+        static const int grid = grid_for((const void *)k_solve_exact32, WARPS32 * 32);
         long long blocks = (n_max + WARPS32 - 1) / WARPS32;
         if (blocks > grid) blocks = grid;
         k_solve_exact32<<<(unsigned)blocks, WARPS32 * 32, SMEM32, s>>>(J, P, node_list, n_list);
     } else {
-        static int grid = 0;
-        if (!grid) grid = grid_for((const void *)k_solve_mixed32, WARPS32 * 32);
+        static const int grid = grid_for((const void *)k_solve_mixed32, WARPS32 * 32);
         long long blocks = (n_max + WARPS32 - 1) / WARPS32;
         if (blocks > grid) blocks = grid;
         k_solve_mixed32<<<(unsigned)blocks, WARPS32 * 32, SMEM32, s>>>(J, P);

@@ -155,14 +155,14 @@ def lvm_512x512x32(shape=(512, 512, 32), seed=4, blobs=200, sigma=3.0):
 _RADIUS_FACTOR = {SPHERICAL: 1.0, EXPONENTIAL: 1.54, GAUSSIAN: 1.24}
 
 
-def serve_job(rng, job_id=0):
+def serve_job(rng, job_id=0, max_cells=256 * 256 * 64):
     """One job of the serving stream: grid log-uniform between 32^3 and
     256x256x64 cells, informed fraction 0.5-3 %, variogram type uniform over
     spherical/exponential/Gaussian, ranges 5-60, nugget 0-0.1, 8-64
     neighbours, radii = ceil(f * range) with f the 1 %-covariance extent
     (1.0 spherical, 1.54 exponential, 1.24 Gaussian); kind 50 % OK, 25 % SK,
     25 % 4-category IK."""
-    lo, hi = math.log(32 ** 3), math.log(256 * 256 * 64)
+    lo, hi = math.log(min(32 ** 3, max_cells)), math.log(max_cells)
     cells = math.exp(rng.uniform(lo, hi))
     aspect = np.array([4.0, 4.0, 1.0]) * rng.uniform(0.8, 1.25, 3)
     s = (cells / np.prod(aspect)) ** (1.0 / 3.0)
@@ -194,14 +194,14 @@ def serve_job(rng, job_id=0):
                 sk_mean=0.0)
 
 
-def serve_stream(n_jobs, rate_per_s, seed=5):
+def serve_stream(n_jobs, rate_per_s, seed=5, max_cells=256 * 256 * 64):
     """Poisson arrivals at ``rate_per_s``: list of (arrival_time_s, job)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for j in range(n_jobs):
         t += rng.exponential(1.0 / rate_per_s)
-        out.append((t, serve_job(rng, j)))
+        out.append((t, serve_job(rng, j, max_cells=max_cells)))
     return out
 
 

@@ -354,6 +354,43 @@ int hpgl_b200_simple_kriging_weights_static(float *center_coords, float *neighbo
                                             float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                             float *weights);
 
+/* Serving: continuous batching of kriging jobs (no counterpart in the
+   reference).  Jobs are planned on host workers, admitted as soon as a
+   stream slot is free and their device footprint fits in the HBM budget,
+   and run concurrently on the GPU, each on its own stream; a job that
+   arrives while others run starts as soon as one finishes.  Each result is
+   exactly what hpgl_b200_krige returns for that job.  The caller keeps the
+   job's input arrays and the result's buffers alive until the job completes
+   (hpgl_b200_server_wait); the job struct and its params array are copied at
+   submission. */
+typedef struct hpgl_b200_server_t hpgl_b200_server_t;
+typedef struct hpgl_b200_server_config_t {
+    long long hbm_budget_bytes;   /* device memory the in-flight jobs may hold */
+    int max_inflight;             /* concurrent jobs (streams), 1..64 */
+    int worker_threads;           /* host planning/IO threads; 0 = 2 * max_inflight */
+} hpgl_b200_server_config_t;
+typedef struct hpgl_b200_server_stats_t {
+    long long submitted, completed, failed;
+    long long systems;            /* kriging systems of the completed jobs */
+    double p50_ms, p99_ms, mean_ms; /* submit-to-completion latency */
+    double wall_s;                /* first submission to last completion */
+    double systems_per_s;
+    int peak_inflight;
+    long long peak_bytes;
+} hpgl_b200_server_stats_t;
+/* Returns NULL on error (see hpgl_get_last_exception_message). */
+hpgl_b200_server_t *hpgl_b200_server_create(const hpgl_b200_server_config_t *config);
+/* Returns a ticket >= 0, or -HPGL_E_* on a rejected submission.  A job whose
+   footprint exceeds the whole budget completes with HPGL_E_CAPACITY. */
+long long hpgl_b200_server_submit(hpgl_b200_server_t *server, const hpgl_b200_job_t *job,
+                                  hpgl_b200_result_t *result);
+/* Waits up to timeout_ms (< 0: forever).  Returns the job's HPGL_* code once
+   it completed, or -1 when it is still running. */
+int hpgl_b200_server_wait(hpgl_b200_server_t *server, long long ticket, int timeout_ms);
+int hpgl_b200_server_stats(hpgl_b200_server_t *server, hpgl_b200_server_stats_t *stats);
+/* Waits for every submitted job, then releases the server. */
+void hpgl_b200_server_destroy(hpgl_b200_server_t *server);
+
 /* Library build and device description, e.g. for logs. */
 const char *hpgl_b200_version(void);
 
