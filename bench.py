@@ -165,6 +165,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=200000)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-jobs", type=int, default=60)
+    ap.add_argument("--serve-rate", type=float, default=40.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -241,6 +244,21 @@ def main():
                 "peak_source": "nominal FP32 CUDA-core peak (MEASURED_PEAKS.json has HBM and bf16 tensor only)",
                 "ms_per_launch": info_m["ms_top_kernel"], "flop_per_launch": flops}
 
+    # Serving: a Poisson stream of mixed OK/SK/IK jobs (grids 32^3 .. 256x256x64,
+    # ranges 5-60, 8-64 neighbours) replayed in real time against the
+    # continuous-batching server; p50/p99 submit-to-completion latency.
+    serve = None
+    if not args.no_serve:
+        from hpgl_b200 import serve as SV
+        stream = W.serve_stream(args.serve_jobs, args.serve_rate, seed=5 + rank)
+        serve = {"rate_jobs_per_s": args.serve_rate, "jobs": args.serve_jobs, "hbm_budget_gb": 120,
+                 "max_inflight": 8}
+        for prec in ("mixed", "fp64"):
+            st, _ = SV.run_stream(stream, precision=prec, hbm_budget_bytes=120 << 30, max_inflight=8)
+            serve[prec] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "systems_per_s": st["systems_per_s"],
+                           "completed": st["completed"], "failed": st["failed"],
+                           "peak_inflight": st["peak_inflight"]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -266,6 +284,7 @@ def main():
             "clocks": clk,
             "gpu_launches": info_m["launches"] * args.steps,
             "cpu_baseline": cpu,
+            "serve": serve,
         }
         print(json.dumps(line))
     if world > 1:

@@ -322,6 +322,40 @@ void hpgl_b200_server_destroy(hpgl_b200_server_t *server) {
     });
 }
 
+long long hpgl_b200_search_template(const hpgl_ik_params_t *params, int *out_xyz, long long cap) {
+    long long n = -1;
+    guarded("hpgl_b200_search_template", [&] {
+        if (!params || (cap > 0 && !out_xyz)) throw HpglError{HPGL_E_INVALID, "null argument"};
+        KrigingParams kp;
+        kp.cov_type = params->m_covariance_type;
+        for (int i = 0; i < 3; ++i) {
+            kp.ranges[i] = params->m_ranges[i];
+            kp.angles[i] = params->m_angles[i];
+            kp.radii[i] = params->m_radiuses[i];
+        }
+        kp.sill = params->m_sill;
+        kp.nugget = params->m_nugget;
+        kp.max_neighbours = params->m_max_neighbours;
+        kp.marginal_prob = params->m_marginal_prob;
+        const unsigned char informed = 1;
+        Plan P;
+        try {
+            build_plan(P, KIND_SK, 1, 1, 1, kp, &informed, host_threads());
+        } catch (const std::domain_error &e) {
+            throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
+        } catch (const std::invalid_argument &e) {
+            throw HpglError{HPGL_E_INVALID, e.what()};
+        }
+        n = (long long)P.tmpl.size();
+        for (long long i = 0; i < n && i < cap; ++i) {
+            out_xyz[3 * i] = P.tmpl[i].dx;
+            out_xyz[3 * i + 1] = P.tmpl[i].dy;
+            out_xyz[3 * i + 2] = P.tmpl[i].dz;
+        }
+    });
+    return n;
+}
+
 const char *hpgl_b200_version(void) { return "hpgl_b200 0.1 (sm_100a kriging path)"; }
 
 int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float *neighbours_y, float *neighbours_z,

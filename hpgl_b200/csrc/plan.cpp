@@ -6,13 +6,22 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <stdexcept>
+#include <mutex>
 #include <thread>
+
+#include "introsort.h"
 
 namespace hpgl_b200 {
 
 static std::atomic<int> g_threads{0};
+
+template <typename F>
+static void parallel_for(long long n, int threads, F f);
 
 int host_threads() {
     int n = g_threads.load();
@@ -38,6 +47,80 @@ static void parallel_for(long long n, int threads, F f) {
         pool.emplace_back([=] { f(lo, hi); });
     }
     for (auto &th : pool) th.join();
+}
+
+// C(v) over the box |v_i| <= r_i into out[((z+rz)*(2ry+1) + y+ry)*(2rx+1) + x+rx],
+// evaluated as f(x, y, z).  C(v) == C(-v) bit for bit (every transformed
+// component only changes sign), so the half with z > 0 or (z == 0, y > 0) or
+// (z == y == 0, x >= 0) is evaluated and mirrored.
+template <typename F>
+static void fill_symmetric(std::vector<double> &out, int rx, int ry, int rz, int threads, F f) {
+    const int xd = 2 * rx + 1, yd = 2 * ry + 1;
+    out.assign((size_t)xd * yd * (2 * rz + 1), 0.0);
+    auto idx = [&](int x, int y, int z) { return ((size_t)(z + rz) * yd + (y + ry)) * xd + (x + rx); };
+    parallel_for(rz + 1, threads, [&](long long lo, long long hi) {
+        for (long long zz = lo; zz < hi; ++zz) {
+            const int z = (int)zz;
+            for (int y = (z == 0 ? 0 : -ry); y <= ry; ++y)
+                for (int x = (z == 0 && y == 0 ? 0 : -rx); x <= rx; ++x) {
+                    const double v = f(x, y, z);
+                    out[idx(x, y, z)] = v;
+                    out[idx(-x, -y, -z)] = v;
+                }
+        }
+    });
+}
+
+// The reference's std::sort permutation (introsort.h) with the independent
+// right-hand sub-ranges of large partitions sorted on other threads: each
+// sub-range's processing touches only its own elements, so the result is
+// the sequential algorithm's, element for element.
+static void sort_subrange(SortArr a, int lo, int hi, int depth, std::atomic<int> &spare,
+                          std::vector<std::thread> &spawned, std::mutex &mu) {
+    while (hi - lo > 16) {
+        if (depth == 0) {
+            sort_heapsort(a, lo, hi);
+            return;
+        }
+        --depth;
+        const int mid = lo + (hi - lo) / 2;
+        sort_median_to_first(a, lo, lo + 1, mid, hi - 1);
+        const int cut = sort_partition(a, lo + 1, hi, lo);
+        if (hi - cut > 65536 && spare.fetch_sub(1) > 0) {
+            std::lock_guard<std::mutex> l(mu);
+            spawned.emplace_back([=, &spare, &spawned, &mu] { sort_subrange(a, cut, hi, depth, spare, spawned, mu); });
+        } else {
+            if (hi - cut > 65536) spare.fetch_add(1);
+            sort_subrange(a, cut, hi, depth, spare, spawned, mu);
+        }
+        hi = cut;
+    }
+}
+
+static void parallel_reference_sort(std::vector<double> &key, std::vector<int> &idx, int threads) {
+    const int n = (int)key.size();
+    if (n <= 1) return;
+    SortArr a{key.data(), idx.data()};
+    std::atomic<int> spare(threads - 1);
+    std::vector<std::thread> spawned;
+    std::mutex mu;
+    sort_subrange(a, 0, n, 2 * sort_floor_log2(n), spare, spawned, mu);
+    while (true) {
+        std::thread t;
+        {
+            std::lock_guard<std::mutex> l(mu);
+            if (spawned.empty()) break;
+            t = std::move(spawned.back());
+            spawned.pop_back();
+        }
+        t.join();
+    }
+    if (n > 16) {
+        sort_insertion(a, 0, 16);
+        for (int i = 16; i < n; ++i) sort_linear_insert(a, i);
+    } else {
+        sort_insertion(a, 0, n);
+    }
 }
 
 // 3x3 product summed left to right, as TNT's matmult (tnt_cmat.h:472-498).
@@ -121,6 +204,14 @@ double informed_mean(const float *values, const uint8_t *mask, long long size) {
 
 void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
                 int threads) {
+    static const bool timing = getenv("HPGL_B200_PLAN_TIMING") != nullptr;
+    auto t_last = std::chrono::steady_clock::now();
+    auto lap = [&](const char *what) {
+        if (!timing) return;
+        auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "plan %-10s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - t_last).count());
+        t_last = now;
+    };
     validate_params(p, kind);
     CovModel cov(p);
     P.kind = kind;
@@ -140,42 +231,86 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     // same order of equal keys).  Every covariance object the reference can
     // pass here (the model, the precalculated table, covariance_field_t)
     // yields these same values inside the box.
-    const int xd = 2 * rx + 1, yd = 2 * ry + 1, zd = 2 * rz + 1;
-    std::vector<double> data((size_t)xd * yd * zd);
-    parallel_for(zd, threads, [&](long long lo, long long hi) {
-        for (long long zi = lo; zi < hi; ++zi)
-            for (int yi = 0; yi < yd; ++yi)
-                for (int xi = 0; xi < xd; ++xi) {
-                    int x = xi - rx, y = yi - ry, z = (int)zi - rz;
-                    data[((size_t)zi * yd + yi) * xd + xi] = cov(0.0 - x, 0.0 - y, 0.0 - z);
-                }
-    });
+    const int xd = 2 * rx + 1, yd = 2 * ry + 1;
+    std::vector<double> data;
+    fill_symmetric(data, rx, ry, rz, threads, [&](int x, int y, int z) { return cov(0.0 - x, 0.0 - y, 0.0 - z); });
+    lap("box");
     const double c0 = cov(0.0, 0.0, 0.0);
     const double threshold = c0 / 100;
-    struct V3 { int c[3]; };
-    std::vector<V3> vecs;
-    for (int z = -rz; z <= rz; ++z)
-        for (int y = -ry; y <= ry; ++y)
-            for (int x = -rx; x <= rx; ++x)
-                if (data[((size_t)(z + rz) * yd + (y + ry)) * xd + (x + rx)] > threshold) vecs.push_back(V3{{-x, -y, -z}});
-    auto key = [&](const V3 &v) { return data[((size_t)(v.c[2] + rz) * yd + (v.c[1] + ry)) * xd + (v.c[0] + rx)]; };
-    std::sort(vecs.begin(), vecs.end(), [&](const V3 &a, const V3 &b) { return key(a) > key(b); });
-    for (size_t i = 0; i < vecs.size(); ++i)
-        if (key(vecs[i]) < threshold) {
-            vecs.resize(i);
+    // Offsets -v in z-y-x order of v, keyed by C(v) (= C(-v)); collected per
+    // z-slab in parallel and concatenated in slab order.
+    std::vector<double> keys;
+    std::vector<int> order;
+    {
+        const int zd = 2 * rz + 1;
+        std::vector<std::vector<double>> kz(zd);
+        std::vector<std::vector<int>> oz(zd);
+        parallel_for(zd, threads, [&](long long lo, long long hi) {
+            for (long long zi = lo; zi < hi; ++zi) {
+                const int z = (int)zi - rz;
+                for (int y = -ry; y <= ry; ++y)
+                    for (int x = -rx; x <= rx; ++x) {
+                        const double k = data[((size_t)(z + rz) * yd + (y + ry)) * xd + (x + rx)];
+                        if (k > threshold) {
+                            kz[zi].push_back(k);
+                            oz[zi].push_back((int)((((size_t)(-z + rz) * yd) + (-y + ry)) * xd + (-x + rx)));
+                        }
+                    }
+            }
+        });
+        size_t total = 0;
+        for (auto &v : kz) total += v.size();
+        keys.reserve(total);
+        order.reserve(total);
+        for (int zi = 0; zi < zd; ++zi) {
+            keys.insert(keys.end(), kz[zi].begin(), kz[zi].end());
+            order.insert(order.end(), oz[zi].begin(), oz[zi].end());
+        }
+    }
+    parallel_reference_sort(keys, order, threads);
+    lap("sort");
+    size_t kept = keys.size();
+    for (size_t i = 0; i < keys.size(); ++i)
+        if (keys[i] < threshold) {
+            kept = i;
             break;
         }
-    P.tmpl.resize(vecs.size());
+    P.tmpl.resize(kept);
+    parallel_for((long long)kept, threads, [&](long long lo, long long hi) {
+        for (long long i = lo; i < hi; ++i) {
+            const int o = order[i];
+            TemplateEntry &e = P.tmpl[i];
+            e.dx = o % xd - rx;
+            e.dy = o / xd % yd - ry;
+            e.dz = o / xd / yd - rz;
+            e.delta = e.dx + nx * (e.dy + ny * e.dz);
+        }
+    });
+    // the template's extent is that of the offsets above the threshold, which
+    // the box scan already knows
     P.ext[0] = P.ext[1] = P.ext[2] = 0;
-    for (size_t i = 0; i < vecs.size(); ++i) {
-        TemplateEntry &e = P.tmpl[i];
-        e.dx = vecs[i].c[0];
-        e.dy = vecs[i].c[1];
-        e.dz = vecs[i].c[2];
-        e.delta = e.dx + nx * (e.dy + ny * e.dz);
-        for (int a = 0; a < 3; ++a) P.ext[a] = std::max(P.ext[a], std::abs(vecs[i].c[a]));
+    for (int z = -rz; z <= rz; ++z)
+        for (int y = -ry; y <= ry; ++y) {
+            const double *row = &data[((size_t)(z + rz) * yd + (y + ry)) * xd];
+            for (int x = -rx; x <= rx; ++x)
+                if (row[x + rx] > threshold) {
+                    P.ext[0] = std::max(P.ext[0], std::abs(x));
+                    P.ext[1] = std::max(P.ext[1], std::abs(y));
+                    P.ext[2] = std::max(P.ext[2], std::abs(z));
+                }
+        }
+    if (kept < keys.size()) {
+        // entries cut after the sort (not reachable with the > threshold
+        // filter, kept for the reference's second cut-off) do not widen ext
+        P.ext[0] = P.ext[1] = P.ext[2] = 0;
+        for (const TemplateEntry &e : P.tmpl) {
+            P.ext[0] = std::max(P.ext[0], std::abs(e.dx));
+            P.ext[1] = std::max(P.ext[1], std::abs(e.dy));
+            P.ext[2] = std::max(P.ext[2], std::abs(e.dz));
+        }
     }
 
+    lap("template");
     // ---- clusterizer (clusterizer.cpp:52-184) ----
     // Boxes of the radii (doubles in the reference: sugarbox_search_ellipsoid_t),
     // mx = (int)(nx / rx + 2); a box overflows past limit = |template| / 250
@@ -244,6 +379,7 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
                 }
             }
 
+    lap("buckets");
     // ---- covariance table ----
     // Truncated kinds read C(v) only for |v| <= radii.  Ordinary kriging uses
     // the untruncated model; the template path needs |v| <= 2*ext (pairs of
@@ -261,17 +397,10 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
         P.B[a] = std::max(0, std::min(need, n3[a] - 1));
         P.trunc[a] = P.truncated ? p.radii[a] : P.B[a];
     }
-    const int bx = 2 * P.B[0] + 1, by = 2 * P.B[1] + 1, bz = 2 * P.B[2] + 1;
-    P.table.assign((size_t)bx * by * bz, 0.0);
-    parallel_for(bz, threads, [&](long long lo, long long hi) {
-        for (long long zi = lo; zi < hi; ++zi)
-            for (int yi = 0; yi < by; ++yi)
-                for (int xi = 0; xi < bx; ++xi) {
-                    int x = xi - P.B[0], y = yi - P.B[1], z = (int)zi - P.B[2];
-                    P.table[((size_t)zi * by + yi) * bx + xi] = cov((double)x, (double)y, (double)z);
-                }
-    });
+    fill_symmetric(P.table, P.B[0], P.B[1], P.B[2], threads,
+                   [&](int x, int y, int z) { return cov((double)x, (double)y, (double)z); });
     P.c0 = c0;
+    lap("table");
 
     // ---- informed-bit rows for the device template search ----
     P.px = 32 * ((P.ext[0] + 31) / 32);

@@ -391,6 +391,14 @@ int hpgl_b200_server_stats(hpgl_b200_server_t *server, hpgl_b200_server_stats_t 
 /* Waits for every submitted job, then releases the server. */
 void hpgl_b200_server_destroy(hpgl_b200_server_t *server);
 
+/* The sorted search template this build derives from `params` (host
+   planning only, no GPU needed): offsets (dx, dy, dz) in the order the
+   search walks them, i.e. the reference's calc_cov_field order
+   (covariance_field.h:62-106).  Writes at most `cap` triples to out_xyz and
+   returns the template's length (> cap: only the first cap written), or -1
+   on error. */
+long long hpgl_b200_search_template(const hpgl_ik_params_t *params, int *out_xyz, long long cap);
+
 /* Library build and device description, e.g. for logs. */
 const char *hpgl_b200_version(void);
 
