@@ -193,4 +193,47 @@ HPGL_HD bool reference_sort(SortArr &a, int n) {
     return true;
 }
 
+// The first `k` positions of reference_sort's result, without sorting the
+// rest.  Sub-ranges are processed independently and the final insertion sort
+// only moves elements within runs of at most 16, so a right-hand part that
+// starts at or beyond k, and insertions of elements at or beyond k + 16,
+// cannot change positions below k: skipping them leaves [0, k) exactly as
+// the full sort would.
+HPGL_HD bool reference_sort_prefix(SortArr &a, int n, int k) {
+    if (n <= 1) return true;
+    if (k >= n) return reference_sort(a, n);
+    struct Frame { int lo, hi, depth; };
+    Frame stack[72];
+    int sp = 0;
+    stack[sp++] = Frame{0, n, 2 * sort_floor_log2(n)};
+    while (sp > 0) {
+        Frame f = stack[--sp];
+        int lo = f.lo, hi = f.hi, depth = f.depth;
+        if (lo >= k) continue;
+        while (hi - lo > 16) {
+            if (depth == 0) {
+                sort_heapsort(a, lo, hi);
+                break;
+            }
+            --depth;
+            int mid = lo + (hi - lo) / 2;
+            sort_median_to_first(a, lo, lo + 1, mid, hi - 1);
+            int cut = sort_partition(a, lo + 1, hi, lo);
+            if (cut < k) {
+                if (sp >= 72) return false;
+                stack[sp++] = Frame{cut, hi, depth};
+            }
+            hi = cut;
+        }
+    }
+    const int end = (k + 16 < n) ? k + 16 : n;
+    if (n > 16) {
+        sort_insertion(a, 0, 16);
+        for (int i = 16; i < end; ++i) sort_linear_insert(a, i);
+    } else {
+        sort_insertion(a, 0, n);
+    }
+    return true;
+}
+
 }  // namespace hpgl_b200

@@ -110,8 +110,9 @@ __global__ void __launch_bounds__(256) k_search_template(DevJob J, DevPlan P) {
 // per node whose 27 boxes are all within their fill limit.  The warp gathers
 // the boxes' informed nodes in the reference's k-j-i / insertion order,
 // keeps those with covariance above C(0)/100 (order-preserving ballot
-// compaction), then one lane sorts them exactly as the reference's std::sort
-// does and the first max_neighbours become the list.
+// compaction), then one lane orders them exactly as the reference's
+// std::sort does — as far as the first max_neighbours positions, which become
+// the list.
 __global__ void __launch_bounds__(128) k_search_cluster(DevJob J, DevPlan P, double *scratch_key, int *scratch_idx,
                                                        int n_warps_total) {
     const int lane = threadIdx.x & 31;
@@ -163,8 +164,9 @@ __global__ void __launch_bounds__(128) k_search_cluster(DevJob J, DevPlan P, dou
         if (n > cap) n = cap;
         __syncwarp();
         if (lane == 0) {
+            // only the first max_neighbours positions of the reference's sort are used
             SortArr a{keys, idxs};
-            if (!reference_sort(a, n)) atomicOr(J.err, DERR_SORT_STACK);
+            if (!reference_sort_prefix(a, n, P.nmax)) atomicOr(J.err, DERR_SORT_STACK);
         }
         __syncwarp();
         const int cnt = n < P.nmax ? n : P.nmax;

@@ -35,6 +35,31 @@ int main(int argc, char **argv) {
                 return 1;
             }
     }
+    // The prefix variant: first k positions equal to the full sort's.
+    for (int c = 0; c < cases; ++c) {
+        int n = (int)(rng() % (c % 10 == 0 ? 6000 : 600));
+        int k = 1 + (int)(rng() % 70);
+        int distinct = 1 + (int)(rng() % (c % 3 == 0 ? 4 : (c % 3 == 1 ? 40 : 100000)));
+        struct E { int index; double cov; };
+        std::vector<E> ref(n);
+        std::vector<double> key(n);
+        std::vector<int> idx(n);
+        for (int i = 0; i < n; ++i) {
+            double kk = (double)(rng() % distinct) * 0.25;
+            if (c % 7 == 0) kk = (double)((n - i) / 3);
+            ref[i] = E{i, kk};
+            key[i] = kk;
+            idx[i] = i;
+        }
+        std::sort(ref.begin(), ref.end(), [](const E &a, const E &b) { return a.cov > b.cov; });
+        hpgl_b200::SortArr a{key.data(), idx.data()};
+        if (!hpgl_b200::reference_sort_prefix(a, n, k)) { printf("stack overflow\n"); return 2; }
+        for (int i = 0; i < k && i < n; ++i)
+            if (ref[i].index != idx[i]) {
+                printf("prefix mismatch case %d n=%d k=%d at %d\n", c, n, k, i);
+                return 1;
+            }
+    }
     // The depth-budget fallback: heap sort of a range, as std::partial_sort
     // over the whole range (heap_select + sort_heap).
     for (int c = 0; c < cases / 10; ++c) {
