@@ -168,6 +168,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=40.0)
+    ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -186,7 +187,8 @@ def main():
     from hpgl_b200 import workloads as W
     if not os.path.exists(N.LIB_PATH):
         build.build()
-    job = W.sk_ok_256x256x64()
+    shape = tuple(int(v) for v in args.grid.split("x")) if args.grid else (256, 256, 64)
+    job = W.sk_ok_256x256x64(shape=shape)
     size = int(np.prod(job["shape"]))
     kriged = int((job["mask"] == 0).sum())
 
@@ -239,8 +241,15 @@ def main():
     # 128 FP32 lanes x 2 flop x 1.965 GHz).
     peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
     achieved = flops / (info_m["ms_top_kernel"] / 1000.0) / 1e12
+    traffic = None
+    try:
+        tj = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["k_solve_mixed32"]
+        # measured on the 128x128x32 cube; DRAM traffic scales with the systems
+        traffic = tj["dram_bytes_per_launch_128x128x32"] * kriged / tj["systems_128x128x32"]
+    except (OSError, KeyError, ValueError):
+        pass
     roofline = {"kernel": info_m["top_kernel"], "bound": "fp32", "achieved": achieved, "peak": peak_fp32,
-                "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic, "traffic_unit": "bytes/launch",
                 "peak_source": "nominal FP32 CUDA-core peak (MEASURED_PEAKS.json has HBM and bf16 tensor only)",
                 "ms_per_launch": info_m["ms_top_kernel"], "flop_per_launch": flops}
 
