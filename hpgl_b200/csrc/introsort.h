@@ -85,6 +85,31 @@ HPGL_HD int sort_partition(SortArr &a, int lo, int hi, int pivot) {
     }
 }
 
+// The same partition computed from its stoppers, the form a warp evaluates
+// in parallel.  Left stoppers L_0 < L_1 < ... are the positions of
+// [lo, hi) whose element is not before the pivot, right stoppers
+// R_0 > R_1 > ... the positions of [pivot, hi) the pivot is not before.  The
+// scans of sort_partition meet stopper k on each side at step k while
+// L_k < R_k, and every such step swaps the pair (L_k, R_k), which no other
+// step touches; with m the first k where L_k >= R_k, the left scan of the
+// last step stops at L_m or, if that lies past R_{m-1}, at R_{m-1} (which
+// holds the swapped-in element of L_{m-1}, a left stopper).  So the result is
+// m disjoint swaps and cut = min(L_m, R_{m-1}).  `lbuf`/`rbuf` hold up to
+// hi - pivot positions each.
+HPGL_HD int sort_partition_pairs(SortArr &a, int lo, int hi, int pivot, int *lbuf, int *rbuf) {
+    int nl = 0, nr = 0;
+    for (int p = lo; p < hi; ++p)
+        if (!a.before(p, pivot)) lbuf[nl++] = p;
+    for (int q = hi - 1; q >= pivot; --q)
+        if (!a.before(pivot, q)) rbuf[nr++] = q;
+    int m = 0;
+    while (m < nl && m < nr && lbuf[m] < rbuf[m]) ++m;
+    for (int k = 0; k < m; ++k) a.swap(lbuf[k], rbuf[k]);
+    const int lm = m < nl ? lbuf[m] : 0x7fffffff;
+    const int rm = m > 0 ? rbuf[m - 1] : 0x7fffffff;
+    return lm < rm ? lm : rm;
+}
+
 // Sift the value (vk, vi) down from `hole` in the heap [first, first+len),
 // then up towards `top`.
 HPGL_HD void sort_adjust_heap(SortArr &a, int first, int hole, int len, double vk, int vi) {

@@ -106,16 +106,148 @@ __global__ void __launch_bounds__(256) k_search_template(DevJob J, DevPlan P) {
 }
 
 // ---------------------------------------------------------------------------
+// Warp form of the reference sort's partition (sort_partition_pairs): each
+// round collects the next 32 left stoppers and 32 right stoppers with
+// ballots, lane k holds the pair (L_k, R_k), the pairs with L_k < R_k (a
+// prefix of the lanes) swap at once, and the first failing pair gives the
+// cut.  Each round scans left from L_{b-1}+1 up to R_{b-1} and right from
+// R_{b-1}-1 down to L_{b-1}; earlier rounds' swaps only ever turn positions
+// at or beyond those bounds into stoppers, which yields the same
+// min(L_m, R_{m-1}).  Ranges up to PAR_PARTITION_MIN elements partition on
+// lane 0.
+constexpr int PAR_PARTITION_MIN = 64;
+constexpr int SORT_STACK = 72;
+
+__device__ int warp_partition(SortArr &a, int lo, int hi, int pivot, int *lbuf, int *rbuf, int lane) {
+    const double pk = a.key[pivot];
+    const uint32_t below = (1u << lane) - 1;
+    int lp = lo, lend = hi - 1;      // left scan window [lp, lend], upwards
+    int rp = hi - 1, rend = pivot;   // right scan window [rend, rp], downwards
+    int rprev = INT_MAX;             // R_{b-1}
+    while (true) {
+        int cnt = 0;
+        for (int p0 = lp; cnt < 32 && p0 <= lend; p0 += 32) {
+            const int p = p0 + lane;
+            const bool st = p <= lend && !(a.key[p] > pk);
+            const uint32_t bal = __ballot_sync(FULL_MASK, st);
+            const int r = cnt + __popc(bal & below);
+            if (st && r < 32) lbuf[r] = p;
+            cnt += __popc(bal);
+        }
+        __syncwarp();
+        const int my_l = lane < cnt ? lbuf[lane] : INT_MAX;
+        cnt = 0;
+        for (int q0 = rp; cnt < 32 && q0 >= rend; q0 -= 32) {
+            const int q = q0 - lane;
+            const bool st = q >= rend && !(pk > a.key[q]);
+            const uint32_t bal = __ballot_sync(FULL_MASK, st);
+            const int r = cnt + __popc(bal & below);
+            if (st && r < 32) rbuf[r] = q;
+            cnt += __popc(bal);
+        }
+        __syncwarp();
+        const int my_r = lane < cnt ? rbuf[lane] : INT_MIN;
+        const bool pair = my_l < my_r;
+        const int m = __popc(__ballot_sync(FULL_MASK, pair));
+        if (pair) a.swap(my_l, my_r);
+        __syncwarp();
+        if (m < 32) {
+            const int lm = __shfl_sync(FULL_MASK, my_l, m);
+            const int rl = __shfl_sync(FULL_MASK, my_r, (m + 31) & 31);
+            const int rm = m > 0 ? rl : rprev;
+            return lm < rm ? lm : rm;
+        }
+        const int l31 = __shfl_sync(FULL_MASK, my_l, 31), r31 = __shfl_sync(FULL_MASK, my_r, 31);
+        lp = l31 + 1;
+        lend = r31;
+        rp = r31 - 1;
+        rend = l31;
+        rprev = r31;
+    }
+}
+
+struct SortFrame {
+    int lo, hi, depth;
+};
+
+// reference_sort_prefix driven by a whole warp: control flow is uniform,
+// lane 0 does the median-of-three, small partitions, heap sorts and the final
+// insertion sort, the warp does the long partitions.  `stack` holds
+// SORT_STACK frames, `lbuf`/`rbuf` 32 positions each (shared memory).
+__device__ bool warp_reference_sort_prefix(SortArr &a, int n, int k, int lane, SortFrame *stack, int *lbuf,
+                                           int *rbuf) {
+    if (n <= 1) return true;
+    if (k > n) k = n;
+    int sp = 0;
+    if (lane == 0) stack[0] = SortFrame{0, n, 2 * sort_floor_log2(n)};
+    ++sp;
+    bool ok = true;
+    while (sp > 0) {
+        __syncwarp();
+        const SortFrame f = stack[--sp];
+        int lo = f.lo, hi = f.hi, depth = f.depth;
+        if (lo >= k) continue;
+        while (hi - lo > 16) {
+            if (depth == 0) {
+                if (lane == 0) sort_heapsort(a, lo, hi);
+                break;
+            }
+            --depth;
+            const int mid = lo + (hi - lo) / 2;
+            if (lane == 0) sort_median_to_first(a, lo, lo + 1, mid, hi - 1);
+            __syncwarp();
+            int cut;
+            if (hi - lo > PAR_PARTITION_MIN) {
+                cut = warp_partition(a, lo + 1, hi, lo, lbuf, rbuf, lane);
+            } else {
+                int c0 = 0;
+                if (lane == 0) c0 = sort_partition(a, lo + 1, hi, lo);
+                cut = __shfl_sync(FULL_MASK, c0, 0);
+            }
+            if (cut < k) {
+                if (sp >= SORT_STACK) {
+                    ok = false;
+                    sp = 0;
+                    break;
+                }
+                __syncwarp();
+                if (lane == 0) stack[sp] = SortFrame{cut, hi, depth};
+                ++sp;
+            }
+            hi = cut;
+        }
+    }
+    __syncwarp();
+    if (!ok) return false;
+    if (lane == 0) {
+        const int end = (k + 16 < n) ? k + 16 : n;
+        if (n > 16) {
+            sort_insertion(a, 0, 16);
+            for (int i = 16; i < end; ++i) sort_linear_insert(a, i);
+        } else {
+            sort_insertion(a, 0, n);
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Clusterizer search (sugarbox_indexed_neighbour_lookup.h:72-121): one warp
 // per node whose 27 boxes are all within their fill limit.  The warp gathers
 // the boxes' informed nodes in the reference's k-j-i / insertion order,
 // keeps those with covariance above C(0)/100 (order-preserving ballot
-// compaction), then one lane orders them exactly as the reference's
+// compaction), then the warp orders them exactly as the reference's
 // std::sort does — as far as the first max_neighbours positions, which become
 // the list.
-__global__ void __launch_bounds__(128) k_search_cluster(DevJob J, DevPlan P, double *scratch_key, int *scratch_idx,
-                                                       int n_warps_total) {
+constexpr int CLUSTER_WARPS = 4;
+
+__global__ void __launch_bounds__(CLUSTER_WARPS * 32) k_search_cluster(DevJob J, DevPlan P, double *scratch_key,
+                                                                      int *scratch_idx, int n_warps_total) {
+    __shared__ SortFrame s_stack[CLUSTER_WARPS][SORT_STACK];
+    __shared__ int s_lbuf[CLUSTER_WARPS][32], s_rbuf[CLUSTER_WARPS][32];
     const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (gw >= n_warps_total) return;
     const int cap = P.max_candidates;
@@ -163,12 +295,12 @@ __global__ void __launch_bounds__(128) k_search_cluster(DevJob J, DevPlan P, dou
                 }
         if (n > cap) n = cap;
         __syncwarp();
-        if (lane == 0) {
+        {
             // only the first max_neighbours positions of the reference's sort are used
             SortArr a{keys, idxs};
-            if (!reference_sort_prefix(a, n, P.nmax)) atomicOr(J.err, DERR_SORT_STACK);
+            if (!warp_reference_sort_prefix(a, n, P.nmax, lane, s_stack[wib], s_lbuf[wib], s_rbuf[wib]) && lane == 0)
+                atomicOr(J.err, DERR_SORT_STACK);
         }
-        __syncwarp();
         const int cnt = n < P.nmax ? n : P.nmax;
         for (int i = lane; i < cnt; i += 32) J.nb[(long long)node * P.nmax + i] = idxs[i];
         if (lane == 0) J.nbcount[node] = cnt;
@@ -780,7 +912,8 @@ void launch_search_template(const DevJob &J, const DevPlan &P, cudaStream_t s) {
 }
 
 void launch_search_cluster(const DevJob &J, const DevPlan &P, double *sk, int *si, int n_warps, cudaStream_t s) {
-    k_search_cluster<<<(unsigned)((n_warps * 32 + 127) / 128), 128, 0, s>>>(J, P, sk, si, n_warps);
+    const int threads = CLUSTER_WARPS * 32;
+    k_search_cluster<<<(unsigned)((n_warps * 32 + threads - 1) / threads), threads, 0, s>>>(J, P, sk, si, n_warps);
 }
 
 template <int NMAX, int MODE>
