@@ -360,8 +360,10 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     return J;
 }
 
+// Events around the first group's phases: search start, solve start, solve
+// end (top kernel), re-solve end.
 struct PassTiming {
-    cudaEvent_t top0 = nullptr, top1 = nullptr;
+    cudaEvent_t search0 = nullptr, top0 = nullptr, top1 = nullptr, resolve1 = nullptr;
     int launches = 0;
 };
 
@@ -375,6 +377,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
     for (size_t gi = 0; gi < S.groups.size(); ++gi) {
         Group &g = S.groups[gi];
         DevJob J = make_devjob(S, g);
+        if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->search0, s));
         CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
         launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
         launch_search_template(J, g.dp, s);
@@ -391,6 +394,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
             launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, J.n_routed, (int)S.size, s);
             ++launches;
         }
+        if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->resolve1, s));
         CUDA_CHECK(cudaGetLastError());
         if (after_group) after_group(g);
         if (S.precision == HPGL_PRECISION_MIXED && gi + 1 < S.groups.size())
@@ -556,12 +560,14 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     }
     CUDA_CHECK(cudaStreamSynchronize(C.stream));
     PassTiming pt;
+    CUDA_CHECK(cudaEventCreate(&pt.search0));
     CUDA_CHECK(cudaEventCreate(&pt.top0));
     CUDA_CHECK(cudaEventCreate(&pt.top1));
+    CUDA_CHECK(cudaEventCreate(&pt.resolve1));
     cudaEvent_t e0, e1;
     CUDA_CHECK(cudaEventCreate(&e0));
     CUDA_CHECK(cudaEventCreate(&e1));
-    double top_sum = 0;
+    double top_sum = 0, search_sum = 0, resolve_sum = 0;
     Counters cnt{};
     for (int it = 0; it < bench.warmup + bench.iters; ++it) {
         if (bench.flush_bytes > 0)
@@ -571,20 +577,28 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
         CUDA_CHECK(cudaEventRecord(e1, C.stream));
         cnt = read_counters(S, C.stream);
         if (it >= bench.warmup) {
-            float ms = 0, tms = 0;
+            float ms = 0, tms = 0, sms = 0, rms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             cudaEventElapsedTime(&tms, pt.top0, pt.top1);
+            cudaEventElapsedTime(&sms, pt.search0, pt.top0);
+            cudaEventElapsedTime(&rms, pt.top1, pt.resolve1);
             if (bench.ms_per_iter) bench.ms_per_iter[it - bench.warmup] = ms;
             top_sum += tms;
+            search_sum += sms;
+            resolve_sum += rms;
         }
     }
     bench.ms_top_kernel = bench.iters > 0 ? top_sum / bench.iters : 0;
+    bench.ms_search = bench.iters > 0 ? search_sum / bench.iters : 0;
+    bench.ms_resolve = bench.iters > 0 ? resolve_sum / bench.iters : 0;
     snprintf(bench.top_kernel, sizeof(bench.top_kernel), "%s",
              S.nmax_all <= 32 ? (S.precision ? "k_solve_mixed32" : "k_solve_exact32")
-                              : (S.precision ? "k_solve<64,1>" : "k_solve<64,0>"));
+                              : (S.precision ? "k_solve<64,1>" : "k_solve_exact64"));
     bench.launches_per_iter = pt.launches;
+    cudaEventDestroy(pt.search0);
     cudaEventDestroy(pt.top0);
     cudaEventDestroy(pt.top1);
+    cudaEventDestroy(pt.resolve1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     download(S, res, cnt, C.stream);

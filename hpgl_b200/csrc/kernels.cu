@@ -941,13 +941,8 @@ void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *n
         launch_solve32(J, P, precision, node_list, n_list, n_max, s);
         return;
     }
-    if (P.nmax <= 32) {
-        if (precision == 0) launch_solve_t<32, 0>(J, P, node_list, n_list, n_max, s);
-        else launch_solve_t<32, 1>(J, P, node_list, n_list, n_max, s);
-    } else {
-        if (precision == 0) launch_solve_t<64, 0>(J, P, node_list, n_list, n_max, s);
-        else launch_solve_t<64, 1>(J, P, node_list, n_list, n_max, s);
-    }
+    if (precision == 0 || node_list) launch_solve64_exact(J, P, node_list, n_list, n_max, s);
+    else launch_solve_t<64, 1>(J, P, node_list, n_list, n_max, s);
 }
 
 void launch_ik_argmax(const DevJob &J, cudaStream_t s) {

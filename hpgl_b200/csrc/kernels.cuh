@@ -89,6 +89,9 @@ void launch_ik_argmax(const DevJob &J, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s);
+// solve64.cu: register-resident exact solves for 33..64 neighbours
+void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
+                          long long n_max, cudaStream_t s);
 int solve_kernel_count();
 
 }  // namespace hpgl_b200

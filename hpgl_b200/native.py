@@ -60,7 +60,8 @@ class Bench(C.Structure):
     _fields_ = [("iters", C.c_int), ("warmup", C.c_int), ("flush_bytes", C.c_longlong),
                 ("ms_per_iter", C.POINTER(C.c_double)), ("ms_top_kernel", C.c_double),
                 ("top_kernel", C.c_char * 64), ("launches_per_iter", C.c_int),
-                ("systems", C.c_longlong), ("systems_fp64", C.c_longlong), ("ms_plan", C.c_double)]
+                ("systems", C.c_longlong), ("systems_fp64", C.c_longlong), ("ms_plan", C.c_double),
+                ("ms_search", C.c_double), ("ms_resolve", C.c_double)]
 
 
 _lib = None
@@ -211,6 +212,7 @@ def bench(job, precision="mixed", iters=5, warmup=3, flush_bytes=256 << 20, kind
     if rc != 0:
         raise HpglError(rc, L.hpgl_get_last_exception_message().decode())
     info = dict(ms_top_kernel=b.ms_top_kernel, top_kernel=b.top_kernel.decode(), launches=b.launches_per_iter,
+                ms_search=b.ms_search, ms_resolve=b.ms_resolve,
                 systems=b.systems, systems_fp64=b.systems_fp64, ms_plan=b.ms_plan, out=p.out,
                 out_mask=p.out_mask)
     return ms, info

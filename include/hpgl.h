@@ -332,6 +332,8 @@ typedef struct hpgl_b200_bench_t {
     long long systems;
     long long systems_fp64;
     double ms_plan;
+    double ms_search;             /* average device time of the first group's searches */
+    double ms_resolve;            /* ... and of its FP64 re-solve of routed systems */
 } hpgl_b200_bench_t;
 int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl_b200_bench_t *bench);
 

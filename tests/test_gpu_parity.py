@@ -26,6 +26,28 @@ CASES = {
     "lvm_96x96x16": (lambda: W.lvm_512x512x32(shape=(96, 96, 16)), "lvm"),
 }
 
+
+
+def _nmax(job, n, **over):
+    """The same job searching up to n neighbours (33..64: the wide solves)."""
+    job = dict(job)
+    job["params"] = [dict(p, max_neighbours=n, **over) for p in job["params"]]
+    return job
+
+
+# Systems of 33 to 64 neighbours, every kind, ragged counts near sparse
+# regions and the grid's edges; the long-range Gaussian model without nugget
+# makes the systems ill-conditioned (about 1.5 % fail the FP64 factorisation,
+# FP32 pivots are routed to the FP64 re-solve).
+CASES.update({
+    "ok_n48_48x48x24": (lambda: _nmax(W.sk_ok_256x256x64(shape=(48, 48, 24)), 48), "ok"),
+    "sk_n64_48x48x24": (lambda: _nmax(W.sk_ok_256x256x64(shape=(48, 48, 24)), 64), "sk"),
+    "ik_n40_40x40x20": (lambda: _nmax(W.ik_200x200x100(shape=(40, 40, 20)), 40), "ik"),
+    "median_ik_n56_40x40x20": (lambda: _nmax(W.ik_200x200x100(shape=(40, 40, 20)), 56), "median_ik"),
+    "ok_gauss_n64_48x48x16": (lambda: _nmax(W.lvm_512x512x32(shape=(48, 48, 16)), 64, nugget=0.0,
+                                            ranges=(300.0, 300.0, 40.0)), "ok"),
+})
+
 _cache = {}
 
 
