@@ -66,4 +66,27 @@ __device__ __forceinline__ double div_by_rcp(double a, double b, double y) {
     return __fma_rn(r, y, q);
 }
 
+// Acceptance of an iterative refinement x <- x + d.  After a correction d_k
+// the remaining error is about rho_k |d_k|, with the contraction rho_k =
+// |d_k| / |d_{k-1}| (for the first correction |d_0| / |x|, the error it
+// removed being about |x|).  A solution is accepted once that estimate is
+// below REFINE_TOL |x| (max norms), so what is accepted is converged to near
+// FP64 accuracy; a refinement that contracts by less than REFINE_RHO_MAX per
+// step is not going to get there and is routed at once.
+constexpr double REFINE_TOL = 1e-13;
+constexpr double REFINE_RHO_MAX = 0.5;
+
+struct RefineGate {
+    double prev = -1.0;
+    // +1 accept, -1 route, 0 correct again
+    __device__ __forceinline__ int step(double dmax, double xmax) {
+        const double rho = prev < 0.0 ? dmax / xmax : dmax / prev;
+        prev = dmax;
+        if (!(xmax > 0.0)) return dmax == 0.0 ? 1 : -1;
+        if (rho * dmax <= REFINE_TOL * xmax) return 1;
+        if (!(rho <= REFINE_RHO_MAX)) return -1;
+        return 0;
+    }
+};
+
 }  // namespace hpgl_b200

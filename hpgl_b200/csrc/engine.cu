@@ -593,7 +593,7 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     bench.ms_resolve = bench.iters > 0 ? resolve_sum / bench.iters : 0;
     snprintf(bench.top_kernel, sizeof(bench.top_kernel), "%s",
              S.nmax_all <= 32 ? (S.precision ? "k_solve_mixed32" : "k_solve_exact32")
-                              : (S.precision ? "k_solve<64,1>" : "k_solve_exact64"));
+                              : (S.precision ? "k_solve_mixed64" : "k_solve_exact64"));
     bench.launches_per_iter = pt.launches;
     cudaEventDestroy(pt.search0);
     cudaEventDestroy(pt.top0);

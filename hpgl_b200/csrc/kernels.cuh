@@ -89,9 +89,10 @@ void launch_ik_argmax(const DevJob &J, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s);
-// solve64.cu: register-resident exact solves for 33..64 neighbours
+// solve64.cu: solves for 33..64 neighbours (exact FP64; FP32 inverse + FP64
+// refinement, routing to `routed`)
 void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
                           long long n_max, cudaStream_t s);
-int solve_kernel_count();
+void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s);
 
 }  // namespace hpgl_b200

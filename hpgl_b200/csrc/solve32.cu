@@ -26,9 +26,7 @@ namespace {
 constexpr int N32 = 32;
 constexpr int WARPS32 = 4;
 constexpr float MIXED_PIVOT_MIN = 1e-3f;  // on the unit-diagonal scaled system
-constexpr double MIXED_ACCEPT_1 = 1e-7;   // |d| / |x| after the first correction
-constexpr double MIXED_ACCEPT_N = 1e-7;   // after later corrections
-constexpr int MIXED_MAX_CORR = 3;
+constexpr int MIXED_MAX_CORR = 4;
 
 struct SysSmem {
     double A[N32 * 34];     // exact: in-place factor (column k at k*34); mixed: full system (LD 33)
@@ -458,6 +456,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
         double xa = (double)apply_inverse(m2, (float)d.b, S.vf[0], lane) * sc;
         double xb = ordinary ? (double)apply_inverse(m2, lane < n ? 1.f : 0.f, S.vf[1], lane) * sc : 0.0;
         const double ba = d.b, bb = lane < n ? 1.0 : 0.0;
+        RefineGate gate;
         bool converged = false;
         for (int corr = 0; corr < MIXED_MAX_CORR; ++corr) {
             const double ra = residual(S, S.vd, xa, ba, lane);
@@ -471,10 +470,9 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
                 dmax = fmax(dmax, fabs(db));
                 xmax = fmax(xmax, fabs(xb));
             }
-            dmax = warp_max(dmax);
-            xmax = warp_max(xmax);
-            if (dmax <= (corr == 0 ? MIXED_ACCEPT_1 : MIXED_ACCEPT_N) * xmax) {
-                converged = true;
+            const int verdict = gate.step(warp_max(dmax), warp_max(xmax));
+            if (verdict != 0) {
+                converged = verdict > 0;
                 break;
             }
         }

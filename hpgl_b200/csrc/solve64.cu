@@ -29,6 +29,8 @@ constexpr int WARPS64_BLOCK = 1;
 // different 16-byte bank groups, 4 each: conflict-free.  Column k is the
 // matrix column A(., k) until its rows are overwritten, one per step, by the
 // factor's row; its diagonal slot stays zero until step k.
+// (col_start_c runs a loop: device code reads the starts from a table the
+// kernels fill once per block.)
 __host__ __device__ constexpr int col_start_c(int k) {
     int start = 0, end = 0;
     for (int c = 0; c <= k; ++c) {
@@ -211,37 +213,41 @@ __device__ __forceinline__ double pair_cov64(const DevJob &J, const DevPlan &P, 
     return cov_lin(P, a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, J.err);
 }
 
+// Build: the n(n-1)/2 entries A(i, k) = C(x_i - x_k), i < k, of the upper
+// triangle into the skewed packed layout, in column order, 32 at a time
+// (pairs[p] = i | k << 8); lanes stay converged and the gathers of 8 pairs
+// are issued together.  Columns from n on are left as they are.
+__device__ __forceinline__ void build_packed(const DevJob &J, const DevPlan &P, double *U, const int4 *nb,
+                                             const int *cs, const uint16_t *pairs, int n, int lane) {
+    const int npairs = n * (n - 1) / 2;
+    for (int p0 = 0; p0 < npairs; p0 += 256) {
+        double v[8];
+        int dst[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int p = p0 + 32 * e + lane;
+            dst[e] = -1;
+            v[e] = 0.0;
+            if (p < npairs) {
+                const int ik = __ldg(pairs + p);
+                const int i = ik & 0xff, k = ik >> 8;
+                v[e] = pair_cov64(J, P, nb[i], nb[k]);
+                dst[e] = cs[k] + i;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            if (dst[e] >= 0) U[dst[e]] = v[e];
+    }
+    __syncwarp();
+}
+
 __device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs,
                                const uint16_t *pairs, int node, int lane, const Node64 &d) {
     const int n = d.n;
     const bool ordinary = J.kind == 0;
     double *U = S.U;
-    // Build: the n(n-1)/2 entries A(i, k) = C(x_i - x_k), i < k, of the upper
-    // triangle in column order, 32 at a time (pairs[p] = i | k << 8); lanes
-    // stay converged and the gathers of 8 pairs are issued together.
-    {
-        const int npairs = n * (n - 1) / 2;
-        for (int p0 = 0; p0 < npairs; p0 += 256) {
-            double v[8];
-            int dst[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int p = p0 + 32 * e + lane;
-                dst[e] = -1;
-                v[e] = 0.0;
-                if (p < npairs) {
-                    const int ik = __ldg(pairs + p);
-                    const int i = ik & 0xff, k = ik >> 8;
-                    v[e] = pair_cov64(J, P, S.nb[i], S.nb[k]);
-                    dst[e] = cs[k] + i;
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < 8; ++e)
-                if (dst[e] >= 0) U[dst[e]] = v[e];
-        }
-    }
-    __syncwarp();
+    build_packed(J, P, U, S.nb, cs, pairs, n, lane);
     const int k0 = lane, k1 = lane + 32;  // the lane's columns in the factorisation
     const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0), the table's centre
     // diagonal slots and pads of the lane's columns are zero until their step
@@ -440,12 +446,271 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, 
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
 
-constexpr size_t SMEM64_EXACT = sizeof(Exact64Smem) * WARPS64_BLOCK;
 
-int grid64_for(const void *fn, size_t smem) {
+// ---------------------------------------------------------------------------
+// Mixed path: FP32 Gauss-Jordan inverse + FP64 refinement.
+
+constexpr float MIXED64_PIVOT_MIN = 1e-3f;  // on the unit-diagonal scaled system
+constexpr int MIXED64_MAX_CORR = 6;
+
+struct Mixed64Smem {
+    double U[U64_SIZE];  // exact FP64 system, skewed packed upper triangle (diagonal = C(0))
+    double xv[2][N64];   // FP64 vectors broadcast for the residuals
+    float row[N64];      // pivot row of the sweep
+    float vf[2][N64];    // FP32 vectors broadcast for the inverse's products
+    int4 nb[N64];
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+__device__ __forceinline__ double warp_sum64(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max64(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
+    return v;
+}
+
+// (y0, y1) = rows lane and lane + 32 of M v with M's diagonal offset removed
+// (the sweep leaves every swept diagonal entry 2 above the sweep operator's
+// value; see the sweep below).
+__device__ __forceinline__ void apply64(const float2 (&m0)[32], const float2 (&m1)[32], float v0, float v1,
+                                        float *buf, int lane, float &y0, float &y1) {
+    buf[lane] = v0;
+    buf[lane + 32] = v1;
+    __syncwarp();
+    float2 a0 = f2(0.f, 0.f), a1 = f2(0.f, 0.f);
+    const float4 *b4 = reinterpret_cast<const float4 *>(buf);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const float4 u = b4[q];
+        a0 = __ffma2_rn(m0[2 * q], f2(u.x, u.y), a0);
+        a1 = __ffma2_rn(m1[2 * q], f2(u.x, u.y), a1);
+        a0 = __ffma2_rn(m0[2 * q + 1], f2(u.z, u.w), a0);
+        a1 = __ffma2_rn(m1[2 * q + 1], f2(u.z, u.w), a1);
+    }
+    __syncwarp();
+    y0 = (a0.x + a0.y) - 2.f * v0;
+    y1 = (a1.x + a1.y) - 2.f * v1;
+}
+
+// Rows lane and lane + 32 of r = b - A x in FP64 for one or two right-hand
+// sides; A from the packed triangle (entries of columns below n only).
+__device__ __forceinline__ void residual64(const Mixed64Smem &S, const int *cs, double a_diag, int n, int lane,
+                                           bool two, double xa0, double xa1, double xb0, double xb1,
+                                           double &ra0, double &ra1, double &rb0, double &rb1) {
+    double *xa = const_cast<double *>(S.xv[0]), *xb = const_cast<double *>(S.xv[1]);
+    xa[lane] = xa0;
+    xa[lane + 32] = xa1;
+    if (two) {
+        xb[lane] = xb0;
+        xb[lane + 32] = xb1;
+    }
+    __syncwarp();
+    const int r0 = lane, r1 = lane + 32;
+    const int cs0 = cs[r0], cs1 = cs[r1];
+    double sa0 = 0.0, sa1 = 0.0, sb0 = 0.0, sb1 = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const int ck = cs[k];
+        const double a = xa[k];
+        const double b = two ? xb[k] : 0.0;
+        // A(r, k): column k at row r above the diagonal, column r at row k below
+        const double e0 = k == r0 ? a_diag : S.U[k > r0 ? ck + r0 : cs0 + k];
+        const double e1 = k == r1 ? a_diag : S.U[k > r1 ? ck + r1 : cs1 + k];
+        sa0 = fma(e0, a, sa0);
+        sa1 = fma(e1, a, sa1);
+        if (two) {
+            sb0 = fma(e0, b, sb0);
+            sb1 = fma(e1, b, sb1);
+        }
+    }
+    __syncwarp();
+    // rows from n on are padding: their residual is zero (their stale
+    // columns must not reach the inverse's products)
+    ra0 = r0 < n ? -sa0 : 0.0;
+    ra1 = r1 < n ? -sa1 : 0.0;
+    rb0 = r0 < n ? -sb0 : 0.0;
+    rb1 = r1 < n ? -sb1 : 0.0;
+}
+
+__global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ int s_cs[N64];
+    const int lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
+    __syncthreads();
+    Mixed64Smem &S = *reinterpret_cast<Mixed64Smem *>(dyn_smem);
+    const int *cs = s_cs;
+    const bool ordinary = J.kind == 0;
+    const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0)
+    const double inv_c0 = 1.0 / P.c0;
+    const int r0 = lane, r1 = lane + 32;
+    const int cs0 = cs[r0], cs1 = cs[r1];
+    for (long long it = blockIdx.x; it < J.size; it += gridDim.x) {
+        const int node = (int)it;
+        if (copy_informed64(J, node, lane)) continue;
+        const Node64 d = load_node64(J, P, S.nb, node, lane);
+        if (d.n <= 0) {
+            write_outputs64(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
+            continue;
+        }
+        const int n = d.n;
+        build_packed(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane);
+        // Rows lane and lane + 32 of the unit-diagonal system A / C(0),
+        // identity beyond n.
+        float2 m0[32], m1[32];
+#pragma unroll
+        for (int c = 0; c < N64; c += 2) {
+            float e[2][2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = h ? r1 : r0, csr = h ? cs1 : cs0;
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const int cc = c + t;
+                    float v;
+                    if (r < n && cc < n) {
+                        const double a = cc == r ? a_diag : S.U[cc > r ? cs[cc] + r : csr + cc];
+                        v = (float)(a * inv_c0);
+                    } else {
+                        v = cc == r ? 1.f : 0.f;
+                    }
+                    e[h][t] = v;
+                }
+            }
+            m0[c / 2] = f2(e[0][0], e[0][1]);
+            m1[c / 2] = f2(e[1][0], e[1][1]);
+        }
+        // Symmetric Gauss-Jordan sweeps over the n live rows: the matrix stays
+        // symmetric, so pivot row p (broadcast by its owner lane) is also
+        // column p and every lane reads its rows' multipliers from it.  The
+        // broadcast entry at p is set to piv - 1, which turns the same fused
+        // update into the sweep's column p (g = m_rp / piv) on every other row
+        // and leaves 2 - 1/piv in place of -1/piv on the pivot itself; swept
+        // diagonal entries are never read again, so the constant offset is
+        // removed when the inverse is applied.  After all sweeps M holds
+        // -(A/C(0))^-1 (+2 on the diagonal).
+        bool low = false;
+        for (int p = 0; p < n; ++p) {
+            const int owner = p & 31;
+            if (lane == owner) {
+                float4 *dst = reinterpret_cast<float4 *>(S.row);
+                if (p < 32) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        dst[q] = make_float4(m0[2 * q].x, m0[2 * q].y, m0[2 * q + 1].x, m0[2 * q + 1].y);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        dst[q] = make_float4(m1[2 * q].x, m1[2 * q].y, m1[2 * q + 1].x, m1[2 * q + 1].y);
+                }
+            }
+            __syncwarp();
+            const float piv = S.row[p];
+            if (!(piv > MIXED64_PIVOT_MIN)) {  // uniform: every lane read the same pivot
+                low = true;
+                break;
+            }
+            const float dinv = __frcp_rn(piv);
+            const float g0 = (S.row[r0] - (r0 == p ? 1.f : 0.f)) * dinv;
+            const float g1 = (S.row[r1] - (r1 == p ? 1.f : 0.f)) * dinv;
+            __syncwarp();
+            if (lane == 0) S.row[p] = piv - 1.f;
+            __syncwarp();
+            const float2 ng0 = f2(-g0, -g0), ng1 = f2(-g1, -g1);
+            const float4 *r4 = reinterpret_cast<const float4 *>(S.row);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const float4 u = r4[q];
+                m0[2 * q] = __ffma2_rn(ng0, f2(u.x, u.y), m0[2 * q]);
+                m1[2 * q] = __ffma2_rn(ng1, f2(u.x, u.y), m1[2 * q]);
+                m0[2 * q + 1] = __ffma2_rn(ng0, f2(u.z, u.w), m0[2 * q + 1]);
+                m1[2 * q + 1] = __ffma2_rn(ng1, f2(u.z, u.w), m1[2 * q + 1]);
+            }
+            __syncwarp();
+        }
+        if (low) {
+            if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+            __syncwarp();
+            continue;
+        }
+        // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
+        // refined with FP64 residuals.
+        const double sc = -inv_c0;
+        const double ba0 = d.b[0], ba1 = d.b[1];
+        const double bb0 = r0 < n ? 1.0 : 0.0, bb1 = r1 < n ? 1.0 : 0.0;
+        float y0, y1;
+        apply64(m0, m1, (float)ba0, (float)ba1, S.vf[0], lane, y0, y1);
+        double xa0 = (double)y0 * sc, xa1 = (double)y1 * sc, xb0 = 0.0, xb1 = 0.0;
+        if (ordinary) {
+            apply64(m0, m1, (float)bb0, (float)bb1, S.vf[1], lane, y0, y1);
+            xb0 = (double)y0 * sc;
+            xb1 = (double)y1 * sc;
+        }
+        RefineGate gate;
+        bool converged = false;
+        for (int corr = 0; corr < MIXED64_MAX_CORR; ++corr) {
+            double ra0, ra1, rb0, rb1;
+            residual64(S, cs, a_diag, n, lane, ordinary, xa0, xa1, xb0, xb1, ra0, ra1, rb0, rb1);
+            ra0 += ba0;
+            ra1 += ba1;
+            apply64(m0, m1, (float)ra0, (float)ra1, S.vf[0], lane, y0, y1);
+            const double da0 = (double)y0 * sc, da1 = (double)y1 * sc;
+            xa0 += da0;
+            xa1 += da1;
+            double dmax = fmax(fabs(da0), fabs(da1)), xmax = fmax(fabs(xa0), fabs(xa1));
+            if (ordinary) {
+                rb0 += bb0;
+                rb1 += bb1;
+                apply64(m0, m1, (float)rb0, (float)rb1, S.vf[1], lane, y0, y1);
+                const double db0 = (double)y0 * sc, db1 = (double)y1 * sc;
+                xb0 += db0;
+                xb1 += db1;
+                dmax = fmax(dmax, fmax(fabs(db0), fabs(db1)));
+                xmax = fmax(xmax, fmax(fabs(xb0), fabs(xb1)));
+            }
+            const int verdict = gate.step(warp_max64(dmax), warp_max64(xmax));
+            if (verdict != 0) {
+                converged = verdict > 0;
+                break;
+            }
+        }
+        if (!converged) {
+            if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+            __syncwarp();
+            continue;
+        }
+        if (r0 >= n) xa0 = xb0 = 0.0;
+        if (r1 >= n) xa1 = xb1 = 0.0;
+        double w0, w1;
+        if (ordinary) {
+            const double mu = (warp_sum64(xa0 + xa1) - 1.0) / warp_sum64(xb0 + xb1);
+            w0 = xa0 - mu * xb0;
+            w1 = xa1 - mu * xb1;
+        } else {
+            w0 = xa0;
+            w1 = xa1;
+        }
+        double variance = -1.0;
+        if (J.variance) {
+            variance = P.c0 - warp_sum64(w0 * d.b[0] + w1 * d.b[1]);
+            if (ordinary) variance -= row_val(w0, w1, n - 1);
+        }
+        write_outputs64(J, P, node, lane, d, ST_SUCCESS, w0, w1, variance);
+        __syncwarp();
+    }
+}
+
+constexpr size_t SMEM64_EXACT = sizeof(Exact64Smem) * WARPS64_BLOCK;
+constexpr size_t SMEM64_MIXED = sizeof(Mixed64Smem);
+
+int grid64_for(const void *fn, size_t smem, int threads) {
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0, dev = 0, sms = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, WARPS64_BLOCK * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return (per_sm < 1 ? 1 : per_sm) * sms;
@@ -456,10 +721,18 @@ int grid64_for(const void *fn, size_t smem) {
 void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
                           long long n_max, cudaStream_t s) {
     if (n_max <= 0) return;
-    static const int grid = grid64_for((const void *)k_solve_exact64, SMEM64_EXACT);
+    static const int grid = grid64_for((const void *)k_solve_exact64, SMEM64_EXACT, WARPS64_BLOCK * 32);
     long long blocks = (n_max + WARPS64_BLOCK - 1) / WARPS64_BLOCK;
     if (blocks > grid) blocks = grid;
     k_solve_exact64<<<(unsigned)blocks, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, node_list, n_list);
+}
+
+void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s) {
+    if (J.size <= 0) return;
+    static const int grid = grid64_for((const void *)k_solve_mixed64, SMEM64_MIXED, 32);
+    long long blocks = J.size;
+    if (blocks > grid) blocks = grid;
+    k_solve_mixed64<<<(unsigned)blocks, 32, SMEM64_MIXED, s>>>(J, P);
 }
 
 }  // namespace hpgl_b200
