@@ -35,11 +35,14 @@ __device__ __forceinline__ double cov_at(const DevPlan &P, int vx, int vy, int v
     return cov_lin(P, vx, vy, vz, vz * P.syx + vy * P.sx + vx, err);
 }
 
-// Node coordinates, sugarbox_grid.cpp:70-74.
-__device__ __forceinline__ void node_xyz(int idx, int nx, int ny, int &x, int &y, int &z) {
-    x = idx % nx;
-    y = idx % (nx * ny) / nx;
-    z = idx / (nx * ny);
+// Node coordinates, sugarbox_grid.cpp:70-74 (x = idx % nx, y = idx % (nx ny) / nx,
+// z = idx / (nx ny)), with the two divisions by multiply-high.
+__device__ __forceinline__ void node_xyz(const DevJob &J, int idx, int &x, int &y, int &z) {
+    const unsigned r = J.div_nx.div((unsigned)idx);
+    const unsigned q = J.div_ny.div(r);
+    x = idx - (int)r * J.nx;
+    y = (int)r - (int)q * J.ny;
+    z = (int)q;
 }
 
 // A node takes the template walk when any of its 27 neighbouring clusterizer
@@ -65,6 +68,19 @@ __device__ __forceinline__ double div_by_rcp(double a, double b, double y) {
     const double r = __fma_rn(-q, b, a);
     return __fma_rn(r, y, q);
 }
+
+// The (row, column) pairs i < k of an upper triangle of up to 64 rows, in
+// column order (i | k << 8): the pairs of an n-row system are the first
+// n(n-1)/2 entries.  Builds walk this list 32 pairs at a time so that every
+// lane gathers the same number of covariances.
+struct PairTable64 {
+    uint16_t v[64 * 63 / 2];
+    constexpr PairTable64() : v() {
+        for (int k = 1, p = 0; k < 64; ++k)
+            for (int i = 0; i < k; ++i) v[p++] = (uint16_t)(i | k << 8);
+    }
+};
+static __device__ const PairTable64 g_pairs64;
 
 // Acceptance of an iterative refinement x <- x + d.  After a correction d_k
 // the remaining error is about rho_k |d_k|, with the contraction rho_k =

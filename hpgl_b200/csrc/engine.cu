@@ -327,6 +327,8 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.nx = job.nx;
     J.ny = job.ny;
     J.nz = job.nz;
+    J.div_nx = FastDiv((unsigned)job.nx);
+    J.div_ny = FastDiv((unsigned)job.ny);
     J.size = S.size;
     J.values = cont ? at<float>(S, A.o_values) : nullptr;
     J.codes = cont ? nullptr : at<uint8_t>(S, A.o_codes);

@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(CLUSTER_WARPS * 32) k_search_cluster(DevJob J,
         const int node = (int)node_l;
         if (!node_needs_kriging(J, node)) continue;
         int x, y, z;
-        node_xyz(node, J.nx, J.ny, x, y, z);
+        node_xyz(J, node, x, y, z);
         if (!node_clean(P, x, y, z)) continue;
         const int cx = (int)(x / P.crx), cy = (int)(y / P.cry), cz = (int)(z / P.crz);
         int n = 0;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(CLUSTER_WARPS * 32) k_search_cluster(DevJob J,
                         if (p < s1) {
                             cand = P.bucket_nodes[p];
                             int qx, qy, qz;
-                            node_xyz(cand, J.nx, J.ny, qx, qy, qz);
+                            node_xyz(J, cand, qx, qy, qz);
                             key = cov_at(P, qx - x, qy - y, qz - z, J.err);
                             keep = key > thr;
                         }

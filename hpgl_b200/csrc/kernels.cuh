@@ -38,9 +38,42 @@ struct DevPlan {
     int max_candidates;
 };
 
+// Division by a runtime-invariant divisor d >= 1 of any n < 2^32 with one
+// multiply-high: t = umulhi(m, n), n / d = (t + ((n - t) >> 1)) >> (l - 1),
+// where l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1 (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994, the variant with the 33-bit multiplier's top bit folded into the
+// add).  d = 1 (l = 0) returns n.  tests/cpp/fastdiv_check.cpp checks it
+// against integer division.
+struct FastDiv {
+    unsigned d = 1, m = 0;
+    int l = 0;
+    FastDiv() = default;
+    explicit FastDiv(unsigned dv) : d(dv) {
+        while ((1ull << l) < dv) ++l;
+        m = (unsigned)((((unsigned long long)1 << 32) * (((unsigned long long)1 << l) - dv)) / dv + 1);
+    }
+#ifdef __CUDACC__
+    __host__ __device__ __forceinline__ unsigned div(unsigned n) const {
+#ifdef __CUDA_ARCH__
+        const unsigned t = __umulhi(m, n);
+#else
+        const unsigned t = (unsigned)(((unsigned long long)m * n) >> 32);
+#endif
+        return l == 0 ? n : (t + ((n - t) >> 1)) >> (l - 1);
+    }
+#else
+    unsigned div(unsigned n) const {
+        const unsigned t = (unsigned)(((unsigned long long)m * n) >> 32);
+        return l == 0 ? n : (t + ((n - t) >> 1)) >> (l - 1);
+    }
+#endif
+};
+
 struct DevJob {
     int kind;
     int nx, ny, nz;
+    FastDiv div_nx, div_ny;  // node index -> (x, y, z)
     long long size;
     const float *values;
     const uint8_t *codes;

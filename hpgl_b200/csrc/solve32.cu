@@ -33,6 +33,7 @@ struct SysSmem {
     double vd[N32];         // double vector broadcast
     float vf[2][N32];       // float vector broadcast
     float row[2][N32];      // mixed: pivot row broadcast (double buffered)
+    int4 nb[N32];           // neighbour offsets from the node (x, y, z, table offset)
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -56,19 +57,46 @@ struct NodeData {
     int ox, oy, oz, lin;  // offset of neighbour `lane` from the node, and its table offset
 };
 
-__device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane) {
+// The first loads of a node, issued one node ahead by the persistent loops
+// (the neighbour count, the lane's neighbour cell and the informed flag start
+// a chain of dependent loads; issuing them while the previous system is
+// solved hides that latency).
+struct NodeFetch {
+    int node;  // -1: past the end
+    int n;
+    int cell;
+    bool informed;
+};
+
+__device__ __forceinline__ NodeFetch fetch_node(const DevJob &J, const DevPlan &P, int node, int lane) {
+    NodeFetch f;
+    f.node = node;
+    f.n = 0;
+    f.cell = 0;
+    f.informed = false;
+    if (node >= 0) {
+        f.n = __ldg(J.nbcount + node);
+        if (lane < P.nmax) f.cell = __ldg(J.nb + (long long)node * P.nmax + lane);
+        f.informed = is_cont(J.kind) && __ldg(J.mask + node) != 0;
+    }
+    return f;
+}
+
+__device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &f,
+                                              int lane) {
     NodeData d;
-    d.n = J.nbcount[node];
+    const int node = f.node;
+    d.n = f.n;
     int x0, y0, z0;
-    node_xyz(node, J.nx, J.ny, x0, y0, z0);
+    node_xyz(J, node, x0, y0, z0);
     d.dv = 0.f;
     d.code = -1;
     d.b = 0.0;
     int ox = 0, oy = 0, oz = 0;
     if (lane < d.n) {
-        const int cell = J.nb[(long long)node * P.nmax + lane];
+        const int cell = f.cell;
         int qx, qy, qz;
-        node_xyz(cell, J.nx, J.ny, qx, qy, qz);
+        node_xyz(J, cell, qx, qy, qz);
         ox = qx - x0;
         oy = qy - y0;
         oz = qz - z0;
@@ -84,41 +112,100 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
     d.oy = oy;
     d.oz = oz;
     d.lin = oz * P.syx + oy * P.sx + ox;
+    S.nb[lane] = make_int4(ox, oy, oz, d.lin);
+    __syncwarp();
     return d;
 }
 
-// A(lane, k) for one column k <= ... : C(x_lane - x_k) (my_kriging_weights.h:53,
-// 160), the identity beyond n.
-__device__ __forceinline__ double pair_cov(const DevJob &J, const DevPlan &P, const NodeData &d, int k, int lane) {
-    const int kx = __shfl_sync(FULL_MASK, d.ox, k), ky = __shfl_sync(FULL_MASK, d.oy, k);
-    const int kz = __shfl_sync(FULL_MASK, d.oz, k), kl = __shfl_sync(FULL_MASK, d.lin, k);
-    if (k >= d.n || lane >= d.n) return lane == k ? 1.0 : 0.0;
-    return cov_lin(P, d.ox - kx, d.oy - ky, d.oz - kz, d.lin - kl, J.err);
-}
-
-// Upper triangle A(i,k), i <= k < n, into S.A at k*LD + i (and the mirror
-// when FULL), identity padding beyond n.
-template <int LD, bool FULL>
-__device__ __forceinline__ void build_system(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeData &d,
-                                             int lane) {
-#pragma unroll 4
-    for (int k = 0; k < N32; ++k) {
-        const int kx = __shfl_sync(FULL_MASK, d.ox, k), ky = __shfl_sync(FULL_MASK, d.oy, k);
-        const int kz = __shfl_sync(FULL_MASK, d.oz, k), kl = __shfl_sync(FULL_MASK, d.lin, k);
-        if (lane <= k) {
-            double v;
-            if (k < d.n) v = cov_lin(P, d.ox - kx, d.oy - ky, d.oz - kz, d.lin - kl, J.err);
-            else v = lane == k ? 1.0 : 0.0;
-            S.A[k * LD + lane] = v;
-            if (FULL) S.A[lane * LD + k] = v;
+// The full symmetric system into S.A (column k at k*33): the n(n-1)/2
+// entries A(i,k) = C(x_i - x_k), i < k (my_kriging_weights.h:49-58,
+// 156-165), gathered 32 pairs at a time with 8 gathers in flight per lane,
+// each stored at (i,k) and (k,i); diagonal C(0); the identity beyond n.
+__device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, SysSmem &S, int n, int lane) {
+    constexpr int LD = 33;
+    const int npairs = n * (n - 1) / 2;
+    for (int p0 = 0; p0 < npairs; p0 += 256) {
+        double v[8];
+        int ik[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int p = p0 + 32 * e + lane;
+            ik[e] = -1;
+            v[e] = 0.0;
+            if (p < npairs) {
+                ik[e] = __ldg(g_pairs64.v + p);
+                const int4 a = S.nb[ik[e] & 0xff], b = S.nb[ik[e] >> 8];
+                v[e] = cov_lin(P, a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, J.err);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            if (ik[e] >= 0) {
+                const int i = ik[e] & 0xff, k = ik[e] >> 8;
+                S.A[k * LD + i] = v[e];
+                S.A[i * LD + k] = v[e];
+            }
+        }
+    }
+    S.A[lane * LD + lane] = lane < n ? __ldg(P.table + P.center) : 1.0;
+    if (lane >= n) {
+        for (int c = 0; c < N32; ++c) {
+            if (c != lane) {
+                S.A[c * LD + lane] = 0.0;
+                S.A[lane * LD + c] = 0.0;
+            }
         }
     }
     __syncwarp();
 }
 
+// init + t_0 + t_1 + ... + t_{n-1} in that order, t_i = `term` of lane i,
+// computed by lane 0 from 16-byte reads of a shared buffer (valid on lane 0).
+__device__ __forceinline__ float seq_fsum(float init, float term, int n, float *buf, int lane) {
+    buf[lane] = term;
+    __syncwarp();
+    float r = init;
+    if (lane == 0) {
+        const float4 *b4 = reinterpret_cast<const float4 *>(buf);
+#pragma unroll
+        for (int q = 0; q < N32 / 4; ++q) {
+            if (4 * q < n) {
+                const float4 v = b4[q];
+                r = __fadd_rn(r, v.x);
+                if (4 * q + 1 < n) r = __fadd_rn(r, v.y);
+                if (4 * q + 2 < n) r = __fadd_rn(r, v.z);
+                if (4 * q + 3 < n) r = __fadd_rn(r, v.w);
+            }
+        }
+    }
+    __syncwarp();
+    return r;
+}
+__device__ __forceinline__ double seq_dsum(double init, double term, int n, double *buf, int lane) {
+    buf[lane] = term;
+    __syncwarp();
+    double r = init;
+    if (lane == 0) {
+        const double2 *b2 = reinterpret_cast<const double2 *>(buf);
+#pragma unroll
+        for (int q = 0; q < N32 / 2; ++q) {
+            if (2 * q < n) {
+                const double2 v = b2[q];
+                r = __dadd_rn(r, v.x);
+                if (2 * q + 1 < n) r = __dadd_rn(r, v.y);
+            }
+        }
+    }
+    __syncwarp();
+    return r;
+}
+
 // Outputs of one solved (or failed) system: weights w (row `lane`), status.
-__device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P, int node, int lane, const NodeData &d,
-                                              int status, double w, double variance) {
+// The estimate sums run on lane 0 in neighbour order (combiner.h:9-24:
+// float terms summed in float; median IK in double), which is also the only
+// lane that stores them.
+__device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane,
+                                              const NodeData &d, int status, double w, double variance) {
     const long long slot = (long long)node * J.status_stride + J.status_offset;
     const bool success = status == ST_SUCCESS;
     const int n = d.n;
@@ -127,10 +214,9 @@ __device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P,
     if (lane == 0) J.status[slot] = (int8_t)status;
     if (is_cont(J.kind)) {
         if (success) {
-            // combine (combiner.h:9-24): float sum in neighbour order.
             const float term = __double2float_rn(__dmul_rn(w, (double)d.dv));
-            float res = J.kind == 1 ? J.sk_mean_f : (J.kind == 2 ? J.mean[node] : 0.f);
-            for (int i = 0; i < n; ++i) res = __fadd_rn(res, __shfl_sync(FULL_MASK, term, i));
+            const float m0 = J.kind == 1 ? J.sk_mean_f : (J.kind == 2 ? J.mean[node] : 0.f);
+            const float res = seq_fsum(m0, term, n, S.vf[0], lane);
             if (lane == 0) {
                 J.out_values[node] = res;
                 J.out_mask[node] = 1;
@@ -152,7 +238,7 @@ __device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P,
             float prob = pk;
             if (success) {
                 const float term = __double2float_rn(__dmul_rn(w, (double)__fsub_rn(d.code == k ? 1.f : 0.f, pk)));
-                for (int i = 0; i < n; ++i) prob = __fadd_rn(prob, __shfl_sync(FULL_MASK, term, i));
+                prob = seq_fsum(pk, term, n, S.vf[0], lane);
             }
             if (lane == 0) J.probs[(long long)node * J.K + k] = prob;
             if (k == J.k0 || (double)prob > best_p) {
@@ -169,7 +255,7 @@ __device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P,
         double prob = (double)m;
         if (success) {
             const double term = __dmul_rn(w, (double)__fsub_rn(d.code == 1 ? 1.f : 0.f, m));
-            for (int i = 0; i < n; ++i) prob = __dadd_rn(prob, __shfl_sync(FULL_MASK, term, i));
+            prob = seq_dsum(prob, term, n, S.vd, lane);
         }
         if (lane == 0) {
             J.probs[node] = (float)prob;
@@ -179,8 +265,9 @@ __device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P,
     }
 }
 
-__device__ __forceinline__ bool copy_informed(const DevJob &J, int node, int lane) {
-    if (is_cont(J.kind) && J.mask[node]) {
+__device__ __forceinline__ bool copy_informed(const DevJob &J, const NodeFetch &f, int lane) {
+    const int node = f.node;
+    if (f.informed) {
         if (lane == 0) {
             J.out_values[node] = J.values[node];
             J.out_mask[node] = 1;
@@ -189,13 +276,6 @@ __device__ __forceinline__ bool copy_informed(const DevJob &J, int node, int lan
         return true;
     }
     return false;
-}
-
-// Sequential sums of the reference (SumSK, SumOnes, variance) over rows.
-__device__ __forceinline__ double seq_sum(double v, int n) {
-    double s = 0.0;
-    for (int i = 0; i < n; ++i) s = __dadd_rn(s, __shfl_sync(FULL_MASK, v, i));
-    return s;
 }
 
 // ---------------------------------------------------------------------------
@@ -311,8 +391,8 @@ __device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, 
             }
         }
         if (ordinary) {
-            const double ssk = seq_sum(lane < n ? xa : 0.0, n);
-            const double son = seq_sum(lane < n ? xb : 0.0, n);
+            const double ssk = __shfl_sync(FULL_MASK, seq_dsum(0.0, lane < n ? xa : 0.0, n, S.vd, lane), 0);
+            const double son = __shfl_sync(FULL_MASK, seq_dsum(0.0, lane < n ? xb : 0.0, n, S.vd, lane), 0);
             const double mu = __ddiv_rn(__dsub_rn(ssk, 1.0), son);
             w = __dsub_rn(xa, __dmul_rn(mu, xb));
         } else {
@@ -321,13 +401,12 @@ __device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, 
     }
     double variance = -1.0;
     if (J.variance && status == ST_SUCCESS) {
-        double v = P.c0;
-        const double p = __dmul_rn(w, d.b);
-        for (int i = 0; i < n; ++i) v = __dsub_rn(v, __shfl_sync(FULL_MASK, p, i));
+        // c0 - p_0 - p_1 - ... (my_kriging_weights.h): subtracting p is adding -p
+        double v = seq_dsum(P.c0, -__dmul_rn(w, d.b), n, S.vd, lane);
         if (ordinary) v = __dsub_rn(v, __shfl_sync(FULL_MASK, w, n - 1));
         variance = v;
     }
-    write_outputs(J, P, node, lane, d, status, w, variance);
+    write_outputs(J, P, S, node, lane, d, status, w, variance);
 }
 
 __global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPlan P, const int *list, const int *n_list) {
@@ -335,18 +414,25 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPla
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
     const long long count = list ? (long long)*n_list : J.size;
+    const long long stride = (long long)gridDim.x * WARPS32;
     unsigned long long solved = 0;
-    for (long long it = (long long)blockIdx.x * WARPS32 + warp; it < count; it += (long long)gridDim.x * WARPS32) {
-        const int node = list ? list[it] : (int)it;
-        if (copy_informed(J, node, lane)) continue;
-        const NodeData d = load_node(J, P, S, node, lane);
-        if (d.n <= 0) {
-            write_outputs(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
-            continue;
+    long long it = (long long)blockIdx.x * WARPS32 + warp;
+    NodeFetch cur = fetch_node(J, P, it < count ? (list ? list[it] : (int)it) : -1, lane);
+    for (; it < count; it += stride) {
+        const long long nx = it + stride;
+        const NodeFetch next = fetch_node(J, P, nx < count ? (list ? list[nx] : (int)nx) : -1, lane);
+        const int node = cur.node;
+        if (!copy_informed(J, cur, lane)) {
+            const NodeData d = load_node(J, P, S, cur, lane);
+            if (d.n <= 0) {
+                write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
+            } else {
+                exact_system(J, P, S, node, lane, d);
+                ++solved;
+            }
         }
-        exact_system(J, P, S, node, lane, d);
-        ++solved;
         __syncwarp();
+        cur = next;
     }
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
@@ -399,16 +485,21 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
     const bool ordinary = J.kind == 0;
     const double inv_c0 = 1.0 / P.c0;
-    for (long long it = (long long)blockIdx.x * WARPS32 + warp; it < J.size; it += (long long)gridDim.x * WARPS32) {
-        const int node = (int)it;
-        if (copy_informed(J, node, lane)) continue;
-        const NodeData d = load_node(J, P, S, node, lane);
+    const long long stride = (long long)gridDim.x * WARPS32;
+    long long it = (long long)blockIdx.x * WARPS32 + warp;
+    NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+    for (; it < J.size; it += stride) {
+        const NodeFetch cur = next;
+        next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
+        const int node = cur.node;
+        if (copy_informed(J, cur, lane)) continue;
+        const NodeData d = load_node(J, P, S, cur, lane);
         if (d.n <= 0) {
-            write_outputs(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
+            write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
             continue;
         }
         const int n = d.n;
-        build_system<33, true>(J, P, S, d, lane);
+        build_full32(J, P, S, n, lane);
         // Row `lane` of the unit-diagonal system A / C(0) (identity padding).
         float2 m2[N32 / 2];
 #pragma unroll
@@ -428,7 +519,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
             __syncwarp();
             const float piv = rb[p];
             low |= !(piv > MIXED_PIVOT_MIN);
-            const float dinv = __frcp_rn(piv);
+            const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
             const float isp = lane == p ? 1.f : 0.f;
             const float g = (mp - isp) * dinv;
             const float2 ng = f2(-g, -g);
@@ -500,7 +591,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
             variance = P.c0 - warp_sum(w * d.b);
             if (ordinary) variance -= __shfl_sync(FULL_MASK, w, n - 1);
         }
-        write_outputs(J, P, node, lane, d, ST_SUCCESS, w, variance);
+        write_outputs(J, P, S, node, lane, d, ST_SUCCESS, w, variance);
         __syncwarp();
     }
 }

@@ -43,16 +43,6 @@ __host__ __device__ constexpr int col_start_c(int k) {
 constexpr int U64_SIZE = col_start_c(N64 - 1) + N64;  // 2558 doubles
 static_assert(col_start_c(3) == 22 && U64_SIZE == 2558, "skewed layout");
 
-// The upper triangle's (row, column) pairs in column order, i | k << 8.
-struct PairTable64 {
-    uint16_t v[N64 * (N64 - 1) / 2];
-    constexpr PairTable64() : v() {
-        for (int k = 1, p = 0; k < N64; ++k)
-            for (int i = 0; i < k; ++i) v[p++] = (uint16_t)(i | k << 8);
-    }
-};
-__device__ const PairTable64 g_pairs64;
-
 struct Exact64Smem {
     double U[U64_SIZE];
     int4 nb[N64];     // neighbour offsets from the node (x, y, z, table offset)
@@ -72,7 +62,7 @@ __device__ __forceinline__ Node64 load_node64(const DevJob &J, const DevPlan &P,
     Node64 d;
     d.n = J.nbcount[node];
     int x0, y0, z0;
-    node_xyz(node, J.nx, J.ny, x0, y0, z0);
+    node_xyz(J, node, x0, y0, z0);
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         const int row = lane + 32 * r;
@@ -83,7 +73,7 @@ __device__ __forceinline__ Node64 load_node64(const DevJob &J, const DevPlan &P,
         if (row < d.n) {
             const int cell = J.nb[(long long)node * P.nmax + row];
             int qx, qy, qz;
-            node_xyz(cell, J.nx, J.ny, qx, qy, qz);
+            node_xyz(J, cell, qx, qy, qz);
             o.x = qx - x0;
             o.y = qy - y0;
             o.z = qz - z0;
@@ -614,7 +604,7 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
                 low = true;
                 break;
             }
-            const float dinv = __frcp_rn(piv);
+            const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
             const float g0 = (S.row[r0] - (r0 == p ? 1.f : 0.f)) * dinv;
             const float g1 = (S.row[r1] - (r1 == p ? 1.f : 0.f)) * dinv;
             __syncwarp();

@@ -152,16 +152,18 @@ def lvm_512x512x32(shape=(512, 512, 32), seed=4, blobs=200, sigma=3.0):
     return dict(name="lvm_512x512x32", kind="lvm", shape=shape, values=values, mask=mask, mean=mean, params=[p])
 
 
-# Search radius = the variogram range along each axis (rounded up), the usual
-# choice of a kriging search ellipsoid.
-_RADIUS_FACTOR = {SPHERICAL: 1.0, EXPONENTIAL: 1.0, GAUSSIAN: 1.0}
+# Search radius = the extent along each axis where the model's covariance
+# falls to 1 % of C(0), rounded up: f * range with f = 1.0 (spherical, zero at
+# the range), 1.54 (exponential, exp(-3h/a) = 0.01) and 1.24 (Gaussian,
+# exp(-3(h/a)^2) = 0.01) -- the extent of the reference's search template.
+_RADIUS_FACTOR = {SPHERICAL: 1.0, EXPONENTIAL: 1.54, GAUSSIAN: 1.24}
 
 
 def serve_job(rng, job_id=0, max_cells=256 * 256 * 64):
     """One job of the serving stream: grid log-uniform between 32^3 and
     256x256x64 cells, informed fraction 0.5-3 %, variogram type uniform over
     spherical/exponential/Gaussian, ranges 5-60, nugget 0-0.1, 8-64
-    neighbours, search radii = the ranges (rounded up); kind 50 % OK, 25 % SK,
+    neighbours, search radii = the 1 % covariance extents (rounded up); kind 50 % OK, 25 % SK,
     25 % 4-category IK."""
     lo, hi = math.log(min(32 ** 3, max_cells)), math.log(max_cells)
     cells = math.exp(rng.uniform(lo, hi))
