@@ -210,6 +210,13 @@ def main():
     flops = algorithmic_flops(nbc, rhs=1)
     del dump
 
+    # Launch autotuning (our own tuner: fused vs separate search/solve and
+    # persistent blocks per SM), untimed.
+    tuning = {}
+    for prec in ("mixed", "fp64"):
+        t = N.autotune(job, precision=prec)
+        tuning[prec] = dict(t["chosen"], candidates=len(t["candidates"]))
+
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
@@ -243,7 +250,7 @@ def main():
     achieved = flops / (info_m["ms_top_kernel"] / 1000.0) / 1e12
     traffic = None
     try:
-        tj = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["k_solve_mixed32"]
+        tj = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[info_m["top_kernel"]]
         # measured on the 128x128x32 cube; DRAM traffic scales with the systems
         traffic = tj["dram_bytes_per_launch_128x128x32"] * kriged / tj["systems_128x128x32"]
     except (OSError, KeyError, ValueError):
@@ -282,7 +289,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": list(job["shape"]), "kriged_nodes_per_step": kriged,
                        "precision": "fp32 factorisation + fp64 refinement, fp64 re-solve of routed systems",
-                       "l2": "256 MiB written between steps", "parallelism": "replicas%d" % world},
+                       "l2": "256 MiB written between steps", "parallelism": "replicas%d" % world,
+                       "launch": tuning, "pass": "one CUDA graph per step"},
             "fp64": {"value": fp64_value, "ms_per_step": t_fp64 / args.steps,
                      "top_kernel_ms": info_f["ms_top_kernel"]},
             "mixed_vs_fp64": value / fp64_value,

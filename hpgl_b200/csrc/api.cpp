@@ -10,6 +10,7 @@
 
 #include "../../include/hpgl.h"
 #include "engine.h"
+#include "kernels.cuh"
 #include "plan.h"
 
 using namespace hpgl_b200;
@@ -275,6 +276,25 @@ int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl
         if (!job || !result || !bench) throw HpglError{HPGL_E_INVALID, "null argument"};
         if (bench->iters < 1 || bench->warmup < 0) throw HpglError{HPGL_E_INVALID, "iters must be >= 1"};
         bench_job(*job, *result, *bench);
+    });
+}
+
+int hpgl_b200_set_launch(int family, int precision, int schedule, int blocks_per_sm) {
+    return guarded("hpgl_b200_set_launch", [&] {
+        if (family < 0 || family > 1 || precision < 0 || precision > 1 || schedule < 0 || schedule > 1 ||
+            blocks_per_sm < 0)
+            throw HpglError{HPGL_E_INVALID, "invalid launch setting"};
+        LaunchTuning t;
+        t.schedule = schedule;
+        t.blocks_per_sm = blocks_per_sm;
+        tuning_set(family, precision, t);
+    });
+}
+
+int hpgl_b200_autotune(const hpgl_b200_job_t *job, hpgl_b200_tune_t *report) {
+    return guarded("hpgl_b200_autotune", [&] {
+        if (!job || !report) throw HpglError{HPGL_E_INVALID, "null argument"};
+        autotune_job(*job, *report);
     });
 }
 

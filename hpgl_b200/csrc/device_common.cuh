@@ -69,6 +69,35 @@ __device__ __forceinline__ double div_by_rcp(double a, double b, double y) {
     return __fma_rn(r, y, q);
 }
 
+// The first loads of a node, issued one node ahead by the persistent loops
+// (the neighbour count, the lane's neighbour cells -- rows lane and lane + 32
+// -- and the informed flag start a chain of dependent loads; issuing them
+// while the previous system is solved hides that latency).  Plain loads: the
+// fused kernels read lists their own warp has just written.
+struct NodeFetch {
+    int node;  // -1: past the end
+    int n;
+    int cell, cell2;
+    bool informed;
+};
+
+__device__ __forceinline__ NodeFetch fetch_node(const DevJob &J, const DevPlan &P, int node, int lane) {
+    NodeFetch f;
+    f.node = node;
+    f.n = 0;
+    f.cell = 0;
+    f.cell2 = 0;
+    f.informed = false;
+    if (node >= 0) {
+        f.n = J.nbcount[node];
+        const int *lst = J.nb + (long long)node * P.nmax;
+        if (lane < P.nmax) f.cell = lst[lane];
+        if (lane + 32 < P.nmax) f.cell2 = lst[lane + 32];
+        f.informed = is_cont(J.kind) && __ldg(J.mask + node) != 0;
+    }
+    return f;
+}
+
 // The (row, column) pairs i < k of an upper triangle of up to 64 rows, in
 // column order (i | k << 8): the pairs of an n-row system are the first
 // n(n-1)/2 entries.  Builds walk this list 32 pairs at a time so that every

@@ -369,7 +369,10 @@ struct PassTiming {
     int launches = 0;
 };
 
-// One device pass over all groups: bits, searches, solve(s), argmax.
+// One device pass over all groups: bits, searches, solve(s), argmax.  The
+// per-node kernels follow the launch tuning of the group's family: either
+// the template search then the solve, or the clusterizer search then the
+// fused search+solve kernel.
 static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
                         const std::function<void(const Group &)> &after_group) {
     const Arena &A = S.ar;
@@ -379,21 +382,31 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
     for (size_t gi = 0; gi < S.groups.size(); ++gi) {
         Group &g = S.groups[gi];
         DevJob J = make_devjob(S, g);
+        const LaunchTuning tune = tuning_get(tuning_family(g.plan.nmax), S.precision);
+        const LaunchTuning tune64 = tuning_get(tuning_family(g.plan.nmax), HPGL_PRECISION_FP64);
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->search0, s));
         CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
         launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
-        launch_search_template(J, g.dp, s);
-        launches += 2;
+        ++launches;
+        if (tune.schedule == SCHED_SPLIT) {
+            launch_search_template(J, g.dp, s);
+            ++launches;
+        }
         if (g.plan.any_clean) {
             launch_search_cluster(J, g.dp, at<double>(S, A.o_skey), at<int>(S, A.o_sidx), (int)A.cluster_warps, s);
             ++launches;
         }
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top0, s));
-        launch_solve(J, g.dp, S.precision, nullptr, nullptr, 0, s);
+        if (tune.schedule == SCHED_FUSED) {
+            if (g.plan.nmax <= 32) launch_fused32(J, g.dp, S.precision, s, tune.blocks_per_sm);
+            else launch_fused64(J, g.dp, S.precision, s, tune.blocks_per_sm);
+        } else {
+            launch_solve(J, g.dp, S.precision, nullptr, nullptr, 0, s, tune.blocks_per_sm);
+        }
         ++launches;
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top1, s));
         if (S.precision == HPGL_PRECISION_MIXED) {
-            launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, J.n_routed, (int)S.size, s);
+            launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, J.n_routed, (int)S.size, s, tune64.blocks_per_sm);
             ++launches;
         }
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->resolve1, s));
@@ -543,6 +556,33 @@ void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     res.ms_total = ms_since(t0);
 }
 
+static const char *top_kernel_name(int nmax, int precision, int schedule) {
+    if (schedule == SCHED_FUSED) {
+        if (nmax <= 32) return precision ? "k_fused32<1>" : "k_fused32<0>";
+        return precision ? "k_fused64<1>" : "k_fused64<0>";
+    }
+    if (nmax <= 32) return precision ? "k_solve_mixed32" : "k_solve_exact32";
+    return precision ? "k_solve_mixed64" : "k_solve_exact64";
+}
+
+// The job's device pass captured once as a CUDA graph and replayed for every
+// timed iteration: one launch per pass instead of one per kernel and memset.
+struct PassGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~PassGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+static void capture_pass(JobState &S, cudaStream_t s, PassGraph &G) {
+    CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    device_pass(S, s, nullptr, nullptr);
+    CUDA_CHECK(cudaStreamEndCapture(s, &G.graph));
+    CUDA_CHECK(cudaGraphInstantiate(&G.exec, G.graph, 0));
+}
+
 void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_bench_t &bench) {
     auto t0 = std::chrono::steady_clock::now();
     JobState S;
@@ -569,33 +609,45 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     cudaEvent_t e0, e1;
     CUDA_CHECK(cudaEventCreate(&e0));
     CUDA_CHECK(cudaEventCreate(&e1));
+    // Phase times from eager passes (events between the launches), then the
+    // timed iterations as graph replays.
     double top_sum = 0, search_sum = 0, resolve_sum = 0;
+    const int phase_runs = std::max(1, std::min(bench.iters, 3));
+    for (int it = 0; it < 1 + phase_runs; ++it) {
+        if (bench.flush_bytes > 0)
+            CUDA_CHECK(cudaMemsetAsync(C.flush, it & 0xff, (size_t)bench.flush_bytes, C.stream));
+        device_pass(S, C.stream, &pt, nullptr);
+        read_counters(S, C.stream);
+        if (it == 0) continue;  // first use of every kernel
+        float tms = 0, sms = 0, rms = 0;
+        cudaEventElapsedTime(&tms, pt.top0, pt.top1);
+        cudaEventElapsedTime(&sms, pt.search0, pt.top0);
+        cudaEventElapsedTime(&rms, pt.top1, pt.resolve1);
+        top_sum += tms;
+        search_sum += sms;
+        resolve_sum += rms;
+    }
+    PassGraph G;
+    capture_pass(S, C.stream, G);
     Counters cnt{};
     for (int it = 0; it < bench.warmup + bench.iters; ++it) {
         if (bench.flush_bytes > 0)
             CUDA_CHECK(cudaMemsetAsync(C.flush, it & 0xff, (size_t)bench.flush_bytes, C.stream));
         CUDA_CHECK(cudaEventRecord(e0, C.stream));
-        device_pass(S, C.stream, &pt, nullptr);
+        CUDA_CHECK(cudaGraphLaunch(G.exec, C.stream));
         CUDA_CHECK(cudaEventRecord(e1, C.stream));
         cnt = read_counters(S, C.stream);
         if (it >= bench.warmup) {
-            float ms = 0, tms = 0, sms = 0, rms = 0;
+            float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
-            cudaEventElapsedTime(&tms, pt.top0, pt.top1);
-            cudaEventElapsedTime(&sms, pt.search0, pt.top0);
-            cudaEventElapsedTime(&rms, pt.top1, pt.resolve1);
             if (bench.ms_per_iter) bench.ms_per_iter[it - bench.warmup] = ms;
-            top_sum += tms;
-            search_sum += sms;
-            resolve_sum += rms;
         }
     }
-    bench.ms_top_kernel = bench.iters > 0 ? top_sum / bench.iters : 0;
-    bench.ms_search = bench.iters > 0 ? search_sum / bench.iters : 0;
-    bench.ms_resolve = bench.iters > 0 ? resolve_sum / bench.iters : 0;
+    bench.ms_top_kernel = top_sum / phase_runs;
+    bench.ms_search = search_sum / phase_runs;
+    bench.ms_resolve = resolve_sum / phase_runs;
     snprintf(bench.top_kernel, sizeof(bench.top_kernel), "%s",
-             S.nmax_all <= 32 ? (S.precision ? "k_solve_mixed32" : "k_solve_exact32")
-                              : (S.precision ? "k_solve_mixed64" : "k_solve_exact64"));
+             top_kernel_name(S.nmax_all, S.precision, tuning_get(tuning_family(S.nmax_all), S.precision).schedule));
     bench.launches_per_iter = pt.launches;
     cudaEventDestroy(pt.search0);
     cudaEventDestroy(pt.top0);
@@ -606,6 +658,97 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     download(S, res, cnt, C.stream);
     bench.systems = res.systems;
     bench.systems_fp64 = res.systems_fp64;
+}
+
+// Autotuner: times the job's device pass (after an L2 flush, median of
+// three) under each candidate launch setting of the job's family and
+// precision -- separate or fused schedule, persistent blocks per SM from
+// "as many as fit" down -- and keeps the fastest in the tuning table, which
+// every later pass of that family and precision uses.
+void autotune_job(const hpgl_b200_job_t &job, hpgl_b200_tune_t &rep) {
+    hpgl_b200_result_t res;
+    memset(&res, 0, sizeof(res));
+    std::vector<float> outv;
+    std::vector<uint8_t> outc, outm;
+    const size_t size = (size_t)job.nx * job.ny * job.nz;
+    outm.assign(job.mask, job.mask + size);
+    if (job.kind <= KIND_LVM) {
+        outv.assign(job.values, job.values + size);
+        res.out_values = outv.data();
+    } else {
+        outc.assign(job.codes, job.codes + size);
+        res.out_codes = outc.data();
+    }
+    res.out_mask = outm.data();
+    JobState S;
+    prepare(S, job, res);
+    std::lock_guard<std::mutex> lock(g_sync_mutex);
+    SyncContext &C = sync_ctx();
+    sync_arena(C, S.ar.total);
+    S.base = C.arena;
+    upload(S, C.stream);
+    const size_t flush = 256u << 20;
+    if (C.flush_cap < flush) {
+        if (C.flush) cudaFree(C.flush);
+        C.flush = nullptr;
+        C.flush_cap = 0;
+        CUDA_CHECK(cudaMalloc(&C.flush, flush));
+        C.flush_cap = flush;
+    }
+    const int family = tuning_family(S.nmax_all), precision = S.precision;
+    const LaunchTuning before = tuning_get(family, precision);
+    const int sched[] = {SCHED_FUSED, SCHED_SPLIT};
+    const int bps[] = {0, 4, 3, 2};
+    cudaEvent_t e0, e1;
+    CUDA_CHECK(cudaEventCreate(&e0));
+    CUDA_CHECK(cudaEventCreate(&e1));
+    rep.candidates = 0;
+    rep.chosen = -1;
+    double best = 1e300;
+    try {
+        for (int sc : sched) {
+            for (int b : bps) {
+                if (rep.candidates >= HPGL_B200_TUNE_MAX) break;
+                LaunchTuning t;
+                t.schedule = sc;
+                t.blocks_per_sm = b;
+                tuning_set(family, precision, t);
+                device_pass(S, C.stream, nullptr, nullptr);  // warm-up
+                read_counters(S, C.stream);
+                float runs[3];
+                for (float &r : runs) {
+                    CUDA_CHECK(cudaMemsetAsync(C.flush, 0, flush, C.stream));
+                    CUDA_CHECK(cudaEventRecord(e0, C.stream));
+                    device_pass(S, C.stream, nullptr, nullptr);
+                    CUDA_CHECK(cudaEventRecord(e1, C.stream));
+                    read_counters(S, C.stream);
+                    cudaEventElapsedTime(&r, e0, e1);
+                }
+                std::sort(runs, runs + 3);
+                const int i = rep.candidates++;
+                rep.schedule[i] = sc;
+                rep.blocks_per_sm[i] = b;
+                rep.ms[i] = runs[1];
+                if (runs[1] < best) {
+                    best = runs[1];
+                    rep.chosen = i;
+                }
+            }
+        }
+    } catch (...) {
+        tuning_set(family, precision, before);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    LaunchTuning t;
+    t.schedule = rep.schedule[rep.chosen];
+    t.blocks_per_sm = rep.blocks_per_sm[rep.chosen];
+    tuning_set(family, precision, t);
+    rep.family = family;
+    rep.precision = precision;
 }
 
 // ---- server: continuous batching ----------------------------------------------

@@ -19,6 +19,9 @@ void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res);
 // Device-resident timing (see hpgl_b200_bench in include/hpgl.h).
 void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_bench_t &bench);
 
+// Autotuner of the per-node kernels' launch setting (see hpgl_b200_autotune).
+void autotune_job(const hpgl_b200_job_t &job, hpgl_b200_tune_t &report);
+
 // Simple-kriging weights of one point (sk_weights.cu).
 void sk_weights_alloc(const float *center, const float *xs, const float *ys, const float *zs, int n,
                       const hpgl_cov_params_t *p, float *weights);

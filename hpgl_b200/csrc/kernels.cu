@@ -8,9 +8,12 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <map>
+#include <mutex>
 
 #include "device_common.cuh"
 #include "introsort.h"
+#include "search_common.cuh"
 #include "kernels.cuh"
 
 namespace hpgl_b200 {
@@ -34,75 +37,15 @@ __global__ void k_build_bits(DevJob J, DevPlan P, uint32_t *bits) {
 }
 
 // ---------------------------------------------------------------------------
-// Template search (neighbour_lookup_t::find, sugarbox_neighbour_lookup.h:35-61).
-// One warp per 32-node x-segment of a grid row walks the sorted template 32
-// entries at a time: lane t loads entry base+t and forms the 32-bit window of
-// informed flags of the segment's 32 target cells at that offset (one
-// funnel shift of two words of bit row (y+dy, z+dz); out-of-grid cells are 0
-// bits, matching is_informed(-1) == false).  A 32x32 bit transpose across
-// the lanes turns the windows into, for node b (lane b), the mask of chunk
-// entries that hit it; lane b appends them in template order until it holds
-// max_neighbours.  Nodes that do not take the template path (clean
-// clusterizer neighbourhoods) or need no kriging never become active.
-__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
-    const uint32_t lo_masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
-#pragma unroll
-    for (int st = 0; st < 5; ++st) {
-        const int j = 16 >> st;
-        const uint32_t m = lo_masks[st];
-        const uint32_t y = __shfl_xor_sync(FULL_MASK, x, j);
-        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y & m) << j));
-    }
-    return x;
-}
-
+// Template search: one warp per 32-node x-segment (template_segment in
+// search_common.cuh), persistent over the segments.
 __global__ void __launch_bounds__(256) k_search_template(DevJob J, DevPlan P) {
     __shared__ int delta_sm[8][32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long total = (long long)P.nseg * J.ny * J.nz;
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    int *dsm = delta_sm[wib];
-    for (long long segi = (long long)blockIdx.x * (blockDim.x >> 5) + wib; segi < total; segi += nwarps) {
-        const int seg = (int)(segi % P.nseg);
-        const long long row = segi / P.nseg;
-        const int y = (int)(row % J.ny), z = (int)(row / J.ny);
-        const int x0 = seg * 32;
-        const int base = (int)(row * J.nx) + x0;
-        const int node = base + lane;
-        const bool act = x0 + lane < J.nx && node_needs_kriging(J, node) && !node_clean(P, x0 + lane, y, z);
-        uint32_t active = __ballot_sync(FULL_MASK, act);
-        if (!active) continue;
-        const int nmax = P.nmax;
-        int cnt = 0;
-        int *out = J.nb + (long long)node * nmax;
-        const uint32_t *bits = J.bits;
-        for (int tb = 0; tb < P.tmpl_len && active; tb += 32) {
-            const int t = tb + lane;
-            uint32_t w = 0;
-            int delta = 0;
-            if (t < P.tmpl_len) {
-                const int4 e = __ldg(&P.tmpl[t]);
-                delta = e.w;
-                const int yy = y + e.y, zz = z + e.z;
-                if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
-                    const uint32_t *rp = bits + ((long long)zz * J.ny + yy) * P.wpr + seg + (e.x >> 5);
-                    w = __funnelshift_r(__ldg(rp), __ldg(rp + 1), e.x & 31);
-                }
-            }
-            w &= active;
-            dsm[lane] = delta;
-            uint32_t hits = transpose32(w, lane);
-            __syncwarp();
-            while (hits && cnt < nmax) {
-                const int tt = __ffs(hits) - 1;
-                hits &= hits - 1;
-                out[cnt++] = node + dsm[tt];
-            }
-            __syncwarp();
-            active = __ballot_sync(FULL_MASK, act && cnt < nmax);
-        }
-        if (act) J.nbcount[node] = cnt;
-    }
+    for (long long segi = (long long)blockIdx.x * (blockDim.x >> 5) + wib; segi < total; segi += nwarps)
+        template_segment(J, P, segi, lane, delta_sm[wib]);
 }
 
 // ---------------------------------------------------------------------------
@@ -354,15 +297,51 @@ void launch_search_cluster(const DevJob &J, const DevPlan &P, double *sk, int *s
 }
 
 void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                  int n_list_max, cudaStream_t s) {
+                  int n_list_max, cudaStream_t s, int blocks_per_sm) {
     long long n_max = node_list ? (long long)n_list_max : J.size;
     if (n_max <= 0) return;
     if (P.nmax <= 32) {
-        launch_solve32(J, P, precision, node_list, n_list, n_max, s);
+        launch_solve32(J, P, precision, node_list, n_list, n_max, s, blocks_per_sm);
         return;
     }
-    if (precision == 0 || node_list) launch_solve64_exact(J, P, node_list, n_list, n_max, s);
-    else launch_solve64_mixed(J, P, s);
+    if (precision == 0 || node_list) launch_solve64_exact(J, P, node_list, n_list, n_max, s, blocks_per_sm);
+    else launch_solve64_mixed(J, P, s, blocks_per_sm);
+}
+
+long long persistent_grid(const void *fn, int threads, size_t smem, int blocks_per_sm, long long units) {
+    // occupancy of each kernel is looked up once
+    static std::mutex mu;
+    static std::map<const void *, int> occ;
+    int per_sm;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = occ.find(fn);
+        if (it == occ.end()) {
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            int v = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, fn, threads, smem);
+            it = occ.emplace(fn, v < 1 ? 1 : v).first;
+        }
+        per_sm = it->second;
+    }
+    if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+    const long long cap = (long long)per_sm * sm_count();
+    return std::max<long long>(1, std::min(units, cap));
+}
+
+namespace {
+std::mutex g_tuning_mu;
+LaunchTuning g_tuning[2][2];
+}  // namespace
+
+LaunchTuning tuning_get(int family, int precision) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    return g_tuning[family & 1][precision & 1];
+}
+
+void tuning_set(int family, int precision, const LaunchTuning &t) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    g_tuning[family & 1][precision & 1] = t;
 }
 
 void launch_ik_argmax(const DevJob &J, cudaStream_t s) {

@@ -109,6 +109,22 @@ struct DevJob {
     int *err;
 };
 
+// Launch tuning of the per-node kernels: the schedule (separate template
+// search and solve, or the fused kernel) and the number of persistent blocks
+// per SM (0 = as many as fit).  One setting per (family, precision), family
+// 0 for max_neighbours <= 32 and 1 above; the autotuner (engine.cu) fills
+// the table, the launchers read it.
+enum Schedule : int { SCHED_SPLIT = 0, SCHED_FUSED = 1 };
+struct LaunchTuning {
+    int schedule = SCHED_SPLIT;
+    int blocks_per_sm = 0;
+};
+LaunchTuning tuning_get(int family, int precision);
+void tuning_set(int family, int precision, const LaunchTuning &t);
+inline int tuning_family(int nmax) { return nmax <= 32 ? 0 : 1; }
+// grid for a persistent kernel: min(units, SMs x min(blocks_per_sm, occupancy))
+long long persistent_grid(const void *fn, int threads, size_t smem, int blocks_per_sm, long long units);
+
 // Launchers (stream-ordered, no synchronisation).
 void launch_build_bits(const DevJob &J, const DevPlan &P, uint32_t *bits, cudaStream_t s);
 void launch_search_template(const DevJob &J, const DevPlan &P, cudaStream_t s);
@@ -117,15 +133,19 @@ void launch_search_cluster(const DevJob &J, const DevPlan &P, double *scratch_ke
 // precision: 0 exact FP64, 1 FP32 + FP64 refinement (routes to `routed`).
 // node_list: optional list of nodes (routed re-solve); else every node.
 void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                  int n_list_max, cudaStream_t s);
+                  int n_list_max, cudaStream_t s, int blocks_per_sm = 0);
 void launch_ik_argmax(const DevJob &J, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                    long long n_max, cudaStream_t s);
+                    long long n_max, cudaStream_t s, int blocks_per_sm);
 // solve64.cu: solves for 33..64 neighbours (exact FP64; FP32 inverse + FP64
 // refinement, routing to `routed`)
 void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
-                          long long n_max, cudaStream_t s);
-void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s);
+                          long long n_max, cudaStream_t s, int blocks_per_sm);
+void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s, int blocks_per_sm);
+// Fused template search + solve of every node (the clusterizer search runs
+// first); precision 0 exact FP64, 1 mixed.
+void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm);
+void launch_fused64(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm);
 
 }  // namespace hpgl_b200

@@ -1,0 +1,76 @@
+// Template search of one 32-node x-segment, shared by the search kernel and
+// the fused search+solve kernels.
+#pragma once
+#include "device_common.cuh"
+
+namespace hpgl_b200 {
+
+// neighbour_lookup_t::find (sugarbox_neighbour_lookup.h:35-61) for the 32
+// nodes of segment `segi` (grid row (y, z), x in [32 seg, 32 seg + 32)): the
+// warp walks the sorted template 32 entries at a time; lane t loads entry
+// base+t and forms the 32-bit window of informed flags of the segment's 32
+// target cells at that offset (one funnel shift of two words of bit row
+// (y+dy, z+dz); out-of-grid cells are 0 bits, matching is_informed(-1) ==
+// false).  A 32x32 bit transpose across the lanes turns the windows into, for
+// node b (lane b), the mask of chunk entries that hit it; lane b appends them
+// in template order until it holds max_neighbours.  Nodes that do not take
+// the template path (clean clusterizer neighbourhoods) or need no kriging
+// never become active.  Lists and counts go to J.nb / J.nbcount.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+    const uint32_t lo_masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int st = 0; st < 5; ++st) {
+        const int j = 16 >> st;
+        const uint32_t m = lo_masks[st];
+        const uint32_t y = __shfl_xor_sync(FULL_MASK, x, j);
+        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y & m) << j));
+    }
+    return x;
+}
+
+// Returns the segment's first node; dsm is a 32-int per-warp scratch.
+__device__ __forceinline__ int template_segment(const DevJob &J, const DevPlan &P, long long segi, int lane,
+                                                int *dsm) {
+    const int seg = (int)(segi % P.nseg);
+    const long long row = segi / P.nseg;
+    const int y = (int)(row % J.ny), z = (int)(row / J.ny);
+    const int x0 = seg * 32;
+    const int base = (int)(row * J.nx) + x0;
+    const int node = base + lane;
+    const bool act = x0 + lane < J.nx && node_needs_kriging(J, node) && !node_clean(P, x0 + lane, y, z);
+    uint32_t active = __ballot_sync(FULL_MASK, act);
+    if (!active) return base;
+    const int nmax = P.nmax;
+    int cnt = 0;
+    int *out = J.nb + (long long)node * nmax;
+    const uint32_t *bits = J.bits;
+    for (int tb = 0; tb < P.tmpl_len && active; tb += 32) {
+        const int t = tb + lane;
+        uint32_t w = 0;
+        int delta = 0;
+        if (t < P.tmpl_len) {
+            const int4 e = __ldg(&P.tmpl[t]);
+            delta = e.w;
+            const int yy = y + e.y, zz = z + e.z;
+            if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
+                const uint32_t *rp = bits + ((long long)zz * J.ny + yy) * P.wpr + seg + (e.x >> 5);
+                w = __funnelshift_r(__ldg(rp), __ldg(rp + 1), e.x & 31);
+            }
+        }
+        w &= active;
+        dsm[lane] = delta;
+        uint32_t hits = transpose32(w, lane);
+        __syncwarp();
+        while (hits && cnt < nmax) {
+            const int tt = __ffs(hits) - 1;
+            hits &= hits - 1;
+            out[cnt++] = node + dsm[tt];
+        }
+        __syncwarp();
+        active = __ballot_sync(FULL_MASK, act && cnt < nmax);
+    }
+    if (act) J.nbcount[node] = cnt;
+    return base;
+}
+
+}  // namespace hpgl_b200

@@ -18,6 +18,7 @@
 // and covariances gathered from the plan's table (my_kriging_weights.h:49-58,
 // 156-165), padded to 32x32 with the identity.
 #include "device_common.cuh"
+#include "search_common.cuh"
 
 namespace hpgl_b200 {
 
@@ -56,31 +57,6 @@ struct NodeData {
     double b;   // b_lane = C(x_lane - x0)
     int ox, oy, oz, lin;  // offset of neighbour `lane` from the node, and its table offset
 };
-
-// The first loads of a node, issued one node ahead by the persistent loops
-// (the neighbour count, the lane's neighbour cell and the informed flag start
-// a chain of dependent loads; issuing them while the previous system is
-// solved hides that latency).
-struct NodeFetch {
-    int node;  // -1: past the end
-    int n;
-    int cell;
-    bool informed;
-};
-
-__device__ __forceinline__ NodeFetch fetch_node(const DevJob &J, const DevPlan &P, int node, int lane) {
-    NodeFetch f;
-    f.node = node;
-    f.n = 0;
-    f.cell = 0;
-    f.informed = false;
-    if (node >= 0) {
-        f.n = __ldg(J.nbcount + node);
-        if (lane < P.nmax) f.cell = __ldg(J.nb + (long long)node * P.nmax + lane);
-        f.informed = is_cont(J.kind) && __ldg(J.mask + node) != 0;
-    }
-    return f;
-}
 
 __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &f,
                                               int lane) {
@@ -409,6 +385,19 @@ __device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, 
     write_outputs(J, P, S, node, lane, d, status, w, variance);
 }
 
+// One node of the exact path; returns whether a system was solved.
+__device__ __forceinline__ bool exact32_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &cur,
+                                             int lane) {
+    if (copy_informed(J, cur, lane)) return false;
+    const NodeData d = load_node(J, P, S, cur, lane);
+    if (d.n <= 0) {
+        write_outputs(J, P, S, cur.node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
+        return false;
+    }
+    exact_system(J, P, S, cur.node, lane, d);
+    return true;
+}
+
 __global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPlan P, const int *list, const int *n_list) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -421,16 +410,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPla
     for (; it < count; it += stride) {
         const long long nx = it + stride;
         const NodeFetch next = fetch_node(J, P, nx < count ? (list ? list[nx] : (int)nx) : -1, lane);
-        const int node = cur.node;
-        if (!copy_informed(J, cur, lane)) {
-            const NodeData d = load_node(J, P, S, cur, lane);
-            if (d.n <= 0) {
-                write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
-            } else {
-                exact_system(J, P, S, node, lane, d);
-                ++solved;
-            }
-        }
+        solved += exact32_node(J, P, S, cur, lane);
         __syncwarp();
         cur = next;
     }
@@ -479,149 +459,193 @@ __device__ __forceinline__ float get2(const float2 (&m2)[N32 / 2]) {
     return (P_ & 1) ? m2[P_ / 2].y : m2[P_ / 2].x;
 }
 
+// One node of the mixed path (FP32 inverse + FP64 refinement); systems that
+// do not qualify are appended to J.routed.
+__device__ __forceinline__ void mixed32_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &cur,
+                                             int lane) {
+    const bool ordinary = J.kind == 0;
+    const double inv_c0 = 1.0 / P.c0;
+    const int node = cur.node;
+    if (copy_informed(J, cur, lane)) return;
+    const NodeData d = load_node(J, P, S, cur, lane);
+    if (d.n <= 0) {
+        write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
+        return;
+    }
+    const int n = d.n;
+    build_full32(J, P, S, n, lane);
+    // Row `lane` of the unit-diagonal system A / C(0) (identity padding).
+    float2 m2[N32 / 2];
+#pragma unroll
+    for (int q = 0; q < N32 / 2; ++q)
+        m2[q] = f2((float)(S.A[(2 * q) * 33 + lane] * inv_c0), (float)(S.A[(2 * q + 1) * 33 + lane] * inv_c0));
+    // Symmetric Gauss-Jordan sweeps (the sweep operator): the matrix stays
+    // symmetric, so row p is column p and every lane publishes its own
+    // element of it; after all sweeps m holds -(A/C(0))^-1.  The pivot
+    // lane's own row update (scaling by 1/pivot) is folded into the same
+    // fused multiply-add as every other lane's elimination.
+    bool low = false;
+#pragma unroll
+    for (int p = 0; p < N32; ++p) {
+        float *rb = S.row[p & 1];
+        const float mp = (p & 1) ? m2[p / 2].y : m2[p / 2].x;
+        rb[lane] = mp;
+        __syncwarp();
+        const float piv = rb[p];
+        low |= !(piv > MIXED_PIVOT_MIN);
+        const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
+        const float isp = lane == p ? 1.f : 0.f;
+        const float g = (mp - isp) * dinv;
+        const float2 ng = f2(-g, -g);
+        const float4 *r4 = reinterpret_cast<const float4 *>(rb);
+#pragma unroll
+        for (int q = 0; q < N32 / 4; ++q) {
+            const float4 u = r4[q];
+            m2[2 * q] = __ffma2_rn(ng, f2(u.x, u.y), m2[2 * q]);
+            m2[2 * q + 1] = __ffma2_rn(ng, f2(u.z, u.w), m2[2 * q + 1]);
+        }
+        if (p & 1) m2[p / 2].y = g - isp;
+        else m2[p / 2].x = g - isp;
+    }
+    if (__any_sync(FULL_MASK, low)) {
+        if (lane == 0) {
+            const int pos = atomicAdd(J.n_routed, 1);
+            J.routed[pos] = node;
+        }
+        __syncwarp();
+        return;
+    }
+    // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
+    // refined with FP64 residuals.
+    const double sc = -inv_c0;
+    double xa = (double)apply_inverse(m2, (float)d.b, S.vf[0], lane) * sc;
+    double xb = ordinary ? (double)apply_inverse(m2, lane < n ? 1.f : 0.f, S.vf[1], lane) * sc : 0.0;
+    const double ba = d.b, bb = lane < n ? 1.0 : 0.0;
+    RefineGate gate;
+    bool converged = false;
+    for (int corr = 0; corr < MIXED_MAX_CORR; ++corr) {
+        const double ra = residual(S, S.vd, xa, ba, lane);
+        const double da = (double)apply_inverse(m2, (float)ra, S.vf[0], lane) * sc;
+        xa += da;
+        double dmax = fabs(da), xmax = fabs(xa);
+        if (ordinary) {
+            const double rbv = residual(S, S.vd, xb, bb, lane);
+            const double db = (double)apply_inverse(m2, (float)rbv, S.vf[1], lane) * sc;
+            xb += db;
+            dmax = fmax(dmax, fabs(db));
+            xmax = fmax(xmax, fabs(xb));
+        }
+        const int verdict = gate.step(warp_max(dmax), warp_max(xmax));
+        if (verdict != 0) {
+            converged = verdict > 0;
+            break;
+        }
+    }
+    if (!converged) {
+        if (lane == 0) {
+            const int pos = atomicAdd(J.n_routed, 1);
+            J.routed[pos] = node;
+        }
+        __syncwarp();
+        return;
+    }
+    if (lane >= n) {
+        xa = 0.0;
+        xb = 0.0;
+    }
+    double w;
+    if (ordinary) {
+        const double mu = (warp_sum(xa) - 1.0) / warp_sum(xb);
+        w = xa - mu * xb;
+    } else {
+        w = xa;
+    }
+    double variance = -1.0;
+    if (J.variance) {
+        variance = P.c0 - warp_sum(w * d.b);
+        if (ordinary) variance -= __shfl_sync(FULL_MASK, w, n - 1);
+    }
+    write_outputs(J, P, S, node, lane, d, ST_SUCCESS, w, variance);
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPlan P) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
-    const bool ordinary = J.kind == 0;
-    const double inv_c0 = 1.0 / P.c0;
     const long long stride = (long long)gridDim.x * WARPS32;
     long long it = (long long)blockIdx.x * WARPS32 + warp;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
     for (; it < J.size; it += stride) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
-        const int node = cur.node;
-        if (copy_informed(J, cur, lane)) continue;
-        const NodeData d = load_node(J, P, S, cur, lane);
-        if (d.n <= 0) {
-            write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
-            continue;
-        }
-        const int n = d.n;
-        build_full32(J, P, S, n, lane);
-        // Row `lane` of the unit-diagonal system A / C(0) (identity padding).
-        float2 m2[N32 / 2];
-#pragma unroll
-        for (int q = 0; q < N32 / 2; ++q)
-            m2[q] = f2((float)(S.A[(2 * q) * 33 + lane] * inv_c0), (float)(S.A[(2 * q + 1) * 33 + lane] * inv_c0));
-        // Symmetric Gauss-Jordan sweeps (the sweep operator): the matrix stays
-        // symmetric, so row p is column p and every lane publishes its own
-        // element of it; after all sweeps m holds -(A/C(0))^-1.  The pivot
-        // lane's own row update (scaling by 1/pivot) is folded into the same
-        // fused multiply-add as every other lane's elimination.
-        bool low = false;
-#pragma unroll
-        for (int p = 0; p < N32; ++p) {
-            float *rb = S.row[p & 1];
-            const float mp = (p & 1) ? m2[p / 2].y : m2[p / 2].x;
-            rb[lane] = mp;
-            __syncwarp();
-            const float piv = rb[p];
-            low |= !(piv > MIXED_PIVOT_MIN);
-            const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
-            const float isp = lane == p ? 1.f : 0.f;
-            const float g = (mp - isp) * dinv;
-            const float2 ng = f2(-g, -g);
-            const float4 *r4 = reinterpret_cast<const float4 *>(rb);
-#pragma unroll
-            for (int q = 0; q < N32 / 4; ++q) {
-                const float4 u = r4[q];
-                m2[2 * q] = __ffma2_rn(ng, f2(u.x, u.y), m2[2 * q]);
-                m2[2 * q + 1] = __ffma2_rn(ng, f2(u.z, u.w), m2[2 * q + 1]);
-            }
-            if (p & 1) m2[p / 2].y = g - isp;
-            else m2[p / 2].x = g - isp;
-        }
-        if (__any_sync(FULL_MASK, low)) {
-            if (lane == 0) {
-                const int pos = atomicAdd(J.n_routed, 1);
-                J.routed[pos] = node;
-            }
-            __syncwarp();
-            continue;
-        }
-        // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
-        // refined with FP64 residuals.
-        const double sc = -inv_c0;
-        double xa = (double)apply_inverse(m2, (float)d.b, S.vf[0], lane) * sc;
-        double xb = ordinary ? (double)apply_inverse(m2, lane < n ? 1.f : 0.f, S.vf[1], lane) * sc : 0.0;
-        const double ba = d.b, bb = lane < n ? 1.0 : 0.0;
-        RefineGate gate;
-        bool converged = false;
-        for (int corr = 0; corr < MIXED_MAX_CORR; ++corr) {
-            const double ra = residual(S, S.vd, xa, ba, lane);
-            const double da = (double)apply_inverse(m2, (float)ra, S.vf[0], lane) * sc;
-            xa += da;
-            double dmax = fabs(da), xmax = fabs(xa);
-            if (ordinary) {
-                const double rbv = residual(S, S.vd, xb, bb, lane);
-                const double db = (double)apply_inverse(m2, (float)rbv, S.vf[1], lane) * sc;
-                xb += db;
-                dmax = fmax(dmax, fabs(db));
-                xmax = fmax(xmax, fabs(xb));
-            }
-            const int verdict = gate.step(warp_max(dmax), warp_max(xmax));
-            if (verdict != 0) {
-                converged = verdict > 0;
-                break;
-            }
-        }
-        if (!converged) {
-            if (lane == 0) {
-                const int pos = atomicAdd(J.n_routed, 1);
-                J.routed[pos] = node;
-            }
-            __syncwarp();
-            continue;
-        }
-        if (lane >= n) {
-            xa = 0.0;
-            xb = 0.0;
-        }
-        double w;
-        if (ordinary) {
-            const double mu = (warp_sum(xa) - 1.0) / warp_sum(xb);
-            w = xa - mu * xb;
-        } else {
-            w = xa;
-        }
-        double variance = -1.0;
-        if (J.variance) {
-            variance = P.c0 - warp_sum(w * d.b);
-            if (ordinary) variance -= __shfl_sync(FULL_MASK, w, n - 1);
-        }
-        write_outputs(J, P, S, node, lane, d, ST_SUCCESS, w, variance);
+        mixed32_node(J, P, S, cur, lane);
         __syncwarp();
     }
 }
 
-constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
-
-int grid_for(const void *fn, int threads) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM32);
-    int per_sm = 0, dev = 0, sms = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, SMEM32);
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return (per_sm < 1 ? 1 : per_sm) * sms;
+// Fused search + solve: each warp takes 32-node x-segments, runs the template
+// search for the segment's template-path nodes (lists to J.nb, still in L2),
+// then solves the segment's nodes one after the other -- the clusterizer-path
+// nodes' lists come from the clusterizer search launched before.  Warps in
+// the search phase (memory latency) and in the solve phase (FP pipes)
+// overlap on every SM.
+template <int MODE>
+__global__ void __launch_bounds__(WARPS32 * 32) k_fused32(DevJob J, DevPlan P) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ int delta_sm[WARPS32][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    const long long total = (long long)P.nseg * J.ny * J.nz;
+    const long long stride = (long long)gridDim.x * WARPS32;
+    unsigned long long solved = 0;
+    for (long long segi = (long long)blockIdx.x * WARPS32 + warp; segi < total; segi += stride) {
+        const int base = template_segment(J, P, segi, lane, delta_sm[warp]);
+        __syncwarp();
+        const int x0 = (int)(segi % P.nseg) * 32;
+        const int cnt = min(32, J.nx - x0);
+        NodeFetch next = fetch_node(J, P, base, lane);
+        for (int b = 0; b < cnt; ++b) {
+            const NodeFetch cur = next;
+            next = fetch_node(J, P, b + 1 < cnt ? base + b + 1 : -1, lane);
+            if (MODE == 0) solved += exact32_node(J, P, S, cur, lane);
+            else mixed32_node(J, P, S, cur, lane);
+            __syncwarp();
+        }
+    }
+    if (MODE == 0 && lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
+
+constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
 
 }  // namespace
 
-void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                    long long n_max, cudaStream_t s) {
-    if (n_max <= 0) return;
-    if (precision == 0 || node_list) {
-        static const int grid = grid_for((const void *)k_solve_exact32, WARPS32 * 32);
-        long long blocks = (n_max + WARPS32 - 1) / WARPS32;
-        if (blocks > grid) blocks = grid;
-        k_solve_exact32<<<(unsigned)blocks, WARPS32 * 32, SMEM32, s>>>(J, P, node_list, n_list);
+void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm) {
+    const long long segs = (long long)P.nseg * J.ny * J.nz;
+    if (segs <= 0) return;
+    const int threads = WARPS32 * 32;
+    if (precision == 0) {
+        const long long g = persistent_grid((const void *)k_fused32<0>, threads, SMEM32, blocks_per_sm,
+                                            (segs + WARPS32 - 1) / WARPS32);
+        k_fused32<0><<<(unsigned)g, threads, SMEM32, s>>>(J, P);
     } else {
-        static const int grid = grid_for((const void *)k_solve_mixed32, WARPS32 * 32);
-        long long blocks = (n_max + WARPS32 - 1) / WARPS32;
-        if (blocks > grid) blocks = grid;
-        k_solve_mixed32<<<(unsigned)blocks, WARPS32 * 32, SMEM32, s>>>(J, P);
+        const long long g = persistent_grid((const void *)k_fused32<1>, threads, SMEM32, blocks_per_sm,
+                                            (segs + WARPS32 - 1) / WARPS32);
+        k_fused32<1><<<(unsigned)g, threads, SMEM32, s>>>(J, P);
+    }
+}
+
+void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
+                    long long n_max, cudaStream_t s, int blocks_per_sm) {
+    if (n_max <= 0) return;
+    const int threads = WARPS32 * 32;
+    const long long units = (n_max + WARPS32 - 1) / WARPS32;
+    if (precision == 0 || node_list) {
+        const long long g = persistent_grid((const void *)k_solve_exact32, threads, SMEM32, blocks_per_sm, units);
+        k_solve_exact32<<<(unsigned)g, threads, SMEM32, s>>>(J, P, node_list, n_list);
+    } else {
+        const long long g = persistent_grid((const void *)k_solve_mixed32, threads, SMEM32, blocks_per_sm, units);
+        k_solve_mixed32<<<(unsigned)g, threads, SMEM32, s>>>(J, P);
     }
 }
 

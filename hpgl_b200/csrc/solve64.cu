@@ -12,7 +12,10 @@
 //                    final at step j, which is all the dot-product form of
 //                    DTRSM needs).  The step loop is a plain runtime loop, so
 //                    the kernel stays small for the instruction caches.
+#include <algorithm>
+
 #include "device_common.cuh"
+#include "search_common.cuh"
 
 namespace hpgl_b200 {
 
@@ -58,9 +61,11 @@ struct Node64 {
     double b[2];  // C(x_row - x0)
 };
 
-__device__ __forceinline__ Node64 load_node64(const DevJob &J, const DevPlan &P, int4 *nb, int node, int lane) {
+__device__ __forceinline__ Node64 load_node64(const DevJob &J, const DevPlan &P, int4 *nb, const NodeFetch &f,
+                                              int lane) {
     Node64 d;
-    d.n = J.nbcount[node];
+    const int node = f.node;
+    d.n = f.n;
     int x0, y0, z0;
     node_xyz(J, node, x0, y0, z0);
 #pragma unroll
@@ -71,7 +76,7 @@ __device__ __forceinline__ Node64 load_node64(const DevJob &J, const DevPlan &P,
         d.b[r] = 0.0;
         int4 o = make_int4(0, 0, 0, 0);
         if (row < d.n) {
-            const int cell = J.nb[(long long)node * P.nmax + row];
+            const int cell = r ? f.cell2 : f.cell;
             int qx, qy, qz;
             node_xyz(J, cell, qx, qy, qz);
             o.x = qx - x0;
@@ -186,8 +191,9 @@ __device__ __forceinline__ void write_outputs64(const DevJob &J, const DevPlan &
     }
 }
 
-__device__ __forceinline__ bool copy_informed64(const DevJob &J, int node, int lane) {
-    if (is_cont(J.kind) && J.mask[node]) {
+__device__ __forceinline__ bool copy_informed64(const DevJob &J, const NodeFetch &f, int lane) {
+    const int node = f.node;
+    if (f.informed) {
         if (lane == 0) {
             J.out_values[node] = J.values[node];
             J.out_mask[node] = 1;
@@ -410,6 +416,19 @@ __device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S
     write_outputs64(J, P, node, lane, d, status, w0, w1, variance);
 }
 
+// One node of the exact path; returns whether a system was solved.
+__device__ __forceinline__ bool exact64_node(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs,
+                                             const NodeFetch &cur, int lane) {
+    if (copy_informed64(J, cur, lane)) return false;
+    const Node64 d = load_node64(J, P, S.nb, cur, lane);
+    if (d.n <= 0) {
+        write_outputs64(J, P, cur.node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
+        return false;
+    }
+    exact64_system(J, P, S, cs, g_pairs64.v, cur.node, lane, d);
+    return true;
+}
+
 __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, DevPlan P, const int *list,
                                                                       const int *n_list) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -419,23 +438,19 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, 
     __syncthreads();
     Exact64Smem &S = reinterpret_cast<Exact64Smem *>(dyn_smem)[warp];
     const long long count = list ? (long long)*n_list : J.size;
+    const long long stride = (long long)gridDim.x * WARPS64_BLOCK;
     unsigned long long solved = 0;
-    for (long long it = (long long)blockIdx.x * WARPS64_BLOCK + warp; it < count;
-         it += (long long)gridDim.x * WARPS64_BLOCK) {
-        const int node = list ? list[it] : (int)it;
-        if (copy_informed64(J, node, lane)) continue;
-        const Node64 d = load_node64(J, P, S.nb, node, lane);
-        if (d.n <= 0) {
-            write_outputs64(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
-            continue;
-        }
-        exact64_system(J, P, S, s_cs, g_pairs64.v, node, lane, d);
-        ++solved;
+    long long it = (long long)blockIdx.x * WARPS64_BLOCK + warp;
+    NodeFetch cur = fetch_node(J, P, it < count ? (list ? list[it] : (int)it) : -1, lane);
+    for (; it < count; it += stride) {
+        const long long nx = it + stride;
+        const NodeFetch next = fetch_node(J, P, nx < count ? (list ? list[nx] : (int)nx) : -1, lane);
+        solved += exact64_node(J, P, S, s_cs, cur, lane);
         __syncwarp();
+        cur = next;
     }
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
-
 
 // ---------------------------------------------------------------------------
 // Mixed path: FP32 Gauss-Jordan inverse + FP64 refinement.
@@ -526,6 +541,168 @@ __device__ __forceinline__ void residual64(const Mixed64Smem &S, const int *cs, 
     rb1 = r1 < n ? -sb1 : 0.0;
 }
 
+// One node of the mixed path; systems that do not qualify are appended to
+// J.routed.
+__device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, Mixed64Smem &S, const int *cs,
+                                             const NodeFetch &cur, int lane) {
+    const bool ordinary = J.kind == 0;
+    const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0)
+    const double inv_c0 = 1.0 / P.c0;
+    const int r0 = lane, r1 = lane + 32;
+    const int cs0 = cs[r0], cs1 = cs[r1];
+    const int node = cur.node;
+    if (copy_informed64(J, cur, lane)) return;
+    const Node64 d = load_node64(J, P, S.nb, cur, lane);
+    if (d.n <= 0) {
+        write_outputs64(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
+        return;
+    }
+    const int n = d.n;
+    build_packed(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane);
+    // Rows lane and lane + 32 of the unit-diagonal system A / C(0),
+    // identity beyond n.
+    float2 m0[32], m1[32];
+#pragma unroll
+    for (int c = 0; c < N64; c += 2) {
+        float e[2][2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = h ? r1 : r0, csr = h ? cs1 : cs0;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int cc = c + t;
+                float v;
+                if (r < n && cc < n) {
+                    const double a = cc == r ? a_diag : S.U[cc > r ? cs[cc] + r : csr + cc];
+                    v = (float)(a * inv_c0);
+                } else {
+                    v = cc == r ? 1.f : 0.f;
+                }
+                e[h][t] = v;
+            }
+        }
+        m0[c / 2] = f2(e[0][0], e[0][1]);
+        m1[c / 2] = f2(e[1][0], e[1][1]);
+    }
+    // Symmetric Gauss-Jordan sweeps over the n live rows: the matrix stays
+    // symmetric, so pivot row p (broadcast by its owner lane) is also
+    // column p and every lane reads its rows' multipliers from it.  The
+    // broadcast entry at p is set to piv - 1, which turns the same fused
+    // update into the sweep's column p (g = m_rp / piv) on every other row
+    // and leaves 2 - 1/piv in place of -1/piv on the pivot itself; swept
+    // diagonal entries are never read again, so the constant offset is
+    // removed when the inverse is applied.  After all sweeps M holds
+    // -(A/C(0))^-1 (+2 on the diagonal).
+    bool low = false;
+    for (int p = 0; p < n; ++p) {
+        const int owner = p & 31;
+        if (lane == owner) {
+            float4 *dst = reinterpret_cast<float4 *>(S.row);
+            if (p < 32) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    dst[q] = make_float4(m0[2 * q].x, m0[2 * q].y, m0[2 * q + 1].x, m0[2 * q + 1].y);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    dst[q] = make_float4(m1[2 * q].x, m1[2 * q].y, m1[2 * q + 1].x, m1[2 * q + 1].y);
+            }
+        }
+        __syncwarp();
+        const float piv = S.row[p];
+        if (!(piv > MIXED64_PIVOT_MIN)) {  // uniform: every lane read the same pivot
+            low = true;
+            break;
+        }
+        const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
+        const float g0 = (S.row[r0] - (r0 == p ? 1.f : 0.f)) * dinv;
+        const float g1 = (S.row[r1] - (r1 == p ? 1.f : 0.f)) * dinv;
+        __syncwarp();
+        if (lane == 0) S.row[p] = piv - 1.f;
+        __syncwarp();
+        const float2 ng0 = f2(-g0, -g0), ng1 = f2(-g1, -g1);
+        const float4 *r4 = reinterpret_cast<const float4 *>(S.row);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const float4 u = r4[q];
+            m0[2 * q] = __ffma2_rn(ng0, f2(u.x, u.y), m0[2 * q]);
+            m1[2 * q] = __ffma2_rn(ng1, f2(u.x, u.y), m1[2 * q]);
+            m0[2 * q + 1] = __ffma2_rn(ng0, f2(u.z, u.w), m0[2 * q + 1]);
+            m1[2 * q + 1] = __ffma2_rn(ng1, f2(u.z, u.w), m1[2 * q + 1]);
+        }
+        __syncwarp();
+    }
+    if (low) {
+        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        __syncwarp();
+        return;
+    }
+    // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
+    // refined with FP64 residuals.
+    const double sc = -inv_c0;
+    const double ba0 = d.b[0], ba1 = d.b[1];
+    const double bb0 = r0 < n ? 1.0 : 0.0, bb1 = r1 < n ? 1.0 : 0.0;
+    float y0, y1;
+    apply64(m0, m1, (float)ba0, (float)ba1, S.vf[0], lane, y0, y1);
+    double xa0 = (double)y0 * sc, xa1 = (double)y1 * sc, xb0 = 0.0, xb1 = 0.0;
+    if (ordinary) {
+        apply64(m0, m1, (float)bb0, (float)bb1, S.vf[1], lane, y0, y1);
+        xb0 = (double)y0 * sc;
+        xb1 = (double)y1 * sc;
+    }
+    RefineGate gate;
+    bool converged = false;
+    for (int corr = 0; corr < MIXED64_MAX_CORR; ++corr) {
+        double ra0, ra1, rb0, rb1;
+        residual64(S, cs, a_diag, n, lane, ordinary, xa0, xa1, xb0, xb1, ra0, ra1, rb0, rb1);
+        ra0 += ba0;
+        ra1 += ba1;
+        apply64(m0, m1, (float)ra0, (float)ra1, S.vf[0], lane, y0, y1);
+        const double da0 = (double)y0 * sc, da1 = (double)y1 * sc;
+        xa0 += da0;
+        xa1 += da1;
+        double dmax = fmax(fabs(da0), fabs(da1)), xmax = fmax(fabs(xa0), fabs(xa1));
+        if (ordinary) {
+            rb0 += bb0;
+            rb1 += bb1;
+            apply64(m0, m1, (float)rb0, (float)rb1, S.vf[1], lane, y0, y1);
+            const double db0 = (double)y0 * sc, db1 = (double)y1 * sc;
+            xb0 += db0;
+            xb1 += db1;
+            dmax = fmax(dmax, fmax(fabs(db0), fabs(db1)));
+            xmax = fmax(xmax, fmax(fabs(xb0), fabs(xb1)));
+        }
+        const int verdict = gate.step(warp_max64(dmax), warp_max64(xmax));
+        if (verdict != 0) {
+            converged = verdict > 0;
+            break;
+        }
+    }
+    if (!converged) {
+        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        __syncwarp();
+        return;
+    }
+    if (r0 >= n) xa0 = xb0 = 0.0;
+    if (r1 >= n) xa1 = xb1 = 0.0;
+    double w0, w1;
+    if (ordinary) {
+        const double mu = (warp_sum64(xa0 + xa1) - 1.0) / warp_sum64(xb0 + xb1);
+        w0 = xa0 - mu * xb0;
+        w1 = xa1 - mu * xb1;
+    } else {
+        w0 = xa0;
+        w1 = xa1;
+    }
+    double variance = -1.0;
+    if (J.variance) {
+        variance = P.c0 - warp_sum64(w0 * d.b[0] + w1 * d.b[1]);
+        if (ordinary) variance -= row_val(w0, w1, n - 1);
+    }
+    write_outputs64(J, P, node, lane, d, ST_SUCCESS, w0, w1, variance);
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ int s_cs[N64];
@@ -533,196 +710,74 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Mixed64Smem &S = *reinterpret_cast<Mixed64Smem *>(dyn_smem);
-    const int *cs = s_cs;
-    const bool ordinary = J.kind == 0;
-    const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0)
-    const double inv_c0 = 1.0 / P.c0;
-    const int r0 = lane, r1 = lane + 32;
-    const int cs0 = cs[r0], cs1 = cs[r1];
-    for (long long it = blockIdx.x; it < J.size; it += gridDim.x) {
-        const int node = (int)it;
-        if (copy_informed64(J, node, lane)) continue;
-        const Node64 d = load_node64(J, P, S.nb, node, lane);
-        if (d.n <= 0) {
-            write_outputs64(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
-            continue;
-        }
-        const int n = d.n;
-        build_packed(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane);
-        // Rows lane and lane + 32 of the unit-diagonal system A / C(0),
-        // identity beyond n.
-        float2 m0[32], m1[32];
-#pragma unroll
-        for (int c = 0; c < N64; c += 2) {
-            float e[2][2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = h ? r1 : r0, csr = h ? cs1 : cs0;
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    const int cc = c + t;
-                    float v;
-                    if (r < n && cc < n) {
-                        const double a = cc == r ? a_diag : S.U[cc > r ? cs[cc] + r : csr + cc];
-                        v = (float)(a * inv_c0);
-                    } else {
-                        v = cc == r ? 1.f : 0.f;
-                    }
-                    e[h][t] = v;
-                }
-            }
-            m0[c / 2] = f2(e[0][0], e[0][1]);
-            m1[c / 2] = f2(e[1][0], e[1][1]);
-        }
-        // Symmetric Gauss-Jordan sweeps over the n live rows: the matrix stays
-        // symmetric, so pivot row p (broadcast by its owner lane) is also
-        // column p and every lane reads its rows' multipliers from it.  The
-        // broadcast entry at p is set to piv - 1, which turns the same fused
-        // update into the sweep's column p (g = m_rp / piv) on every other row
-        // and leaves 2 - 1/piv in place of -1/piv on the pivot itself; swept
-        // diagonal entries are never read again, so the constant offset is
-        // removed when the inverse is applied.  After all sweeps M holds
-        // -(A/C(0))^-1 (+2 on the diagonal).
-        bool low = false;
-        for (int p = 0; p < n; ++p) {
-            const int owner = p & 31;
-            if (lane == owner) {
-                float4 *dst = reinterpret_cast<float4 *>(S.row);
-                if (p < 32) {
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        dst[q] = make_float4(m0[2 * q].x, m0[2 * q].y, m0[2 * q + 1].x, m0[2 * q + 1].y);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        dst[q] = make_float4(m1[2 * q].x, m1[2 * q].y, m1[2 * q + 1].x, m1[2 * q + 1].y);
-                }
-            }
-            __syncwarp();
-            const float piv = S.row[p];
-            if (!(piv > MIXED64_PIVOT_MIN)) {  // uniform: every lane read the same pivot
-                low = true;
-                break;
-            }
-            const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
-            const float g0 = (S.row[r0] - (r0 == p ? 1.f : 0.f)) * dinv;
-            const float g1 = (S.row[r1] - (r1 == p ? 1.f : 0.f)) * dinv;
-            __syncwarp();
-            if (lane == 0) S.row[p] = piv - 1.f;
-            __syncwarp();
-            const float2 ng0 = f2(-g0, -g0), ng1 = f2(-g1, -g1);
-            const float4 *r4 = reinterpret_cast<const float4 *>(S.row);
-#pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const float4 u = r4[q];
-                m0[2 * q] = __ffma2_rn(ng0, f2(u.x, u.y), m0[2 * q]);
-                m1[2 * q] = __ffma2_rn(ng1, f2(u.x, u.y), m1[2 * q]);
-                m0[2 * q + 1] = __ffma2_rn(ng0, f2(u.z, u.w), m0[2 * q + 1]);
-                m1[2 * q + 1] = __ffma2_rn(ng1, f2(u.z, u.w), m1[2 * q + 1]);
-            }
-            __syncwarp();
-        }
-        if (low) {
-            if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
-            __syncwarp();
-            continue;
-        }
-        // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
-        // refined with FP64 residuals.
-        const double sc = -inv_c0;
-        const double ba0 = d.b[0], ba1 = d.b[1];
-        const double bb0 = r0 < n ? 1.0 : 0.0, bb1 = r1 < n ? 1.0 : 0.0;
-        float y0, y1;
-        apply64(m0, m1, (float)ba0, (float)ba1, S.vf[0], lane, y0, y1);
-        double xa0 = (double)y0 * sc, xa1 = (double)y1 * sc, xb0 = 0.0, xb1 = 0.0;
-        if (ordinary) {
-            apply64(m0, m1, (float)bb0, (float)bb1, S.vf[1], lane, y0, y1);
-            xb0 = (double)y0 * sc;
-            xb1 = (double)y1 * sc;
-        }
-        RefineGate gate;
-        bool converged = false;
-        for (int corr = 0; corr < MIXED64_MAX_CORR; ++corr) {
-            double ra0, ra1, rb0, rb1;
-            residual64(S, cs, a_diag, n, lane, ordinary, xa0, xa1, xb0, xb1, ra0, ra1, rb0, rb1);
-            ra0 += ba0;
-            ra1 += ba1;
-            apply64(m0, m1, (float)ra0, (float)ra1, S.vf[0], lane, y0, y1);
-            const double da0 = (double)y0 * sc, da1 = (double)y1 * sc;
-            xa0 += da0;
-            xa1 += da1;
-            double dmax = fmax(fabs(da0), fabs(da1)), xmax = fmax(fabs(xa0), fabs(xa1));
-            if (ordinary) {
-                rb0 += bb0;
-                rb1 += bb1;
-                apply64(m0, m1, (float)rb0, (float)rb1, S.vf[1], lane, y0, y1);
-                const double db0 = (double)y0 * sc, db1 = (double)y1 * sc;
-                xb0 += db0;
-                xb1 += db1;
-                dmax = fmax(dmax, fmax(fabs(db0), fabs(db1)));
-                xmax = fmax(xmax, fmax(fabs(xb0), fabs(xb1)));
-            }
-            const int verdict = gate.step(warp_max64(dmax), warp_max64(xmax));
-            if (verdict != 0) {
-                converged = verdict > 0;
-                break;
-            }
-        }
-        if (!converged) {
-            if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
-            __syncwarp();
-            continue;
-        }
-        if (r0 >= n) xa0 = xb0 = 0.0;
-        if (r1 >= n) xa1 = xb1 = 0.0;
-        double w0, w1;
-        if (ordinary) {
-            const double mu = (warp_sum64(xa0 + xa1) - 1.0) / warp_sum64(xb0 + xb1);
-            w0 = xa0 - mu * xb0;
-            w1 = xa1 - mu * xb1;
-        } else {
-            w0 = xa0;
-            w1 = xa1;
-        }
-        double variance = -1.0;
-        if (J.variance) {
-            variance = P.c0 - warp_sum64(w0 * d.b[0] + w1 * d.b[1]);
-            if (ordinary) variance -= row_val(w0, w1, n - 1);
-        }
-        write_outputs64(J, P, node, lane, d, ST_SUCCESS, w0, w1, variance);
+    long long it = blockIdx.x;
+    NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+    for (; it < J.size; it += gridDim.x) {
+        const NodeFetch cur = next;
+        next = fetch_node(J, P, it + gridDim.x < J.size ? (int)(it + gridDim.x) : -1, lane);
+        mixed64_node(J, P, S, s_cs, cur, lane);
         __syncwarp();
     }
+}
+
+// Fused search + solve (one warp per block): template search of a 32-node
+// segment, then the segment's systems, as in the 32-neighbour fused kernel.
+template <int MODE>
+__global__ void __launch_bounds__(32) k_fused64(DevJob J, DevPlan P) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ int s_cs[N64];
+    __shared__ int delta_sm[32];
+    const int lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
+    __syncthreads();
+    const long long total = (long long)P.nseg * J.ny * J.nz;
+    unsigned long long solved = 0;
+    for (long long segi = blockIdx.x; segi < total; segi += gridDim.x) {
+        const int base = template_segment(J, P, segi, lane, delta_sm);
+        __syncwarp();
+        const int x0 = (int)(segi % P.nseg) * 32;
+        const int cnt = min(32, J.nx - x0);
+        NodeFetch next = fetch_node(J, P, base, lane);
+        for (int b = 0; b < cnt; ++b) {
+            const NodeFetch cur = next;
+            next = fetch_node(J, P, b + 1 < cnt ? base + b + 1 : -1, lane);
+            if (MODE == 0) solved += exact64_node(J, P, *reinterpret_cast<Exact64Smem *>(dyn_smem), s_cs, cur, lane);
+            else mixed64_node(J, P, *reinterpret_cast<Mixed64Smem *>(dyn_smem), s_cs, cur, lane);
+            __syncwarp();
+        }
+    }
+    if (MODE == 0 && lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
 
 constexpr size_t SMEM64_EXACT = sizeof(Exact64Smem) * WARPS64_BLOCK;
 constexpr size_t SMEM64_MIXED = sizeof(Mixed64Smem);
 
-int grid64_for(const void *fn, size_t smem, int threads) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0, dev = 0, sms = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return (per_sm < 1 ? 1 : per_sm) * sms;
-}
-
 }  // namespace
 
 void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
-                          long long n_max, cudaStream_t s) {
+                          long long n_max, cudaStream_t s, int blocks_per_sm) {
     if (n_max <= 0) return;
-    static const int grid = grid64_for((const void *)k_solve_exact64, SMEM64_EXACT, WARPS64_BLOCK * 32);
-    long long blocks = (n_max + WARPS64_BLOCK - 1) / WARPS64_BLOCK;
-    if (blocks > grid) blocks = grid;
-    k_solve_exact64<<<(unsigned)blocks, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, node_list, n_list);
+    const long long g = persistent_grid((const void *)k_solve_exact64, WARPS64_BLOCK * 32, SMEM64_EXACT,
+                                        blocks_per_sm, (n_max + WARPS64_BLOCK - 1) / WARPS64_BLOCK);
+    k_solve_exact64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, node_list, n_list);
 }
 
-void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s) {
+void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s, int blocks_per_sm) {
     if (J.size <= 0) return;
-    static const int grid = grid64_for((const void *)k_solve_mixed64, SMEM64_MIXED, 32);
-    long long blocks = J.size;
-    if (blocks > grid) blocks = grid;
-    k_solve_mixed64<<<(unsigned)blocks, 32, SMEM64_MIXED, s>>>(J, P);
+    const long long g = persistent_grid((const void *)k_solve_mixed64, 32, SMEM64_MIXED, blocks_per_sm, J.size);
+    k_solve_mixed64<<<(unsigned)g, 32, SMEM64_MIXED, s>>>(J, P);
+}
+
+void launch_fused64(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm) {
+    const long long segs = (long long)P.nseg * J.ny * J.nz;
+    if (segs <= 0) return;
+    if (precision == 0) {
+        const long long g = persistent_grid((const void *)k_fused64<0>, 32, sizeof(Exact64Smem), blocks_per_sm, segs);
+        k_fused64<0><<<(unsigned)g, 32, sizeof(Exact64Smem), s>>>(J, P);
+    } else {
+        const long long g = persistent_grid((const void *)k_fused64<1>, 32, SMEM64_MIXED, blocks_per_sm, segs);
+        k_fused64<1><<<(unsigned)g, 32, SMEM64_MIXED, s>>>(J, P);
+    }
 }
 
 }  // namespace hpgl_b200

@@ -218,6 +218,39 @@ def bench(job, precision="mixed", iters=5, warmup=3, flush_bytes=256 << 20, kind
     return ms, info
 
 
+TUNE_MAX = 16
+
+
+class Tune(C.Structure):
+    _fields_ = [("candidates", C.c_int), ("schedule", C.c_int * TUNE_MAX), ("blocks_per_sm", C.c_int * TUNE_MAX),
+                ("ms", C.c_double * TUNE_MAX), ("chosen", C.c_int), ("family", C.c_int), ("precision", C.c_int)]
+
+
+def autotune(job, precision="mixed", kind=None):
+    """Runs hpgl_b200_autotune on the job; returns the candidates tried and
+    the launch setting now in force for its family and precision."""
+    L = lib()
+    p = _Prepared(job, precision, kind, False, False, None)
+    t = Tune()
+    rc = L.hpgl_b200_autotune(C.byref(p.job), C.byref(t))
+    if rc != 0:
+        raise HpglError(rc, L.hpgl_get_last_exception_message().decode())
+    names = {0: "split", 1: "fused"}
+    cands = [dict(schedule=names[t.schedule[i]], blocks_per_sm=t.blocks_per_sm[i], ms=t.ms[i])
+             for i in range(t.candidates)]
+    return dict(candidates=cands, chosen=cands[t.chosen], family=t.family, precision=t.precision)
+
+
+def set_launch(family, precision, schedule, blocks_per_sm=0):
+    """Pins the launch setting of a family (0: <= 32 neighbours, 1: above)
+    and precision ("fp64"/"mixed"): schedule "split" or "fused"."""
+    L = lib()
+    prec = {"fp64": 0, "mixed": 1}[precision]
+    rc = L.hpgl_b200_set_launch(int(family), prec, {"split": 0, "fused": 1}[schedule], int(blocks_per_sm))
+    if rc != 0:
+        raise HpglError(rc, L.hpgl_get_last_exception_message().decode())
+
+
 class HpglCovParams(C.Structure):
     _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
                 ("sill", C.c_double), ("nugget", C.c_double)]

@@ -337,6 +337,32 @@ typedef struct hpgl_b200_bench_t {
 } hpgl_b200_bench_t;
 int hpgl_b200_bench(const hpgl_b200_job_t *job, hpgl_b200_result_t *result, hpgl_b200_bench_t *bench);
 
+/* No counterpart in the reference.  Launch autotuner: runs the job's device
+   pass (planned and uploaded once, results discarded) under each candidate
+   setting of the per-node kernels -- the fused template-search+solve kernel
+   or separate search and solve kernels, and the number of persistent blocks
+   per SM -- times each (median of three passes after an L2 flush) and keeps
+   the fastest for the job's family (max_neighbours <= 32, or above) and
+   precision; every later call of that family and precision in the process
+   uses it.  Without a tuning run the separate schedule at full occupancy
+   is used.  Returns 0, or -1 with the error recorded. */
+#define HPGL_B200_TUNE_MAX 16
+typedef struct hpgl_b200_tune_t {
+    int candidates;                        /* settings tried */
+    int schedule[HPGL_B200_TUNE_MAX];      /* 0 separate search and solve, 1 fused */
+    int blocks_per_sm[HPGL_B200_TUNE_MAX]; /* 0 = as many as fit */
+    double ms[HPGL_B200_TUNE_MAX];         /* device time of one pass */
+    int chosen;                            /* index of the setting now in force */
+    int family;                            /* 0: max_neighbours <= 32, 1: above */
+    int precision;                         /* HPGL_PRECISION_* tuned */
+} hpgl_b200_tune_t;
+int hpgl_b200_autotune(const hpgl_b200_job_t *job, hpgl_b200_tune_t *report);
+/* No counterpart in the reference.  Sets the launch setting of a family
+   (0: max_neighbours <= 32, 1: above) and precision directly (schedule 0
+   separate, 1 fused; blocks_per_sm 0 = as many as fit).  Returns 0, or -1
+   on invalid arguments. */
+int hpgl_b200_set_launch(int family, int precision, int schedule, int blocks_per_sm);
+
 /* No counterpart in the reference.  hpgl_simple_kriging_weights for callers
    that cannot allocate device memory: cudaMalloc and cudaFree synchronise
    the whole device, stalling the caller's other GPU work, and a host
