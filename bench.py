@@ -169,6 +169,7 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -192,17 +193,7 @@ def main():
     size = int(np.prod(job["shape"]))
     kriged = int((job["mask"] == 0).sum())
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    from hpgl_b200.replicas import barrier, max_over_ranks, whole_job_rate
 
     # Untimed run of each path first (library warm-up, neighbour counts).
     dump = N.krige(job, precision="fp64", dumps=True)
@@ -214,6 +205,9 @@ def main():
     # persistent blocks per SM), untimed.
     tuning = {}
     for prec in ("mixed", "fp64"):
+        if args.no_autotune:
+            tuning[prec] = {"schedule": "split", "blocks_per_sm": 0, "candidates": 0}
+            continue
         t = N.autotune(job, precision=prec)
         tuning[prec] = dict(t["chosen"], candidates=len(t["candidates"]))
 
@@ -227,8 +221,8 @@ def main():
     barrier()
     t_mixed = max_over_ranks(float(ms_mixed.sum()))
     t_fp64 = max_over_ranks(float(ms_fp64.sum()))
-    value = world * kriged * args.steps / (t_mixed / 1000.0)
-    fp64_value = world * kriged * args.steps / (t_fp64 / 1000.0)
+    value = whole_job_rate(world, kriged * args.steps, t_mixed)
+    fp64_value = whole_job_rate(world, kriged * args.steps, t_fp64)
 
     # End to end through the public API from host buffers.
     for _ in range(1):
@@ -239,7 +233,7 @@ def main():
         r = N.krige(job, precision="mixed")
         e2e_ms.append(r["ms_total"])
     t_e2e = max_over_ranks(float(np.sum(e2e_ms)))
-    e2e_value = world * kriged * args.steps / (t_e2e / 1000.0)
+    e2e_value = whole_job_rate(world, kriged * args.steps, t_e2e)
     h2d = size * 4 + size * 1
     d2h = size * 4 + size * 1
 
