@@ -214,3 +214,37 @@ CONFIGS = {
     "ik_200x200x100": ik_200x200x100,
     "lvm_512x512x32": lvm_512x512x32,
 }
+
+
+def cokriging_job(shape=(48, 48, 12), mark=1, seed=6, informed=0.02, secondary_informed=0.9,
+                  max_neighbours=16, correlation=0.7):
+    """Colocated simple cokriging (Markov model I or II): a sparse primary
+    property and a dense, correlated secondary one on the same grid.  The
+    primary is a seeded Gaussian field (spherical covariance), the secondary
+    0.7 x the same field + 0.7 x an independent one, informed at
+    `secondary_informed` of the cells; means and the secondary variance are
+    those of the informed values."""
+    rng = np.random.default_rng(seed)
+    size = int(np.prod(shape))
+    f1 = gaussian_field(rng, shape, 12.0).reshape(-1, order="F")
+    f2 = gaussian_field(rng, shape, 12.0).reshape(-1, order="F")
+    prim = (2.0 + f1).astype(np.float32)
+    sec = (5.0 + 0.7 * f1 + 0.7 * f2).astype(np.float32)
+    values = np.full(size, -99.0, dtype=np.float32)
+    mask = np.zeros(size, dtype=np.uint8)
+    cells = _choose_cells(rng, size, informed)
+    values[cells] = prim[cells]
+    mask[cells] = 1
+    smask = (rng.uniform(size=size) < secondary_informed).astype(np.uint8)
+    svalues = np.where(smask > 0, sec, np.float32(-99.0)).astype(np.float32)
+    p = cov_params(SPHERICAL, (14, 14, 5), sill=1.0, nugget=0.0, radii=(14, 14, 5), max_neighbours=max_neighbours)
+    job = dict(name="cok%d_%dx%dx%d" % ((mark,) + tuple(shape)), kind="cok%d" % mark, shape=tuple(shape),
+               values=values, mask=mask, secondary_values=svalues, secondary_mask=smask, params=[p],
+               primary_mean=float(values[cells].astype(np.float64).mean()),
+               secondary_mean=float(svalues[smask > 0].astype(np.float64).mean()),
+               correlation=float(correlation))
+    if mark == 1:
+        job["secondary_variance"] = float(svalues[smask > 0].astype(np.float64).var())
+    else:
+        job["secondary_cov"] = cov_params(EXPONENTIAL, (20, 20, 6), sill=1.0, nugget=0.05)
+    return job

@@ -3,7 +3,8 @@
 // or calls it.  It is the checker the GPU results are compared against.
 //
 // CPU restatement of HPGL 0.9.9's kriging estimation path (ordinary, simple,
-// locally-varying-mean, indicator and median-indicator kriging).  Each piece
+// locally-varying-mean, indicator and median-indicator kriging, and colocated
+// simple cokriging with the Markov models I and II).  Each piece
 // cites the reference file:line it follows (paths relative to the reference's
 // src/geo_bsd/hpgl/).  Parity of this restatement is pinned by comparing it
 // with the reference's own sources compiled by oracle/build_ref.sh (estimates,
@@ -568,9 +569,176 @@ void median_ik(const grid3 &g, const unsigned char *codes, const unsigned char *
     }
 }
 
+// gauss_solve (gauss_solver.cpp:5-63): for column i the first row not yet
+// used whose entry is non-zero becomes the pivot row (no magnitude
+// pivoting); it is divided by its pivot entry from column i on, and
+// eliminated from every unused row; back substitution reads B in position
+// order (B[i]) with the pivot rows' coefficients, as the reference does.
+// A is row-major size x size and is overwritten; returns false when a
+// column has no usable pivot.
+bool gauss_solve(double *A, double *B, double *X, int size) {
+    std::vector<int> flags(size, 0), order(size, 0);
+    for (int i = 0; i < size; ++i) {
+        int row = -1;
+        for (int j = 0; j < size; ++j)
+            if (flags[j] == 0 && A[(size_t)j * size + i] != 0) {
+                row = j;
+                flags[j] = 1;
+                order[i] = j;
+                break;
+            }
+        if (row < 0) return false;
+        const double coef = A[(size_t)row * size + i];
+        for (int j = i; j < size; ++j) A[(size_t)row * size + j] /= coef;
+        B[row] /= coef;
+        for (int j = 0; j < size; ++j) {
+            if (flags[j] == 0) {
+                const double c = A[(size_t)j * size + i];
+                for (int k = i; k < size; ++k) A[(size_t)j * size + k] -= c * A[(size_t)row * size + k];
+                B[j] -= c * B[row];
+            }
+        }
+    }
+    for (int i = size - 1; i >= 0; --i) {
+        const int row = order[i];
+        X[i] = B[i];
+        for (int j = size - 1; j > i; --j) X[i] -= A[(size_t)row * size + j] * X[j];
+    }
+    return true;
+}
+
+// simple_cokriging_markI / markII (simple_cokriging_markI.cpp:19-307):
+// colocated simple cokriging with the Markov model I or II cross
+// covariance.  The search is neighbour_lookup_t over the untruncated primary
+// model (no clusterizer); the (N+1)-row system holds the primary covariances,
+// the cross covariances coef * C_x(center - x_i) in its last row and column,
+// and the secondary variance in the corner; b = (C(x_i - center), coef * C_x(0)).
+// Means are floats (mean_t); the estimate is
+// m1 + sum (v_i - m1) w_i + w_N (s - m2), each step widened to double and
+// rounded back to the float result; failures give m1 + s - m2.
+void cokriging(int mark, const grid3 &g, const float *values, const unsigned char *mask, const float *svalues,
+               const unsigned char *smask, const oracle_params_t &pp, const oracle_params_t *sp, float m1, float m2,
+               double secondary_variance_m1, double corr, const outputs &o, const int *list, int n_list) {
+    covariance cov(pp, false);
+    const cov_model &model = cov.model;
+    cov_model smodel(mark == 2 ? *sp : pp);
+    const int zero[3] = {0, 0, 0};
+    double coef, secondary_variance;
+    if (mark == 1) {
+        // cross_cov_model_mark_i_t: p12 * sqrt(d2) / sqrt(C(0))
+        coef = corr * sqrt(secondary_variance_m1) / sqrt(model.at(zero, zero));
+        secondary_variance = secondary_variance_m1;
+    } else {
+        // cross_cov_model_mark_ii_t: p12 * sqrt(C2(0) / C1(0))
+        const double pv = model.at(zero, zero);
+        secondary_variance = smodel.at(zero, zero);
+        coef = corr * sqrt(secondary_variance / pv);
+    }
+    const cov_model &cross = mark == 1 ? model : smodel;
+    const std::vector<int> tmpl = build_template(cov, pp);
+    const int n_t = (int)tmpl.size() / 3;
+    const int size = g.size();
+    const int count = list ? n_list : size;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int it = 0; it < count; ++it) {
+        const int idx = list ? list[it] : it;
+        float result;
+        std::vector<int> nb;
+        std::vector<double> w;
+        int status = ST_NOT_KRIGED;
+        if (mask[idx]) {
+            result = values[idx];
+        } else {
+            const float sv = smask[idx] ? svalues[idx] : m2;
+            int center[3];
+            g.loc(idx, center);
+            // neighbour_lookup_t::find (sugarbox_neighbour_lookup.h:35-61)
+            for (int t = 0; t < n_t && (int)nb.size() < pp.max_neighbours; ++t) {
+                int pt[3] = {center[0] + tmpl[3 * t], center[1] + tmpl[3 * t + 1], center[2] + tmpl[3 * t + 2]};
+                const int q = g.index(pt);
+                if (q >= 0 && mask[q]) nb.push_back(q);
+            }
+            bool ok = !nb.empty();
+            status = ok ? ST_SUCCESS : ST_NO_NEIGHBOURS;
+            if (ok) {
+                // build_system (simple_cokriging_markI.cpp:19-54)
+                const int n = (int)nb.size(), ms = n + 1;
+                std::vector<int> coords;
+                coords_of(g, nb, coords);
+                std::vector<double> A((size_t)ms * ms), b(ms);
+                for (int i = 0; i < n; ++i)
+                    for (int j = i; j < n; ++j) {
+                        A[(size_t)i * ms + j] = model.at(&coords[3 * i], &coords[3 * j]);
+                        A[(size_t)j * ms + i] = A[(size_t)i * ms + j];
+                    }
+                for (int i = 0; i < n; ++i) {
+                    A[(size_t)n * ms + i] = coef * cross.at(center, &coords[3 * i]);
+                    A[(size_t)i * ms + n] = A[(size_t)n * ms + i];
+                    b[i] = model.at(&coords[3 * i], center);
+                }
+                b[n] = coef * cross.at(zero, zero);
+                A[(size_t)ms * ms - 1] = secondary_variance;
+                w.resize(ms);
+                ok = gauss_solve(A.data(), b.data(), w.data(), ms);
+                if (!ok) status = ST_SINGULAR;
+            }
+            if (ok) {
+                // combine (simple_cokriging_markI.cpp:84-105)
+                const int n = (int)nb.size();
+                result = m1;
+                for (int i = 0; i < n; ++i) result += (values[nb[i]] - m1) * w[i];
+                result += w[n] * (sv - m2);
+            } else {
+                result = m1 + sv - m2;
+            }
+        }
+        o.out_values[idx] = result;
+        o.out_mask[idx] = 1;
+        if (o.status) o.status[idx] = (signed char)status;
+        if (o.nb_count) o.nb_count[idx] = (int)nb.size();
+        if (o.nb_index)
+            for (size_t i = 0; i < nb.size() && (int)i < o.nb_cap; ++i) o.nb_index[(size_t)idx * o.nb_cap + i] = nb[i];
+        if (o.weights && status == ST_SUCCESS)
+            for (size_t i = 0; i < w.size() && (int)i <= o.nb_cap; ++i)
+                o.weights[(size_t)idx * (o.nb_cap + 1) + i] = w[i];
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+// Colocated simple cokriging (mark 1 or 2) of a primary cube with a
+// secondary cube of the same shape.  `secondary` (Markov model II only) is
+// the secondary covariance; `secondary_variance` is Markov model I's d2.
+// Optional dumps per node: status, neighbour count and indices (`nb_cap`
+// per node), weights (`nb_cap` + 1 per node, the last one the secondary's).
+int oracle_cokriging(int mark, int nx, int ny, int nz, const float *values, const unsigned char *mask,
+                     const float *svalues, const unsigned char *smask, const oracle_params_t *primary,
+                     const oracle_params_t *secondary, double primary_mean, double secondary_mean,
+                     double secondary_variance, double corr, float *out_values, unsigned char *out_mask,
+                     signed char *status, int *nb_count, int *nb_index, double *weights, int nb_cap,
+                     const int *node_list, int n_nodes, int threads, char *err, int err_len) {
+    try {
+        if (threads > 0) omp_set_num_threads(threads);
+        if (mark != 1 && mark != 2) throw std::runtime_error("mark must be 1 or 2");
+        for (int i = 0; i < 3; ++i)
+            if (primary->radii[i] <= 0) throw std::runtime_error("search radii must be positive");
+        grid3 g{nx, ny, nz};
+        outputs o{out_values, nullptr, out_mask, nullptr, status, nb_count, nb_index, weights, nullptr, nullptr,
+                  nb_cap};
+        // the reference passes the means as mean_t (float)
+        cokriging(mark, g, values, mask, svalues, smask, *primary, secondary, (float)primary_mean,
+                  (float)secondary_mean, secondary_variance, corr, o, node_list, n_nodes);
+        return 0;
+    } catch (const std::exception &e) {
+        if (err && err_len > 0) {
+            strncpy(err, e.what(), err_len - 1);
+            err[err_len - 1] = 0;
+        }
+        return 1;
+    }
+}
 
 // Runs one kriging job.  kind: 0 OK, 1 SK, 2 LVM, 3 IK, 4 median IK.
 // Inputs: `values` (OK/SK/LVM) or `codes` (IK/median IK), `mask`,

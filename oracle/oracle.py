@@ -340,3 +340,106 @@ def ref_sk_weights(center, xs, ys, zs, p):
     ref.hpgl_simple_kriging_weights(c, _ptr(x, C.c_float), _ptr(y, C.c_float), _ptr(z, C.c_float), n, C.byref(cp),
                                     _ptr(w, C.c_float))
     return w
+
+
+class HpglCovParams(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double)]
+
+
+class HpglCokM1Params(C.Structure):
+    _fields_ = HpglOkParams._fields_ + [("primary_mean", C.c_double), ("secondary_mean", C.c_double),
+                                        ("secondary_variance", C.c_double), ("correlation_coef", C.c_double)]
+
+
+class HpglCokM2Params(C.Structure):
+    _fields_ = [("primary_cov", HpglCovParams), ("secondary_cov", HpglCovParams), ("radiuses", C.c_int * 3),
+                ("max_neighbours", C.c_int), ("primary_mean", C.c_double), ("secondary_mean", C.c_double),
+                ("correlation_coef", C.c_double)]
+
+
+def _cov_params(p):
+    cp = HpglCovParams()
+    cp.covariance_type = p["cov_type"]
+    cp.ranges[:] = p["ranges"]
+    cp.angles[:] = p["angles"]
+    cp.sill = p["sill"]
+    cp.nugget = p["nugget"]
+    return cp
+
+
+def cokriging(job, dumps=True, node_list=None, threads=0):
+    """Restated colocated simple cokriging (job kind "cok1" or "cok2", see
+    hpgl_b200.workloads.cokriging_job).  Returns out, out_mask and, with
+    ``dumps``, per node: status, nb_count, nb_index (cap per node), weights
+    (cap + 1 per node)."""
+    lib = restated()
+    mark = {"cok1": 1, "cok2": 2}[job["kind"]]
+    nx, ny, nz = job["shape"]
+    size = nx * ny * nz
+    p = job["params"][0]
+    cap = p["max_neighbours"]
+    values = np.ascontiguousarray(job["values"], dtype=np.float32)
+    mask = np.ascontiguousarray(job["mask"], dtype=np.uint8)
+    sv = np.ascontiguousarray(job["secondary_values"], dtype=np.float32)
+    sm = np.ascontiguousarray(job["secondary_mask"], dtype=np.uint8)
+    out, out_mask = values.copy(), mask.copy()
+    res = {}
+    if dumps:
+        res["status"] = np.full(size, -2, dtype=np.int8)
+        res["nb_count"] = np.full(size, -1, dtype=np.int32)
+        res["nb_index"] = np.full(size * cap, -1, dtype=np.int32)
+        res["weights"] = np.zeros(size * (cap + 1))
+    sp = oracle_params(job["secondary_cov"]) if mark == 2 else None
+    nl = None if node_list is None else np.ascontiguousarray(node_list, dtype=np.int32)
+    err = C.create_string_buffer(512)
+    rc = lib.oracle_cokriging(
+        mark, nx, ny, nz, _ptr(values, C.c_float), _ptr(mask, C.c_ubyte), _ptr(sv, C.c_float), _ptr(sm, C.c_ubyte),
+        C.byref(oracle_params(p)), None if sp is None else C.byref(sp), C.c_double(job["primary_mean"]),
+        C.c_double(job["secondary_mean"]), C.c_double(job.get("secondary_variance", 0.0)),
+        C.c_double(job["correlation"]), _ptr(out, C.c_float), _ptr(out_mask, C.c_ubyte),
+        _ptr(res.get("status"), C.c_byte), _ptr(res.get("nb_count"), C.c_int), _ptr(res.get("nb_index"), C.c_int),
+        _ptr(res.get("weights"), C.c_double), cap, _ptr(nl, C.c_int), 0 if nl is None else len(nl), threads, err, 512)
+    if rc != 0:
+        raise RuntimeError("oracle: " + err.value.decode())
+    res["out"] = out
+    res["out_mask"] = out_mask
+    res["cap"] = cap
+    return res
+
+
+def ref_cokriging(job):
+    """The compiled reference's hpgl_simple_cokriging_mark1/2 through its C
+    ABI, from a clone of the primary input like geo.py; returns (out, mask)."""
+    ref = reference()
+    sh = _shape(job["shape"])
+    p = job["params"][0]
+    values = np.array(job["values"], dtype=np.float32)
+    mask = np.array(job["mask"], dtype=np.uint8)
+    sv = np.array(job["secondary_values"], dtype=np.float32)
+    sm = np.array(job["secondary_mask"], dtype=np.uint8)
+    out, out_mask = values.copy(), mask.copy()
+    a = HpglContArray(_ptr(values, C.c_float), _ptr(mask, C.c_ubyte), sh)
+    s = HpglContArray(_ptr(sv, C.c_float), _ptr(sm, C.c_ubyte), sh)
+    b = HpglContArray(_ptr(out, C.c_float), _ptr(out_mask, C.c_ubyte), sh)
+    if job["kind"] == "cok1":
+        q = HpglCokM1Params()
+        base = _ok_params(p)
+        for name, _ in HpglOkParams._fields_:
+            setattr(q, name, getattr(base, name))
+        q.primary_mean = job["primary_mean"]
+        q.secondary_mean = job["secondary_mean"]
+        q.secondary_variance = job["secondary_variance"]
+        q.correlation_coef = job["correlation"]
+        ref.hpgl_simple_cokriging_mark1(C.byref(a), C.byref(s), C.byref(q), C.byref(b))
+    else:
+        q = HpglCokM2Params()
+        q.primary_cov = _cov_params(p)
+        q.secondary_cov = _cov_params(job["secondary_cov"])
+        q.radiuses[:] = p["radii"]
+        q.max_neighbours = p["max_neighbours"]
+        q.primary_mean = job["primary_mean"]
+        q.secondary_mean = job["secondary_mean"]
+        q.correlation_coef = job["correlation"]
+        ref.hpgl_simple_cokriging_mark2(C.byref(a), C.byref(s), C.byref(q), C.byref(b))
+    return out, out_mask
