@@ -429,13 +429,86 @@ void hpgl_sis_simulation_lvm(hpgl_ind_masked_array_t *, hpgl_ik_params_t *, hpgl
                              hpgl_ubyte_array_t *, int) {
     guarded("hpgl_sis_simulation_lvm", [&] { not_provided("sequential indicator simulation"); });
 }
-void hpgl_simple_cokriging_mark1(hpgl_cont_masked_array_t *, hpgl_cont_masked_array_t *, hpgl_cokriging_m1_params_t *,
-                                 hpgl_cont_masked_array_t *) {
-    guarded("hpgl_simple_cokriging_mark1", [&] { not_provided("simple cokriging"); });
+// hpgl_simple_cokriging_mark1/2 (api.cpp:587-713 of the reference): the
+// three arrays must have the same size (the reference raises otherwise).
+static void cokriging_sizes(const hpgl_cont_masked_array_t *a, const hpgl_cont_masked_array_t *b,
+                            const hpgl_cont_masked_array_t *c) {
+    if (!a || !b || !c) throw HpglError{HPGL_E_INVALID, "null array"};
+    if (volume(&a->m_shape) != volume(&b->m_shape))
+        throw HpglError{HPGL_E_INVALID, "size of secondary data is different from size of primary data"};
+    if (volume(&a->m_shape) != volume(&c->m_shape))
+        throw HpglError{HPGL_E_INVALID, "size of output data is different from size of primary data"};
 }
-void hpgl_simple_cokriging_mark2(hpgl_cont_masked_array_t *, hpgl_cont_masked_array_t *, hpgl_cokriging_m2_params_t *,
-                                 hpgl_cont_masked_array_t *) {
-    guarded("hpgl_simple_cokriging_mark2", [&] { not_provided("simple cokriging"); });
+
+void hpgl_simple_cokriging_mark1(hpgl_cont_masked_array_t *input_data, hpgl_cont_masked_array_t *secondary_data,
+                                 hpgl_cokriging_m1_params_t *params, hpgl_cont_masked_array_t *output_data) {
+    guarded("hpgl_simple_cokriging_mark1", [&] {
+        cokriging_sizes(input_data, secondary_data, output_data);
+        if (!params) throw HpglError{HPGL_E_INVALID, "params are null"};
+        hpgl_ik_params_t p;
+        memset(&p, 0, sizeof(p));
+        p.m_covariance_type = params->m_covariance_type;
+        for (int i = 0; i < 3; ++i) {
+            p.m_ranges[i] = params->m_ranges[i];
+            p.m_angles[i] = params->m_angles[i];
+            p.m_radiuses[i] = params->m_radiuses[i];
+        }
+        p.m_sill = params->m_sill;
+        p.m_nugget = params->m_nugget;
+        p.m_max_neighbours = params->m_max_neighbours;
+        hpgl_b200_job_t job = base_job(HPGL_KIND_COKRIGING_M1, &input_data->m_shape);
+        job.values = input_data->m_data;
+        job.mask = input_data->m_mask;
+        job.secondary_values = secondary_data->m_data;
+        job.secondary_mask = secondary_data->m_mask;
+        job.params = &p;
+        job.n_params = 1;
+        job.primary_mean = params->m_primary_mean;
+        job.secondary_mean = params->m_secondary_mean;
+        job.secondary_variance = params->m_secondary_variance;
+        job.correlation = params->m_correlation_coef;
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_values = output_data->m_data;
+        res.out_mask = output_data->m_mask;
+        run("Simple Colocated Cokriging Markov Model I", job, res);
+    });
+}
+
+void hpgl_simple_cokriging_mark2(hpgl_cont_masked_array_t *primary_data, hpgl_cont_masked_array_t *secondary_data,
+                                 hpgl_cokriging_m2_params_t *params, hpgl_cont_masked_array_t *output_data) {
+    guarded("hpgl_simple_cokriging_mark2", [&] {
+        cokriging_sizes(primary_data, secondary_data, output_data);
+        if (!params) throw HpglError{HPGL_E_INVALID, "params are null"};
+        const hpgl_cov_params_t &pc = params->m_primary_cov_params;
+        hpgl_ik_params_t p;
+        memset(&p, 0, sizeof(p));
+        p.m_covariance_type = pc.m_covariance_type;
+        for (int i = 0; i < 3; ++i) {
+            p.m_ranges[i] = pc.m_ranges[i];
+            p.m_angles[i] = pc.m_angles[i];
+            p.m_radiuses[i] = params->m_radiuses[i];
+        }
+        p.m_sill = pc.m_sill;
+        p.m_nugget = pc.m_nugget;
+        p.m_max_neighbours = params->m_max_neighbours;
+        hpgl_b200_job_t job = base_job(HPGL_KIND_COKRIGING_M2, &primary_data->m_shape);
+        job.values = primary_data->m_data;
+        job.mask = primary_data->m_mask;
+        job.secondary_values = secondary_data->m_data;
+        job.secondary_mask = secondary_data->m_mask;
+        job.params = &p;
+        job.n_params = 1;
+        job.primary_mean = params->m_primary_mean;
+        job.secondary_mean = params->m_secondary_mean;
+        job.correlation = params->m_correlation_coef;
+        job.secondary_cov = &params->m_secondary_cov_params;
+        hpgl_b200_result_t res;
+        memset(&res, 0, sizeof(res));
+        res.out_values = output_data->m_data;
+        res.out_mask = output_data->m_mask;
+        run("Simple Colocated Cokriging Markov Model II", job, res);
+    });
 }
 
 }  // extern "C"

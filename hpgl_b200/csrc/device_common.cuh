@@ -8,7 +8,8 @@ namespace hpgl_b200 {
 
 #define FULL_MASK 0xffffffffu
 
-__device__ __forceinline__ bool is_cont(int kind) { return kind <= 2; }
+// kinds with a continuous property: OK, SK, LVM and the two cokriging kinds
+__device__ __forceinline__ bool is_cont(int kind) { return kind <= 2 || kind == 5 || kind == 6; }
 
 // Covariance of offset v (grid steps) from the plan's table.  Truncated kinds
 // read 0 beyond the search radii (precalculated_covariance.h:60-75,

@@ -87,7 +87,8 @@ struct Group {
 
 struct Arena {
     size_t o_values, o_codes, o_mask, o_mean, o_out_values, o_out_codes, o_out_mask, o_probs, o_pk, o_status,
-        o_variance, o_weights, o_nb, o_nbcount, o_untouched, o_routed, o_counters, o_skey, o_sidx;
+        o_variance, o_weights, o_nb, o_nbcount, o_untouched, o_routed, o_counters, o_skey, o_sidx, o_svalues,
+        o_smask, o_cross;
     size_t total;
     long long cluster_warps;
 };
@@ -105,6 +106,10 @@ struct JobState {
     int nmax_all;
     bool want_variance, want_weights;
     long long kriged;
+    // cokriging
+    bool cok = false;
+    double cok_coef = 0, cok_svar = 0;
+    std::vector<double> cross_table;  // Markov model II: the secondary model's table
     Arena ar;
     char *base = nullptr;
 };
@@ -127,8 +132,10 @@ static KrigingParams to_params(const hpgl_ik_params_t &p) {
 static void invalid(const std::string &m) { throw HpglError{HPGL_E_INVALID, m}; }
 
 static void check_result(const JobState &S, const hpgl_b200_result_t &res) {
-    if (S.job.kind <= KIND_LVM && !res.out_values) invalid("out_values is null");
-    if (S.job.kind > KIND_LVM && !res.out_codes) invalid("out_codes is null");
+    if (kind_is_cont(S.job.kind) && !res.out_values) invalid("out_values is null");
+    if (!kind_is_cont(S.job.kind) && !res.out_codes) invalid("out_codes is null");
+    if (S.cok && res.weights && res.nb_stride < S.nmax_all + 1)
+        invalid("nb_stride smaller than max_neighbours + 1 (cokriging weights)");
     if (!res.out_mask) invalid("out_mask is null");
     if ((res.nb_index || res.weights) && res.nb_stride < S.nmax_all) invalid("nb_stride smaller than max_neighbours");
 }
@@ -138,19 +145,23 @@ static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 // Host planning and arena layout (no device work).
 static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_result_t &res) {
     S.job = job;
-    if (job.kind < 0 || job.kind > 4) invalid("unknown kriging kind");
+    if (job.kind < 0 || job.kind > 6) invalid("unknown kriging kind");
     if (job.nx <= 0 || job.ny <= 0 || job.nz <= 0) invalid("grid dimensions must be positive");
     S.size = (long long)job.nx * job.ny * job.nz;
     if (S.size > 2147483647LL) invalid("grid larger than 2^31-1 nodes (node indices are int, typedefs.h:112)");
     if (!job.mask) invalid("mask is null");
     if (!job.params || job.n_params < 1) invalid("params missing");
-    const bool cont = job.kind <= KIND_LVM;
+    const bool cont = kind_is_cont(job.kind);
+    S.cok = kind_is_cokriging(job.kind);
     if (cont && !job.values) invalid("values are null");
+    if (S.cok && (!job.secondary_values || !job.secondary_mask)) invalid("secondary property is null");
+    if (job.kind == KIND_COK2 && !job.secondary_cov) invalid("secondary covariance is null");
     if (!cont && !job.codes) invalid("codes are null");
     if (job.kind == KIND_LVM && !job.mean) invalid("mean cube is null");
     if (job.kind != KIND_IK && job.n_params != 1) invalid("exactly one params entry expected");
     if (job.kind == KIND_IK && job.n_params > 255) invalid("too many categories");
     S.precision = job.precision >= 0 ? job.precision : g_precision;
+    if (S.cok) S.precision = HPGL_PRECISION_FP64;  // cokriging is solved in the reference's order only
     if (S.precision != HPGL_PRECISION_FP64 && S.precision != HPGL_PRECISION_MIXED) invalid("unknown precision");
     S.K = job.kind == KIND_IK ? job.n_params : 1;
     std::vector<KrigingParams> kp;
@@ -181,6 +192,33 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
         throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
     } catch (const std::invalid_argument &e) {
         throw HpglError{HPGL_E_INVALID, e.what()};
+    }
+    if (S.cok) {
+        // cross covariance models (simple_cokriging_markI.cpp:140-181); the
+        // means are mean_t (float) in the reference
+        const Plan &P = S.groups[0].plan;
+        const double pv = P.c0;  // C(0) of the primary model
+        if (job.kind == KIND_COK1) {
+            S.cok_coef = job.correlation * sqrt(job.secondary_variance) / sqrt(pv);
+            S.cok_svar = job.secondary_variance;
+        } else {
+            KrigingParams sp = kp[0];
+            sp.cov_type = job.secondary_cov->m_covariance_type;
+            for (int i = 0; i < 3; ++i) {
+                sp.ranges[i] = job.secondary_cov->m_ranges[i];
+                sp.angles[i] = job.secondary_cov->m_angles[i];
+            }
+            sp.sill = job.secondary_cov->m_sill;
+            sp.nugget = job.secondary_cov->m_nugget;
+            try {
+                validate_params(sp, KIND_OK);
+            } catch (const std::invalid_argument &e) {
+                throw HpglError{HPGL_E_INVALID, std::string("secondary covariance: ") + e.what()};
+            }
+            S.cok_svar = CovModel(sp)(0.0, 0.0, 0.0);
+            S.cok_coef = job.correlation * sqrt(S.cok_svar / pv);
+            fill_cov_table(S.cross_table, P.B, sp, threads);
+        }
     }
     check_result(S, res);
     // The reference keeps marginal probabilities as float (ik_params.h:41,
@@ -219,7 +257,10 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     A.o_pk = take(S.K * 4);
     A.o_status = take(slots);
     A.o_variance = S.want_variance ? take(slots * 8) : 0;
-    A.o_weights = S.want_weights ? take(slots * S.nmax_all * 8) : 0;
+    A.o_weights = S.want_weights ? take(slots * (S.nmax_all + (S.cok ? 1 : 0)) * 8) : 0;
+    A.o_svalues = S.cok ? take(n * 4) : 0;
+    A.o_smask = S.cok ? take(n) : 0;
+    A.o_cross = S.cross_table.empty() ? 0 : take(S.cross_table.size() * 8);
     A.o_nb = take(n * (size_t)S.nmax_all * 4);
     A.o_nbcount = take(n * 4);
     A.o_untouched = take(n * 4);
@@ -264,13 +305,20 @@ static void upload(JobState &S, cudaStream_t s) {
     const size_t n = (size_t)S.size;
     const Arena &A = S.ar;
     CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_mask), job.mask, n, cudaMemcpyHostToDevice, s));
-    if (job.kind <= KIND_LVM)
+    if (kind_is_cont(job.kind))
         CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_values), job.values, n * 4, cudaMemcpyHostToDevice, s));
     else
         CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_codes), job.codes, n, cudaMemcpyHostToDevice, s));
     if (job.kind == KIND_LVM)
         CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_mean), job.mean, n * 4, cudaMemcpyHostToDevice, s));
     CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_pk), S.pk.data(), S.K * 4, cudaMemcpyHostToDevice, s));
+    if (S.cok) {
+        CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_svalues), job.secondary_values, n * 4, cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_smask), job.secondary_mask, n, cudaMemcpyHostToDevice, s));
+        if (!S.cross_table.empty())
+            CUDA_CHECK(cudaMemcpyAsync(at<double>(S, A.o_cross), S.cross_table.data(), S.cross_table.size() * 8,
+                                       cudaMemcpyHostToDevice, s));
+    }
     for (auto &g : S.groups) {
         const Plan &P = g.plan;
         if (!g.tmpl_dev.empty())
@@ -320,7 +368,7 @@ static void upload(JobState &S, cudaStream_t s) {
 static DevJob make_devjob(const JobState &S, const Group &g) {
     const hpgl_b200_job_t &job = S.job;
     const Arena &A = S.ar;
-    const bool cont = job.kind <= KIND_LVM;
+    const bool cont = kind_is_cont(job.kind);
     DevJob J;
     memset(&J, 0, sizeof(J));
     J.kind = job.kind;
@@ -359,6 +407,15 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.n_routed = &cnt->n_routed;
     J.n_fp64 = &cnt->n_fp64;
     J.err = &cnt->err;
+    if (S.cok) {
+        J.svalues = at<float>(S, A.o_svalues);
+        J.smask = at<uint8_t>(S, A.o_smask);
+        J.cross_table = S.cross_table.empty() ? g.dp.table : at<double>(S, A.o_cross);
+        J.cok_coef = S.cok_coef;
+        J.cok_svar = S.cok_svar;
+        J.cok_m1 = (float)job.primary_mean;
+        J.cok_m2 = (float)job.secondary_mean;
+    }
     return J;
 }
 
@@ -388,6 +445,20 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
         CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
         launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
         ++launches;
+        if (S.cok) {
+            // template search, then the cokriging systems (FP64, reference order)
+            launch_search_template(J, g.dp, s);
+            if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top0, s));
+            launch_cokriging(J, g.dp, s);
+            if (pt && gi == 0) {
+                CUDA_CHECK(cudaEventRecord(pt->top1, s));
+                CUDA_CHECK(cudaEventRecord(pt->resolve1, s));
+            }
+            launches += 2;
+            CUDA_CHECK(cudaGetLastError());
+            if (after_group) after_group(g);
+            continue;
+        }
         if (tune.schedule == SCHED_SPLIT) {
             launch_search_template(J, g.dp, s);
             ++launches;
@@ -465,7 +536,7 @@ static void download(const JobState &S, hpgl_b200_result_t &res, const Counters 
             saved_m[i] = res.out_mask[untouched[i]];
         }
     }
-    if (job.kind <= KIND_LVM)
+    if (kind_is_cont(job.kind))
         CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, A.o_out_values), n * 4, cudaMemcpyDeviceToHost, s));
     else
         CUDA_CHECK(cudaMemcpyAsync(res.out_codes, at<uint8_t>(S, A.o_out_codes), n, cudaMemcpyDeviceToHost, s));
@@ -477,9 +548,11 @@ static void download(const JobState &S, hpgl_b200_result_t &res, const Counters 
     if (res.probs && job.kind >= KIND_IK)
         CUDA_CHECK(cudaMemcpyAsync(res.probs, at<float>(S, A.o_probs), n * (job.kind == KIND_IK ? S.K : 1) * 4,
                                    cudaMemcpyDeviceToHost, s));
-    if (res.weights)
-        CUDA_CHECK(cudaMemcpy2DAsync(res.weights, (size_t)res.nb_stride * 8, at<double>(S, A.o_weights),
-                                     (size_t)S.nmax_all * 8, (size_t)S.nmax_all * 8, slots, cudaMemcpyDeviceToHost, s));
+    if (res.weights) {
+        const size_t wn = (size_t)S.nmax_all + (S.cok ? 1 : 0);
+        CUDA_CHECK(cudaMemcpy2DAsync(res.weights, (size_t)res.nb_stride * 8, at<double>(S, A.o_weights), wn * 8,
+                                     wn * 8, slots, cudaMemcpyDeviceToHost, s));
+    }
     CUDA_CHECK(cudaStreamSynchronize(s));
     for (int i = 0; i < cnt.n_untouched; ++i) {
         res.out_values[untouched[i]] = saved_v[i];
@@ -672,7 +745,7 @@ void autotune_job(const hpgl_b200_job_t &job, hpgl_b200_tune_t &rep) {
     std::vector<uint8_t> outc, outm;
     const size_t size = (size_t)job.nx * job.ny * job.nz;
     outm.assign(job.mask, job.mask + size);
-    if (job.kind <= KIND_LVM) {
+    if (kind_is_cont(job.kind)) {
         outv.assign(job.values, job.values + size);
         res.out_values = outv.data();
     } else {

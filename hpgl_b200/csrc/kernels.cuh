@@ -107,6 +107,13 @@ struct DevJob {
     // counters
     unsigned long long *n_fp64;
     int *err;
+    // colocated cokriging (kinds 5, 6)
+    const float *svalues;        // secondary property
+    const uint8_t *smask;
+    const double *cross_table;   // covariance of the cross model, laid out like DevPlan::table
+    double cok_coef;             // cross covariance = coef * cross_table
+    double cok_svar;             // secondary variance (the system's corner)
+    float cok_m1, cok_m2;        // primary and secondary means (float, mean_t)
 };
 
 // Launch tuning of the per-node kernels: the schedule (separate template
@@ -135,6 +142,8 @@ void launch_search_cluster(const DevJob &J, const DevPlan &P, double *scratch_ke
 void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                   int n_list_max, cudaStream_t s, int blocks_per_sm = 0);
 void launch_ik_argmax(const DevJob &J, cudaStream_t s);
+// cokriging.cu: colocated simple cokriging of every node (after the template search)
+void launch_cokriging(const DevJob &J, const DevPlan &P, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm);

@@ -220,7 +220,11 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     P.nz = nz;
     P.size = (long long)nx * ny * nz;
     P.nmax = p.max_neighbours;
-    P.truncated = kind != KIND_OK;
+    // Ordinary kriging and cokriging use the model itself; cokriging searches
+    // with neighbour_lookup_t alone (simple_cokriging_markI.cpp:201, no
+    // clusterizer).
+    P.truncated = kind != KIND_OK && !kind_is_cokriging(kind);
+    P.clusterizer = !kind_is_cokriging(kind);
     for (int i = 0; i < 3; ++i) P.radii[i] = p.radii[i];
     const int rx = p.radii[0], ry = p.radii[1], rz = p.radii[2];
 
@@ -372,6 +376,7 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
                             cand += count[b];
                         }
                 long long b = ((long long)cz * P.my + cy) * P.mx + cx;
+                if (!P.clusterizer) clean = false;
                 P.bucket_clean[b] = clean ? 1 : 0;
                 if (clean) {
                     P.any_clean = true;
@@ -406,6 +411,12 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     P.px = 32 * ((P.ext[0] + 31) / 32);
     P.nseg = (nx + 31) / 32;
     P.wpr = P.nseg + 2 * (P.px / 32) + 2;
+}
+
+void fill_cov_table(std::vector<double> &table, const int B[3], const KrigingParams &p, int threads) {
+    CovModel cov(p);
+    fill_symmetric(table, B[0], B[1], B[2], threads,
+                   [&](int x, int y, int z) { return cov((double)x, (double)y, (double)z); });
 }
 
 }  // namespace hpgl_b200

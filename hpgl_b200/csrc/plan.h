@@ -11,7 +11,10 @@
 
 namespace hpgl_b200 {
 
-enum Kind { KIND_OK = 0, KIND_SK = 1, KIND_LVM = 2, KIND_IK = 3, KIND_MEDIAN_IK = 4 };
+enum Kind { KIND_OK = 0, KIND_SK = 1, KIND_LVM = 2, KIND_IK = 3, KIND_MEDIAN_IK = 4, KIND_COK1 = 5, KIND_COK2 = 6 };
+inline bool kind_is_cokriging(int k) { return k == KIND_COK1 || k == KIND_COK2; }
+// kinds with a continuous property (values in, values out)
+inline bool kind_is_cont(int k) { return k <= KIND_LVM || kind_is_cokriging(k); }
 
 struct KrigingParams {
     int cov_type;
@@ -48,6 +51,7 @@ struct Plan {
     long long size = 0;
     int nmax = 0;            // max_neighbours
     bool truncated = false;  // covariance returns 0 outside +-radii (SK, LVM, IK, median IK)
+    bool clusterizer = true; // the search may take the clusterizer path (not for cokriging)
     int radii[3] = {0, 0, 0};
 
     // sorted search template (covariance_field.h:62-106)
@@ -83,6 +87,9 @@ void validate_params(const KrigingParams &p, int kind);
 // Builds the plan of one kind/params over the informed `mask` (size nx*ny*nz).
 void build_plan(Plan &plan, int kind, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
                 int threads);
+
+// C(v) of `p`'s model over the box +-B, laid out like Plan::table.
+void fill_cov_table(std::vector<double> &table, const int B[3], const KrigingParams &p, int threads);
 
 // True when two categories' parameters give identical searches and systems.
 bool same_system(const KrigingParams &a, const KrigingParams &b);

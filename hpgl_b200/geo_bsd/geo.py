@@ -1,7 +1,8 @@
 """Kriging entry points with the names and arguments of the reference's
 geo_bsd/geo.py (Python 2) — ``ordinary_kriging`` (geo.py:381-399),
 ``simple_kriging`` (:401-425), ``lvm_kriging`` (:427-450), ``median_ik``
-(:452-469), ``indicator_kriging`` (:489-509), ``simple_kriging_weights``
+(:452-469), ``indicator_kriging`` (:489-509), ``simple_cokriging_markI``
+(:512-534), ``simple_cokriging_markII`` (:536-572), ``simple_kriging_weights``
 (:568-600) — plus the property, grid and covariance classes they take
 (:85-166) and the thread/handler settings (:364-368, 602-618).
 
@@ -17,12 +18,13 @@ import ctypes as C
 
 import numpy
 
-from .hpgl_wrap import (_HPGL_CONT_MASKED_ARRAY, _HPGL_COV_PARAMS, _HPGL_IK_PARAMS, _HPGL_IND_MASKED_ARRAY,
+from .hpgl_wrap import (_HPGL_COKRIGING_M1_PARAMS, _HPGL_COKRIGING_M2_PARAMS, _HPGL_CONT_MASKED_ARRAY, _HPGL_COV_PARAMS, _HPGL_IK_PARAMS, _HPGL_IND_MASKED_ARRAY,
                         _HPGL_MEDIAN_IK_PARAMS, _HPGL_OK_PARAMS, _HPGL_SHAPE, _HPGL_SK_PARAMS, HpglError, _hpgl_so,
                         check_last_error, hpgl_output_handler, hpgl_progress_handler)
 
 __all__ = ["ContProperty", "IndProperty", "SugarboxGrid", "CovarianceModel", "covariance", "ordinary_kriging",
            "simple_kriging", "lvm_kriging", "median_ik", "indicator_kriging", "simple_kriging_weights",
+           "simple_cokriging_markI", "simple_cokriging_markII",
            "set_thread_num", "get_thread_num", "set_output_handler", "set_progress_handler", "calc_mean",
            "set_precision", "get_precision", "HpglError"]
 
@@ -275,6 +277,44 @@ def indicator_kriging(prop, grid, data, marginal_probs, precision=None):
     with _Precision(precision):
         _hpgl_so.hpgl_indicator_kriging(C.byref(inp), C.byref(outp), params, len(data))
         check_last_error()
+    return out_prop
+
+
+def _cov_fields(cov_model):
+    return dict(covariance_type=cov_model.type, ranges=_c_array(C.c_double, 3, cov_model.ranges),
+                angles=_c_array(C.c_double, 3, cov_model.angles), sill=cov_model.sill, nugget=cov_model.nugget)
+
+
+def simple_cokriging_markI(prop, grid, secondary_data, primary_mean, secondary_mean, secondary_variance,
+                           correlation_coef, radiuses, max_neighbours, cov_model):
+    """Colocated simple cokriging, Markov model I (always the reference's FP64 arithmetic)."""
+    prop = _tuple_to_prop(prop)
+    secondary_data = _tuple_to_prop(secondary_data)
+    out_prop = _clone_prop(prop)
+    p = _HPGL_COKRIGING_M1_PARAMS(primary_mean=primary_mean, secondary_mean=secondary_mean,
+                                  secondary_variance=secondary_variance, correlation_coef=correlation_coef,
+                                  **_kriging_fields(cov_model, radiuses, max_neighbours))
+    inp, sec, outp = _cont_array(prop, grid), _cont_array(secondary_data, grid), _cont_array(out_prop, grid)
+    _hpgl_so.hpgl_simple_cokriging_mark1(C.byref(inp), C.byref(sec), C.byref(p), C.byref(outp))
+    check_last_error()
+    return out_prop
+
+
+def simple_cokriging_markII(grid, primary_data, secondary_data, correlation_coef, radiuses, max_neighbours):
+    """Colocated simple cokriging, Markov model II.  ``primary_data`` and
+    ``secondary_data`` are dicts with "data" (a property), "mean" and
+    "cov_model", as in the reference."""
+    prim = _tuple_to_prop(primary_data["data"])
+    sec = _tuple_to_prop(secondary_data["data"])
+    out_prop = _clone_prop(prim)
+    p = _HPGL_COKRIGING_M2_PARAMS(
+        primary_cov_params=_HPGL_COV_PARAMS(**_cov_fields(primary_data["cov_model"])),
+        secondary_cov_params=_HPGL_COV_PARAMS(**_cov_fields(secondary_data["cov_model"])),
+        radiuses=_c_array(C.c_int, 3, radiuses), max_neighbours=max_neighbours,
+        primary_mean=primary_data["mean"], secondary_mean=secondary_data["mean"], correlation_coef=correlation_coef)
+    inp, secp, outp = _cont_array(prim, grid), _cont_array(sec, grid), _cont_array(out_prop, grid)
+    _hpgl_so.hpgl_simple_cokriging_mark2(C.byref(inp), C.byref(secp), C.byref(p), C.byref(outp))
+    check_last_error()
     return out_prop
 
 

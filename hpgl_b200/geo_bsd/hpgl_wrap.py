@@ -53,6 +53,17 @@ class _HPGL_COV_PARAMS(C.Structure):
                 ("sill", C.c_double), ("nugget", C.c_double)]
 
 
+class _HPGL_COKRIGING_M1_PARAMS(C.Structure):
+    _fields_ = _KRIGING_FIELDS + [("primary_mean", C.c_double), ("secondary_mean", C.c_double),
+                                  ("secondary_variance", C.c_double), ("correlation_coef", C.c_double)]
+
+
+class _HPGL_COKRIGING_M2_PARAMS(C.Structure):
+    _fields_ = [("primary_cov_params", _HPGL_COV_PARAMS), ("secondary_cov_params", _HPGL_COV_PARAMS),
+                ("radiuses", C.c_int * 3), ("max_neighbours", C.c_int), ("primary_mean", C.c_double),
+                ("secondary_mean", C.c_double), ("correlation_coef", C.c_double)]
+
+
 _LIB_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 _hpgl_so = NC.load_library("hpgl", _LIB_DIR)
 
@@ -98,6 +109,15 @@ _hpgl_so.hpgl_median_ik.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.POINTER
 _hpgl_so.hpgl_indicator_kriging.restype = None
 _hpgl_so.hpgl_indicator_kriging.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.POINTER(_HPGL_IND_MASKED_ARRAY),
                                             C.POINTER(_HPGL_IK_PARAMS), C.c_int]
+
+_hpgl_so.hpgl_simple_cokriging_mark1.restype = None
+_hpgl_so.hpgl_simple_cokriging_mark1.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_CONT_MASKED_ARRAY),
+                                                 C.POINTER(_HPGL_COKRIGING_M1_PARAMS),
+                                                 C.POINTER(_HPGL_CONT_MASKED_ARRAY)]
+_hpgl_so.hpgl_simple_cokriging_mark2.restype = None
+_hpgl_so.hpgl_simple_cokriging_mark2.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_CONT_MASKED_ARRAY),
+                                                 C.POINTER(_HPGL_COKRIGING_M2_PARAMS),
+                                                 C.POINTER(_HPGL_CONT_MASKED_ARRAY)]
 
 _hpgl_so.hpgl_set_thread_num.restype = None
 _hpgl_so.hpgl_set_thread_num.argtypes = [C.c_int]

@@ -15,7 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "hpgl.so")
 
-KINDS = {"ok": 0, "sk": 1, "lvm": 2, "ik": 3, "median_ik": 4}
+KINDS = {"ok": 0, "sk": 1, "lvm": 2, "ik": 3, "median_ik": 4, "cok1": 5, "cok2": 6}
+CONT_KINDS = ("ok", "sk", "lvm", "cok1", "cok2")
 PRECISION = {"fp64": 0, "mixed": 1}
 
 HPGL_OK = 0
@@ -42,7 +43,10 @@ class Job(C.Structure):
                 ("mask", C.POINTER(C.c_ubyte)), ("mean", C.POINTER(C.c_float)),
                 ("params", C.POINTER(HpglIkParams)), ("n_params", C.c_int),
                 ("sk_automatic_mean", C.c_int), ("sk_mean", C.c_double), ("median_marginal1", C.c_double),
-                ("precision", C.c_int)]
+                ("precision", C.c_int),
+                ("secondary_values", C.POINTER(C.c_float)), ("secondary_mask", C.POINTER(C.c_ubyte)),
+                ("primary_mean", C.c_double), ("secondary_mean", C.c_double), ("secondary_variance", C.c_double),
+                ("correlation", C.c_double), ("secondary_cov", C.c_void_p)]
 
 
 class Result(C.Structure):
@@ -119,7 +123,8 @@ class _Prepared:
         self.kind = kind or job["kind"]
         nx, ny, nz = job["shape"]
         self.size = nx * ny * nz
-        self.cont = self.kind in ("ok", "sk", "lvm")
+        self.cont = self.kind in CONT_KINDS
+        self.cok = self.kind in ("cok1", "cok2")
         self.params = job["params"] if self.kind == "ik" else job["params"][:1]
         self.K = len(self.params) if self.kind == "ik" else 1
         self.pk = make_params(self.params)
@@ -141,10 +146,23 @@ class _Prepared:
         m1 = job.get("median_marginal1", 0.5) if median_marginal1 is None else median_marginal1
         j.median_marginal1 = m1
         j.precision = -1 if precision is None else PRECISION.get(precision, precision)
+        if self.cok:
+            self.svalues = np.ascontiguousarray(job["secondary_values"], dtype=np.float32)
+            self.smask = np.ascontiguousarray(job["secondary_mask"], dtype=np.uint8)
+            j.secondary_values = _ptr(self.svalues, C.c_float)
+            j.secondary_mask = _ptr(self.smask, C.c_ubyte)
+            j.primary_mean = job["primary_mean"]
+            j.secondary_mean = job["secondary_mean"]
+            j.secondary_variance = job.get("secondary_variance", 0.0)
+            j.correlation = job["correlation"]
+            if self.kind == "cok2":
+                self.scov = cov_struct(job["secondary_cov"])
+                j.secondary_cov = C.cast(C.pointer(self.scov), C.c_void_p)
         self.job = j
         self.out = self.values.copy() if self.cont else self.codes.copy()
         self.out_mask = self.mask.copy()
-        cap = max(p["max_neighbours"] for p in self.params)
+        # list stride; cokriging weights hold one more (the secondary's)
+        cap = max(p["max_neighbours"] for p in self.params) + (1 if self.cok else 0)
         per_cat = self.kind == "ik" and any(
             (p["cov_type"], tuple(p["ranges"]), tuple(p["angles"]), p["sill"], p["nugget"], tuple(p["radii"]),
              p["max_neighbours"]) != (self.params[0]["cov_type"], tuple(self.params[0]["ranges"]),

@@ -258,6 +258,8 @@ int hpgl_b200_get_precision(void);
 #define HPGL_KIND_LVM 2
 #define HPGL_KIND_IK 3
 #define HPGL_KIND_MEDIAN_IK 4
+#define HPGL_KIND_COKRIGING_M1 5  /* colocated simple cokriging, Markov model I */
+#define HPGL_KIND_COKRIGING_M2 6  /* colocated simple cokriging, Markov model II */
 
 /* One kriging job for hpgl_b200_krige.  `params` holds `n_params` entries
    (one per category for IK, else 1); hpgl_ik_params_t carries every field
@@ -275,6 +277,15 @@ typedef struct hpgl_b200_job_t {
     double sk_mean;               /* SK: mean when not automatic */
     double median_marginal1;      /* median IK: marginal probability of code 1 */
     int precision;                /* HPGL_PRECISION_*, or -1 for the global one */
+    /* colocated simple cokriging (HPGL_KIND_COKRIGING_M1 / _M2): `values` and
+       `mask` are the primary property, params[0] its covariance and search;
+       always solved in FP64 in the reference's operation order */
+    const float *secondary_values;
+    const unsigned char *secondary_mask;
+    double primary_mean, secondary_mean;
+    double secondary_variance;    /* Markov model I: variance of the secondary */
+    double correlation;           /* correlation coefficient of the two */
+    const hpgl_cov_params_t *secondary_cov;  /* Markov model II: secondary covariance */
 } hpgl_b200_job_t;
 
 /* Outputs of hpgl_b200_krige.  out_values (cont) or out_codes (IK) and
@@ -285,7 +296,9 @@ typedef struct hpgl_b200_job_t {
    status       int8     0 solved, 1 no neighbours, 2 singular, -1 not kriged
    nb_count     int32    neighbour count
    nb_index     int32    neighbour node indices, nb_stride per slot
-   weights      double   kriging weights, nb_stride per slot
+   weights      double   kriging weights, nb_stride per slot (cokriging: the
+                         neighbours' then the secondary's, so nb_stride must
+                         be >= max_neighbours + 1)
    probs        float    IK: probability per node*K + k; median IK: per node
    nb_stride must be >= max_neighbours when nb_index or weights is given. */
 typedef struct hpgl_b200_result_t {
