@@ -7,11 +7,13 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/hpgl.h"
 #include "engine.h"
 #include "kernels.cuh"
 #include "plan.h"
+#include "textio.h"
 
 using namespace hpgl_b200;
 
@@ -98,6 +100,53 @@ void run(const char *name, hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
 void not_provided(const char *what) {
     throw HpglError{HPGL_E_UNSUPPORTED, std::string(what) + " is not provided by this build (kriging path only)"};
 }
+}  // namespace
+
+namespace {
+// The INC / GSLIB entry points' errors keep the reference's own messages, "where: what".
+template <typename F>
+void guarded_io(const char *where, F f) {
+    try {
+        f();
+        set_error(HPGL_OK, "");
+    } catch (const HpglError &e) {
+        set_error(e.code, e.message);
+    } catch (const std::bad_alloc &) {
+        set_error(HPGL_E_CAPACITY, std::string(where) + ": out of host memory");
+    } catch (const std::exception &e) {
+        set_error(HPGL_E_INTERNAL, std::string(where) + ": " + e.what());
+    } catch (...) {
+        set_error(HPGL_E_INTERNAL, std::string(where) + ": unknown error");
+    }
+}
+
+// init_remap_table (api.cpp:117-136 of the reference): the indicator values
+// that the bytes 0..indicator_count-1 are written as.
+std::vector<unsigned char> remap_table(const unsigned char *values, int values_count, int indicator_count) {
+    std::vector<unsigned char> t;
+    if (values_count > 0 && !values) throw HpglError{HPGL_E_INVALID, "values are null"};
+    if (values_count == indicator_count) {
+        t.assign(values, values + values_count);
+    } else if (values_count > indicator_count) {
+        log_line("Given " + std::to_string(values_count) + " values for " + std::to_string(indicator_count) +
+                 " indicators. Ignoring extra values.\n");
+        t.assign(values, values + indicator_count);
+    } else {
+        if (values_count > 0)
+            log_line("Warning: Given " + std::to_string(values_count) + " values for " +
+                     std::to_string(indicator_count) + " indicators. Ignoring values. Using [0, 1, 2 ..]\n");
+        for (int i = 0; i < indicator_count; ++i) t.push_back((unsigned char)i);
+    }
+    return t;
+}
+
+// (unsigned char) of a double as the x86-64 compilers convert it: through a
+// 32-bit integer, keeping the low byte.
+unsigned char byte_of_double(double v) {
+    if (!(v > -2147483649.0 && v < 2147483648.0)) return 0;
+    return (unsigned char)(unsigned)(int)v;
+}
+
 }  // namespace
 
 extern "C" {
@@ -395,25 +444,69 @@ int hpgl_b200_simple_kriging_weights_static(float *center_coords, float *neighbo
     return rc == HPGL_OK ? 0 : -1;
 }
 
-void hpgl_read_inc_file_float(char *, float, int, float *, unsigned char *) {
-    guarded("hpgl_read_inc_file_float", [&] { not_provided("INC file reading"); });
+// INC / GSLIB property files (api.cpp:54-193 of the reference; textio.cu).
+void hpgl_read_inc_file_float(char *filename, float undefined_value, int size, float *data, unsigned char *mask) {
+    guarded_io("hpgl_read_inc_file_float", [&] {
+        inc_read(filename, false, undefined_value, 0, size, data, nullptr, mask, nullptr, 0, nullptr);
+    });
 }
-void hpgl_read_inc_file_byte(char *, int, int, unsigned char *, unsigned char *, unsigned char *, int) {
-    guarded("hpgl_read_inc_file_byte", [&] { not_provided("INC file reading"); });
+void hpgl_read_inc_file_byte(char *filename, int undefined_value, int size, unsigned char *data, unsigned char *mask,
+                             unsigned char *values, int values_count) {
+    guarded_io("hpgl_read_inc_file_byte", [&] {
+        inc_read(filename, true, 0.f, undefined_value, size, nullptr, data, mask, values, values_count, nullptr);
+    });
 }
-void hpgl_write_inc_file_float(char *, hpgl_cont_masked_array_t *, float, char *) {
-    guarded("hpgl_write_inc_file_float", [&] { not_provided("INC file writing"); });
+void hpgl_write_inc_file_float(char *filename, hpgl_cont_masked_array_t *arr, float undefined_value, char *name) {
+    guarded_io("hpgl_write_inc_file_float", [&] {
+        if (!arr) throw HpglError{HPGL_E_INVALID, "hpgl_write_inc_file_float: array is null"};
+        prop_write(0, false, filename, name, arr->m_data, nullptr, arr->m_mask, volume(&arr->m_shape), undefined_value,
+                   0, nullptr, 0, nullptr);
+    });
 }
-void hpgl_write_inc_file_byte(char *, hpgl_ind_masked_array_t *, int, char *, unsigned char *, int) {
-    guarded("hpgl_write_inc_file_byte", [&] { not_provided("INC file writing"); });
+void hpgl_write_inc_file_byte(char *filename, hpgl_ind_masked_array_t *arr, int undefined_value, char *name,
+                              unsigned char *values, int values_count) {
+    guarded_io("hpgl_write_inc_file_byte", [&] {
+        if (!arr) throw HpglError{HPGL_E_INVALID, "hpgl_write_inc_file_byte: array is null"};
+        const std::vector<unsigned char> t = remap_table(values, values_count, arr->m_indicator_count);
+        prop_write(0, true, filename, name, nullptr, arr->m_data, arr->m_mask, volume(&arr->m_shape), 0.f,
+                   (unsigned char)undefined_value, t.data(), (int)t.size(), nullptr);
+    });
 }
-void hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *, const char *, const char *, double) {
-    guarded("hpgl_write_gslib_cont_property", [&] { not_provided("GSLIB writing"); });
+void hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *data, const char *filename, const char *name,
+                                    double undefined_value) {
+    guarded_io("hpgl_write_gslib_cont_property", [&] {
+        if (!data) throw HpglError{HPGL_E_INVALID, "hpgl_write_gslib_cont_property: array is null"};
+        prop_write(1, false, filename, name, data->m_data, nullptr, data->m_mask, volume(&data->m_shape),
+                   (float)undefined_value, 0, nullptr, 0, nullptr);
+    });
 }
-void hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *, const char *, const char *, double, unsigned char *,
-                                    int) {
-    guarded("hpgl_write_gslib_byte_property", [&] { not_provided("GSLIB writing"); });
+void hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *data, const char *filename, const char *name,
+                                    double undefined_value, unsigned char *values, int values_count) {
+    guarded_io("hpgl_write_gslib_byte_property", [&] {
+        if (!data) throw HpglError{HPGL_E_INVALID, "hpgl_write_gslib_byte_property: array is null"};
+        const std::vector<unsigned char> t = remap_table(values, values_count, data->m_indicator_count);
+        prop_write(1, true, filename, name, nullptr, data->m_data, data->m_mask, volume(&data->m_shape), 0.f,
+                   byte_of_double(undefined_value), t.data(), (int)t.size(), nullptr);
+    });
 }
+long long hpgl_b200_inc_count_values(const char *filename) {
+    long long n = -1;
+    guarded_io("hpgl_b200_inc_count_values", [&] { n = inc_count(filename, false, nullptr); });
+    return n;
+}
+
+void hpgl_b200_io_last_timing(hpgl_b200_io_timing_t *out) {
+    if (!out) return;
+    const TextIoTiming t = last_io_timing();
+    out->ms_file = t.ms_file;
+    out->ms_h2d = t.ms_h2d;
+    out->ms_device = t.ms_device;
+    out->ms_d2h = t.ms_d2h;
+    out->ms_total = t.ms_total;
+    out->bytes = t.bytes;
+    out->tokens = t.tokens;
+}
+
 void hpgl_sgs_simulation(hpgl_cont_masked_array_t *, hpgl_sgs_params_t *, hpgl_non_parametric_cdf_t *, double *,
                          hpgl_ubyte_array_t *) {
     guarded("hpgl_sgs_simulation", [&] { not_provided("sequential Gaussian simulation"); });

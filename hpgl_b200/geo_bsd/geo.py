@@ -4,21 +4,37 @@ geo_bsd/geo.py (Python 2) — ``ordinary_kriging`` (geo.py:381-399),
 (:452-469), ``indicator_kriging`` (:489-509), ``simple_cokriging_markI``
 (:512-534), ``simple_cokriging_markII`` (:536-572), ``simple_kriging_weights``
 (:568-600) — plus the property, grid and covariance classes they take
-(:85-166) and the thread/handler settings (:364-368, 602-618).
+(:85-166), the thread/handler settings (:364-368, 602-618) and the INC /
+GSLIB property files: ``write_property`` (:277-305), ``write_gslib_property``
+(:307-322), ``load_cont_property`` (:324-329), ``read_inc_file_float``
+(:331-342), ``read_inc_file_byte`` (:344-355), ``load_ind_property``
+(:357-362), ``get_gslib_property`` (:608-616).
 
 Differences from the reference, all additive:
 * every call checks the library's last-error state and raises
   ``HpglError`` (the reference's C++ exceptions crossed the C boundary);
 * each kriging call takes an optional ``precision`` keyword ("fp64" — the
   reference's arithmetic, bit for bit — or "mixed"); None uses the library
-  default (``set_precision``).
+  default (``set_precision``);
+* ``load_cont_property`` / ``load_ind_property`` without ``size`` read the
+  file's values with the same INC rules as with a size (the count comes
+  from ``hpgl_b200_inc_count_values``), where the reference switched to a
+  pure-Python reader with looser rules; the result is one-dimensional, as
+  the reference's was;
+* ``write_property`` of an indicator property passes ``indicator_values``
+  as bytes (the reference handed the bytes of an int64 array to a uint8
+  pointer, so the table it wrote through held the low bytes of its first
+  values' int64 words);
+* file names and property names may be ``str`` (encoded with
+  ``os.fsencode`` / UTF-8) or ``bytes``.
 """
 
 import ctypes as C
+import os
 
 import numpy
 
-from .hpgl_wrap import (_HPGL_COKRIGING_M1_PARAMS, _HPGL_COKRIGING_M2_PARAMS, _HPGL_CONT_MASKED_ARRAY, _HPGL_COV_PARAMS, _HPGL_IK_PARAMS, _HPGL_IND_MASKED_ARRAY,
+from .hpgl_wrap import (_HPGL_B200_IO_TIMING, _HPGL_COKRIGING_M1_PARAMS, _HPGL_COKRIGING_M2_PARAMS, _HPGL_CONT_MASKED_ARRAY, _HPGL_COV_PARAMS, _HPGL_IK_PARAMS, _HPGL_IND_MASKED_ARRAY,
                         _HPGL_MEDIAN_IK_PARAMS, _HPGL_OK_PARAMS, _HPGL_SHAPE, _HPGL_SK_PARAMS, HpglError, _hpgl_so,
                         check_last_error, hpgl_output_handler, hpgl_progress_handler)
 
@@ -26,7 +42,9 @@ __all__ = ["ContProperty", "IndProperty", "SugarboxGrid", "CovarianceModel", "co
            "simple_kriging", "lvm_kriging", "median_ik", "indicator_kriging", "simple_kriging_weights",
            "simple_cokriging_markI", "simple_cokriging_markII",
            "set_thread_num", "get_thread_num", "set_output_handler", "set_progress_handler", "calc_mean",
-           "set_precision", "get_precision", "HpglError"]
+           "set_precision", "get_precision", "HpglError", "write_property", "write_gslib_property",
+           "load_cont_property", "read_inc_file_float", "read_inc_file_byte", "load_ind_property",
+           "get_gslib_property", "io_last_timing"]
 
 _PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -376,3 +394,109 @@ def set_progress_handler(handler, param):
         h = hpgl_progress_handler(handler)
         _handlers["progress"] = h
         _hpgl_so.hpgl_set_progress_handler(h, param)
+
+
+# ---- INC / GSLIB property files ---------------------------------------------
+
+def _fs(name):
+    return name if isinstance(name, bytes) else os.fsencode(name)
+
+
+def _text(name):
+    return name if isinstance(name, bytes) else str(name).encode("utf-8")
+
+
+def _file_shape(data):
+    return data.shape if data.ndim == 3 else (data.size, 1, 1)
+
+
+def _ubyte_ptr(values):
+    arr = numpy.ascontiguousarray(numpy.array(values, dtype="uint8").reshape(-1))
+    return arr, arr.ctypes.data_as(C.POINTER(C.c_ubyte)), arr.size
+
+
+def write_property(prop, filename, prop_name, undefined_value, indicator_values=[]):
+    """INC file of a property: name line, one value per cell, "/"."""
+    prop = _tuple_to_prop(prop)
+    sh = _create_hpgl_shape(_file_shape(prop.data))
+    if isinstance(prop, ContProperty):
+        marr = _HPGL_CONT_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_float)),
+                                       mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh)
+        _hpgl_so.hpgl_write_inc_file_float(_fs(filename), C.byref(marr), undefined_value, _text(prop_name))
+    else:
+        marr = _HPGL_IND_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                      mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh,
+                                      indicator_count=prop.indicator_count)
+        keep, ptr, n = _ubyte_ptr(indicator_values)
+        _hpgl_so.hpgl_write_inc_file_byte(_fs(filename), C.byref(marr), int(undefined_value), _text(prop_name), ptr, n)
+    check_last_error()
+
+
+def write_gslib_property(prop, filename, prop_name, undefined_value, indicator_values=[]):
+    """GSLIB file of a property: "HPGL saved GSLIB file", "1", name, values."""
+    prop = _tuple_to_prop(prop)
+    sh = _create_hpgl_shape(_file_shape(prop.data))
+    if isinstance(prop, ContProperty):
+        marr = _HPGL_CONT_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_float)),
+                                       mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh)
+        _hpgl_so.hpgl_write_gslib_cont_property(C.byref(marr), _fs(filename), _text(prop_name), undefined_value)
+    else:
+        marr = _HPGL_IND_MASKED_ARRAY(data=prop.data.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                      mask=prop.mask.ctypes.data_as(C.POINTER(C.c_ubyte)), shape=sh,
+                                      indicator_count=prop.indicator_count)
+        keep, ptr, n = _ubyte_ptr(indicator_values)
+        _hpgl_so.hpgl_write_gslib_byte_property(C.byref(marr), _fs(filename), _text(prop_name), undefined_value,
+                                                ptr, n)
+    check_last_error()
+
+
+def _count_values(filename):
+    n = _hpgl_so.hpgl_b200_inc_count_values(_fs(filename))
+    check_last_error()
+    return int(n)
+
+
+def read_inc_file_float(filename, undefined_value, size):
+    """`size` = (nx, ny, nz): a ContProperty of that shape (Fortran order)."""
+    data = numpy.zeros(size, dtype="float32", order="F")
+    mask = numpy.zeros(size, dtype="uint8", order="F")
+    _hpgl_so.hpgl_read_inc_file_float(_fs(filename), undefined_value, int(data.size), data, mask)
+    check_last_error()
+    return ContProperty(data, mask)
+
+
+def read_inc_file_byte(filename, undefined_value, size, indicator_values):
+    """`size` = (nx, ny, nz): an IndProperty whose informed values are the
+    indices of the file's values in `indicator_values`."""
+    data = numpy.zeros(size, dtype="uint8", order="F")
+    mask = numpy.zeros(size, dtype="uint8", order="F")
+    values = numpy.array(indicator_values, dtype="uint8").reshape(-1)
+    _hpgl_so.hpgl_read_inc_file_byte(_fs(filename), int(undefined_value), int(data.size), data, mask, values,
+                                     len(values))
+    check_last_error()
+    return IndProperty(data, mask, len(indicator_values))
+
+
+def load_cont_property(filename, undefined_value, size=None):
+    if size is None:
+        return read_inc_file_float(filename, undefined_value, (_count_values(filename),))
+    return read_inc_file_float(filename, undefined_value, size)
+
+
+def load_ind_property(filename, undefined_value, indicator_values, size=None):
+    if size is None:
+        return read_inc_file_byte(filename, undefined_value, (_count_values(filename),), indicator_values)
+    return read_inc_file_byte(filename, undefined_value, size, indicator_values)
+
+
+def get_gslib_property(prop_dict, prop_name, undefined_value):
+    """(values, informed mask) of one column of a GSLIB table held as a dict."""
+    prop = prop_dict[prop_name]
+    return (prop, (numpy.asarray(prop) != undefined_value).astype(numpy.uint8))
+
+
+def io_last_timing():
+    """Timings (ms) and sizes of this process's last INC/GSLIB call."""
+    t = _HPGL_B200_IO_TIMING()
+    _hpgl_so.hpgl_b200_io_last_timing(C.byref(t))
+    return {k: getattr(t, k) for k, _ in t._fields_}

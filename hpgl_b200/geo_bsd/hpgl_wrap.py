@@ -119,6 +119,36 @@ _hpgl_so.hpgl_simple_cokriging_mark2.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARR
                                                  C.POINTER(_HPGL_COKRIGING_M2_PARAMS),
                                                  C.POINTER(_HPGL_CONT_MASKED_ARRAY)]
 
+_hpgl_so.hpgl_read_inc_file_float.restype = None
+_hpgl_so.hpgl_read_inc_file_float.argtypes = [C.c_char_p, C.c_float, C.c_int, NC.ndpointer(dtype=numpy.float32, flags=_F),
+                                              NC.ndpointer(dtype=numpy.ubyte, flags=_F)]
+_hpgl_so.hpgl_read_inc_file_byte.restype = None
+_hpgl_so.hpgl_read_inc_file_byte.argtypes = [C.c_char_p, C.c_int, C.c_int, NC.ndpointer(dtype=numpy.ubyte, flags=_F),
+                                             NC.ndpointer(dtype=numpy.ubyte, flags=_F),
+                                             NC.ndpointer(dtype=numpy.ubyte, flags=_F), C.c_int]
+_hpgl_so.hpgl_write_inc_file_float.restype = None
+_hpgl_so.hpgl_write_inc_file_float.argtypes = [C.c_char_p, C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.c_float, C.c_char_p]
+_hpgl_so.hpgl_write_inc_file_byte.restype = None
+_hpgl_so.hpgl_write_inc_file_byte.argtypes = [C.c_char_p, C.POINTER(_HPGL_IND_MASKED_ARRAY), C.c_int, C.c_char_p,
+                                              C.POINTER(C.c_ubyte), C.c_int]
+_hpgl_so.hpgl_write_gslib_cont_property.restype = None
+_hpgl_so.hpgl_write_gslib_cont_property.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.c_char_p, C.c_char_p,
+                                                    C.c_double]
+_hpgl_so.hpgl_write_gslib_byte_property.restype = None
+_hpgl_so.hpgl_write_gslib_byte_property.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.c_char_p, C.c_char_p,
+                                                    C.c_double, C.POINTER(C.c_ubyte), C.c_int]
+_hpgl_so.hpgl_b200_inc_count_values.restype = C.c_longlong
+_hpgl_so.hpgl_b200_inc_count_values.argtypes = [C.c_char_p]
+
+
+class _HPGL_B200_IO_TIMING(C.Structure):
+    _fields_ = [("ms_file", C.c_double), ("ms_h2d", C.c_double), ("ms_device", C.c_double), ("ms_d2h", C.c_double),
+                ("ms_total", C.c_double), ("bytes", C.c_longlong), ("tokens", C.c_longlong)]
+
+
+_hpgl_so.hpgl_b200_io_last_timing.restype = None
+_hpgl_so.hpgl_b200_io_last_timing.argtypes = [C.POINTER(_HPGL_B200_IO_TIMING)]
+
 _hpgl_so.hpgl_set_thread_num.restype = None
 _hpgl_so.hpgl_set_thread_num.argtypes = [C.c_int]
 _hpgl_so.hpgl_get_thread_num.restype = C.c_int

@@ -197,10 +197,20 @@ int hpgl_simple_kriging_weights(float *center_coords, float *neighbours_x, float
                                 float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,
                                 float *weights);
 
-/* api.h:171-215, 253-265, 279-309.  Outside the kriging path (file I/O,
-   sequential simulation, cokriging).  They exist so that the reference's
-   ctypes layer loads; each records "not provided by this build" in the
-   last-error state and returns without touching its buffers. */
+/* Eclipse INC and GSLIB property files (api.h:171-215; api.cpp:54-193 of the
+   reference), parsed and formatted on the GPU.  Same arguments, results and
+   files as the reference's; on failure the last-error state holds the
+   reference's exception text ("read_prop_name: Property name not found.",
+   "load_floats_into_vector: Error parsing 'x' string.", ...), where the
+   reference's exception would have crossed the C boundary.
+   hpgl_read_inc_file_float: `size` values, mask = (value != undefined).
+   hpgl_read_inc_file_byte: `size` integer values as bytes, mask = (value !=
+   undefined), informed bytes replaced by their index in `values`.
+   The writers write every cell of the array's shape in memory order:
+   INC = name line, one "%E" / "%d" line per cell, "/" line; GSLIB = "HPGL
+   saved GSLIB file", "1", name line, one line per cell.  Byte values are
+   written through the table built from `values` (the reference's
+   init_remap_table); an informed byte outside that table is an error here. */
 void hpgl_read_inc_file_float(char *filename, float undefined_value, int size, float *data, unsigned char *mask);
 void hpgl_read_inc_file_byte(char *filename, int undefined_value, int size, unsigned char *data,
                              unsigned char *mask, unsigned char *values, int values_count);
@@ -211,6 +221,10 @@ void hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *data, const char *
                                     double undefined_value);
 void hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *data, const char *filename, const char *name,
                                     double undefined_value, unsigned char *values, int values_count);
+
+/* api.h:253-265, 279-309.  Sequential simulation, outside this build: each
+   records "not provided by this build" in the last-error state and returns
+   without touching its buffers. */
 void hpgl_sgs_simulation(hpgl_cont_masked_array_t *prop, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
                          double *mean, hpgl_ubyte_array_t *simulation_mask);
 void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params,
@@ -439,6 +453,23 @@ void hpgl_b200_server_destroy(hpgl_b200_server_t *server);
    returns the template's length (> cap: only the first cap written), or -1
    on error. */
 long long hpgl_b200_search_template(const hpgl_ik_params_t *params, int *out_xyz, long long cap);
+
+/* Number of values an INC file holds (value tokens before the first '/'
+   outside a comment, or before the end of the file), or -1 on error.  Lets a
+   caller size the buffers of hpgl_read_inc_file_float/_byte. */
+long long hpgl_b200_inc_count_values(const char *filename);
+
+/* Timings of the calling process's last INC/GSLIB call, milliseconds. */
+typedef struct {
+    double ms_file;   /* reading or writing the file on the host */
+    double ms_h2d;    /* host -> device copies */
+    double ms_device; /* kernels (CUDA events) */
+    double ms_d2h;    /* device -> host copies */
+    double ms_total;
+    long long bytes;  /* file size (read) or text size (written) */
+    long long tokens; /* tokens read, or cells written */
+} hpgl_b200_io_timing_t;
+void hpgl_b200_io_last_timing(hpgl_b200_io_timing_t *out);
 
 /* Library build and device description, e.g. for logs. */
 const char *hpgl_b200_version(void);

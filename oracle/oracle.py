@@ -443,3 +443,113 @@ def ref_cokriging(job):
         q.correlation_coef = job["correlation"]
         ref.hpgl_simple_cokriging_mark2(C.byref(a), C.byref(s), C.byref(q), C.byref(b))
     return out, out_mask
+
+
+# ---- INC / GSLIB property files -----------------------------------------------
+
+class OracleIoError(RuntimeError):
+    pass
+
+
+def _b(s):
+    return s if isinstance(s, bytes) else os.fsencode(s)
+
+
+def read_inc(path, size, undefined, is_byte=False, values=()):
+    """Restated reader (textio_oracle.cpp).  Returns (data, mask) of length
+    `size`, or raises OracleIoError(message, partial data, partial mask)."""
+    lib = restated()
+    lib.oracle_read_inc.restype = C.c_int
+    data = np.zeros(size, dtype=np.uint8 if is_byte else np.float32)
+    mask = np.zeros(size, dtype=np.uint8)
+    vals = np.ascontiguousarray(np.array(values, dtype=np.uint8).reshape(-1))
+    err = C.create_string_buffer(1024)
+    rc = lib.oracle_read_inc(_b(path), int(bool(is_byte)), C.c_float(0.0 if is_byte else undefined),
+                             int(undefined) if is_byte else 0, C.c_longlong(size),
+                             None if is_byte else _ptr(data, C.c_float), _ptr(data, C.c_ubyte) if is_byte else None,
+                             _ptr(mask, C.c_ubyte), _ptr(vals, C.c_ubyte), len(vals), err, 1024)
+    if rc != 0:
+        e = OracleIoError(err.value.decode(errors="replace"))
+        e.data, e.mask = data, mask
+        raise e
+    return data, mask
+
+
+def inc_count(path):
+    lib = restated()
+    lib.oracle_inc_count.restype = C.c_longlong
+    err = C.create_string_buffer(1024)
+    n = lib.oracle_inc_count(_b(path), err, 1024)
+    if n < 0:
+        raise OracleIoError(err.value.decode(errors="replace"))
+    return int(n)
+
+
+def remap_table(values, indicator_count):
+    """init_remap_table (api.cpp:117-136)."""
+    values = list(values)
+    if len(values) == indicator_count:
+        return values
+    if len(values) > indicator_count:
+        return values[:indicator_count]
+    return list(range(indicator_count))
+
+
+def write_prop(path, name, data, mask, undefined, fmt="inc", is_byte=False, remap=()):
+    """Restated writer; fmt "inc" or "gslib".  For bytes, `remap` is the
+    table (remap_table's result) and `undefined` the byte written for
+    uninformed cells."""
+    lib = restated()
+    lib.oracle_write_prop.restype = C.c_int
+    data = np.ascontiguousarray(data, dtype=np.uint8 if is_byte else np.float32).reshape(-1)
+    mask = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    rm = np.ascontiguousarray(np.array(remap, dtype=np.uint8).reshape(-1))
+    err = C.create_string_buffer(1024)
+    rc = lib.oracle_write_prop(0 if fmt == "inc" else 1, int(bool(is_byte)), _b(path), _b(name),
+                               None if is_byte else _ptr(data, C.c_float), _ptr(data, C.c_ubyte) if is_byte else None,
+                               _ptr(mask, C.c_ubyte), C.c_longlong(data.size),
+                               C.c_float(0.0 if is_byte else undefined), C.c_ubyte(int(undefined) & 0xff if is_byte else 0),
+                               _ptr(rm, C.c_ubyte), len(rm), err, 1024)
+    if rc != 0:
+        raise OracleIoError(err.value.decode(errors="replace"))
+
+
+def ref_read_inc(path, size, undefined, is_byte=False, values=()):
+    """The reference's own hpgl_read_inc_file_float/_byte.  Only for files it
+    reads without an error: its exceptions cross the C boundary and end the
+    process."""
+    ref = reference()
+    data = np.zeros(size, dtype=np.uint8 if is_byte else np.float32)
+    mask = np.zeros(size, dtype=np.uint8)
+    if is_byte:
+        vals = np.ascontiguousarray(np.array(values, dtype=np.uint8).reshape(-1))
+        ref.hpgl_read_inc_file_byte(_b(path), int(undefined), int(size), _ptr(data, C.c_ubyte),
+                                    _ptr(mask, C.c_ubyte), _ptr(vals, C.c_ubyte), len(vals))
+    else:
+        ref.hpgl_read_inc_file_float(_b(path), C.c_float(undefined), int(size), _ptr(data, C.c_float),
+                                     _ptr(mask, C.c_ubyte))
+    return data, mask
+
+
+def ref_write_prop(path, name, data, mask, undefined, fmt="inc", is_byte=False, values=(), indicator_count=None):
+    """The reference's own writers (api.cpp:101-193), one-dimensional shape."""
+    ref = reference()
+    data = np.ascontiguousarray(data, dtype=np.uint8 if is_byte else np.float32).reshape(-1)
+    mask = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    sh = _shape((data.size, 1, 1))
+    if is_byte:
+        vals = np.ascontiguousarray(np.array(values, dtype=np.uint8).reshape(-1))
+        arr = HpglIndArray(_ptr(data, C.c_ubyte), _ptr(mask, C.c_ubyte), sh,
+                           indicator_count if indicator_count is not None else len(vals))
+        if fmt == "inc":
+            ref.hpgl_write_inc_file_byte(_b(path), C.byref(arr), int(undefined), _b(name), _ptr(vals, C.c_ubyte),
+                                         len(vals))
+        else:
+            ref.hpgl_write_gslib_byte_property(C.byref(arr), _b(path), _b(name), C.c_double(undefined),
+                                               _ptr(vals, C.c_ubyte), len(vals))
+    else:
+        arr = HpglContArray(_ptr(data, C.c_float), _ptr(mask, C.c_ubyte), sh)
+        if fmt == "inc":
+            ref.hpgl_write_inc_file_float(_b(path), C.byref(arr), C.c_float(undefined), _b(name))
+        else:
+            ref.hpgl_write_gslib_cont_property(C.byref(arr), _b(path), _b(name), C.c_double(undefined))
