@@ -21,6 +21,9 @@ Metric: kriged nodes/s.
   oracle/build_ref.sh) on a node sample of the same job, all host threads.
 * ``--impl reference``: that reference CPU path as the timed arm.
 
+``--workload inc_io``: the INC property file reader and writer instead
+(hpgl_b200/bench_io.py), with the reference's own reader and writer beside.
+
 Multi-GPU: the path has no exchange step; N ranks (torchrun, one per GPU)
 each krige their own copy of the job ("replicas only", weak scaling).
 """
@@ -170,7 +173,12 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
+    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io"],
+                    help="inc_io: INC property file read/write (hpgl_b200/bench_io.py), one GPU")
     args = ap.parse_args()
+    if args.workload == "inc_io":
+        from hpgl_b200 import bench_io
+        return bench_io.run(args, ROOT)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)

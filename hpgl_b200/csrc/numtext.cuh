@@ -95,11 +95,15 @@ NT_FN int clz32(uint32_t x) {
 #endif
 }
 
-// Bytes of one token: positions at or past len read as 0.
-struct Tok {
+// Bytes of one token: positions at or past len read as 0.  With
+// Bounded = false the bytes are read as they lie, for a token that a blank
+// follows: no rule of the grammar accepts a blank (nor a 0 byte), so the
+// result is the same and the per-byte bound check is gone.
+template <bool Bounded = true>
+struct TokT {
     const unsigned char *s;
     int len;
-    NT_FN unsigned at(int i) const { return i < len ? s[i] : 0u; }
+    NT_FN unsigned at(int i) const { return (!Bounded || i < len) ? s[i] : 0u; }
 };
 
 // ---- exact slow path: little-endian 32-bit limbs ---------------------------
@@ -167,7 +171,8 @@ NT_FN int big_cmp(const BigU &a, const BigU &b) {
 // Sign of (D * 10^q - mid), D = the significant digits in [sig, end) (a '.'
 // among them is skipped), mid a positive normal double.  Kept out of line:
 // it holds two big integers and runs only for rare tokens.
-NT_SLOW int cmp_decimal_mid(const Tok &t, int sig, int end, int q, double mid) {
+template <bool B>
+NT_SLOW int cmp_decimal_mid(const TokT<B> &t, int sig, int end, int q, double mid) {
     BigU L, R;
     L.n = 0;
     uint32_t acc = 0, scale = 1;
@@ -235,7 +240,8 @@ NT_FN uint32_t round_binary(uint64_t m, bool sticky, int e2) {
     return (uint32_t)bits;
 }
 
-NT_FN bool scan_hex(const Tok &t, int i, uint32_t sign, float &out) {
+template <bool B>
+NT_FN bool scan_hex(const TokT<B> &t, int i, uint32_t sign, float &out) {
     unsigned c = t.at(i);
     if (!(hex_val(c) >= 0 || c == '.')) return false;
     uint64_t m = 0;
@@ -294,7 +300,8 @@ NT_FN double exact_pow10(int k) {
     return r;
 }
 
-NT_FN bool scan_dec(const Tok &t, int i, uint32_t sign, float &out) {
+template <bool B>
+NT_FN bool scan_dec(const TokT<B> &t, int i, uint32_t sign, float &out) {
     int ndig = 0, nfrac = 0, nsig = 0, nw = 0, sig = -1;
     uint64_t w = 0;
     bool trunc = false;
@@ -418,8 +425,9 @@ NT_FN bool scan_dec(const Tok &t, int i, uint32_t sign, float &out) {
 }
 
 // sscanf(token, "%f", &out) == 1
+template <bool Bounded = true>
 NT_FN bool scan_f32(const unsigned char *s, int len, float &out) {
-    const Tok t{s, len};
+    const TokT<Bounded> t{s, len};
     int i = 0;
     uint32_t sign = 0;
     unsigned c = t.at(0);
@@ -447,8 +455,9 @@ NT_FN bool scan_f32(const unsigned char *s, int len, float &out) {
 }
 
 // sscanf(token, "%d", &out) == 1
+template <bool Bounded = true>
 NT_FN bool scan_int(const unsigned char *s, int len, int &out) {
-    const Tok t{s, len};
+    const TokT<Bounded> t{s, len};
     int i = 0;
     bool neg = false;
     unsigned c = t.at(0);
@@ -476,9 +485,21 @@ NT_FN bool scan_int(const unsigned char *s, int len, int &out) {
 
 // ---- formatting -------------------------------------------------------------
 
+// 5^k for 0 <= k <= 27
+NT_FN uint64_t pow5_u64_small(int k) {
+    uint64_t r = 1, b = 5;
+    while (k) {
+        if (k & 1) r *= b;
+        b *= b;
+        k >>= 1;
+    }
+    return r;
+}
+
+// 5^k for 0 <= k <= 55 (< 2^128)
 NT_FN u128 pow5_u128(int k) {
-    u128 r = 1;
-    while (k-- > 0) r *= 5u;
+    u128 r = pow5_u64_small(k < 27 ? k : 27);
+    if (k > 27) r *= (u128)pow5_u64_small(k - 27);
     return r;
 }
 
@@ -504,7 +525,42 @@ NT_FN int format_E(float x, char *o) {
         const int e = ef ? ef - 150 : -149;
         const int bexp = e + (32 - clz32(M)) - 1;  // x in [2^bexp, 2^(bexp+1))
         E = ((bexp + 1) * 78913) >> 18;             // floor((bexp+1) log10 2): E10 or E10 + 1
-        for (int it = 0; it < 4; ++it) {
+        // Fast path: y = |x| * 10^(6-E) with an exact power of ten, one
+        // rounding (error < 2^-30 for y < 2^24); its integer part and the
+        // side of .5 are those of the exact product unless y lies within
+        // 2^-26 of a half, where the exact path below decides.  Exponents
+        // near a power of ten resolve to the same digits either way (a
+        // rounded 10^6 or 10^7 carries as the exact value would).
+        bool done = false;
+        {
+            const double xa = (double)u2f(a);
+            int Ef = E;
+            for (int it = 0; it < 3; ++it) {
+                const int k = 6 - Ef;
+                if (k < -22 || k > 22) break;
+                const double y = k >= 0 ? xa * exact_pow10(k) : xa / exact_pow10(-k);
+                if (y < 1e6) {
+                    --Ef;
+                    continue;
+                }
+                if (y >= 1e7) {
+                    ++Ef;
+                    continue;
+                }
+                const uint32_t fl = (uint32_t)y;
+                const double fr = y - (double)fl;
+                const double dh = fr - 0.5;
+                if (dh < 1.0 / 67108864.0 && dh > -1.0 / 67108864.0) break;
+                digits = fl + (fr > 0.5 ? 1u : 0u);
+                E = Ef;
+                done = true;
+                break;
+            }
+        }
+        // exact path: floor(|x| / 10^(E-6)) and the rounding bit in 128-bit
+        // integers (|x| = M * 2^e; every intermediate < 2^128 for E = E10
+        // or E10 + 1)
+        for (int it = 0; it < 4 && !done; ++it) {
             const int k = E - 6;
             u128 qq;
             bool up;

@@ -34,9 +34,11 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -104,30 +106,58 @@ __device__ __forceinline__ bool blank(const Region &R, long long p, unsigned c) 
     return p < R.begin || p >= R.end || is_ws(c);
 }
 
-__device__ __forceinline__ void load16(const unsigned char *p, unsigned char (&c)[PER]) {
-    const uint4 v = *reinterpret_cast<const uint4 *>(p);
-    const unsigned w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-    for (int j = 0; j < PER; ++j) c[j] = (unsigned char)(w[j >> 2] >> (8 * (j & 3)));
+// The top bit of each byte of x gathered into bits 0..3.
+__device__ __forceinline__ unsigned movemask4(unsigned x) { return ((x & 0x80808080u) * 0x00204081u) >> 28; }
+
+// Bits 0..3: which bytes of w are one of " \t\n\v\f\r".
+__device__ __forceinline__ unsigned blank4(unsigned w) {
+    return movemask4(__vcmpeq4(w, 0x20202020u) | __vcmpltu4(__vsub4(w, 0x09090909u), 0x05050505u));
+}
+
+// One thread's 16 bytes as bit masks (bit j = byte pos0 + j): blanks
+// (bytes outside the data section included), newlines inside it, and the
+// blank state of the bytes just before and after.
+struct Bytes16 {
+    unsigned blank, nl;
+    bool prev_blank, next_blank;
+};
+
+__device__ __forceinline__ Bytes16 scan16(const Region &R, long long pos0) {
+    const uint4 v = *reinterpret_cast<const uint4 *>(R.txt + pos0);
+    Bytes16 b;
+    b.blank = blank4(v.x) | blank4(v.y) << 4 | blank4(v.z) << 8 | blank4(v.w) << 12;
+    b.nl = movemask4(__vcmpeq4(v.x, 0x0a0a0a0au)) | movemask4(__vcmpeq4(v.y, 0x0a0a0a0au)) << 4 |
+           movemask4(__vcmpeq4(v.z, 0x0a0a0a0au)) << 8 | movemask4(__vcmpeq4(v.w, 0x0a0a0a0au)) << 12;
+    const long long lo = R.begin - pos0, hi = R.end - pos0;
+    const int l = lo <= 0 ? 0 : (lo >= PER ? PER : (int)lo);
+    const int h = hi <= 0 ? 0 : (hi >= PER ? PER : (int)hi);
+    const unsigned inside = ((1u << h) - 1u) & ~((1u << l) - 1u);
+    b.blank = (b.blank | ~inside) & 0xffffu;
+    b.nl &= inside;
+    // neighbours' edge bytes: from the lanes next door, else from memory
+    const int lane = threadIdx.x & 31;
+    const unsigned up = __shfl_up_sync(FULL_MASK, b.blank, 1);
+    const unsigned down = __shfl_down_sync(FULL_MASK, b.blank, 1);
+    b.prev_blank = lane ? (up >> 15) & 1u : (pos0 == 0 ? true : blank(R, pos0 - 1, R.txt[pos0 - 1]));
+    b.next_blank = lane < 31 ? down & 1u : blank(R, pos0 + PER, R.txt[pos0 + PER]);
+    return b;
+}
+
+// bit j: a run of non-blank bytes starts at byte j
+__device__ __forceinline__ unsigned starts16(const Bytes16 &b) {
+    return ~b.blank & ((b.blank << 1) | (b.prev_blank ? 1u : 0u)) & 0xffffu;
+}
+// bit j: a run ends with byte j
+__device__ __forceinline__ unsigned ends16(const Bytes16 &b) {
+    return ~b.blank & ((b.blank >> 1) | (b.next_blank ? 0x8000u : 0u)) & 0xffffu;
 }
 
 // Per tile: token starts (bits 0-19) and newlines (bits 20-39).
 __global__ void __launch_bounds__(NT) k_tile_count(Region R, long long tile0, unsigned long long *tile_cnt) {
     const long long pos0 = (tile0 + blockIdx.x) * (long long)BLK + threadIdx.x * PER;
-    unsigned char c[PER];
-    load16(R.txt + pos0, c);
-    bool pb = pos0 == 0 ? true : blank(R, pos0 - 1, R.txt[pos0 - 1]);
-    unsigned starts = 0, nl = 0;
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const long long p = pos0 + j;
-        const bool b = blank(R, p, c[j]);
-        starts += (!b && pb) ? 1u : 0u;
-        nl += (c[j] == '\n' && p >= R.begin && p < R.end) ? 1u : 0u;
-        pb = b;
-    }
+    const Bytes16 b = scan16(R, pos0);
     unsigned long long tot;
-    block_scan<NT>(starts | ((unsigned long long)nl << 20), tot);
+    block_scan<NT>((unsigned)__popc(starts16(b)) | ((unsigned long long)__popc(b.nl) << 20), tot);
     if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
 }
 
@@ -158,52 +188,33 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(const unsigned long long *c
 }
 
 // Start, end (exclusive) and line number of every run of non-blank bytes.
+// The runs that ended before a thread's first byte are the runs that started
+// before it, less one when a run crosses into the thread's first byte.
 __global__ void __launch_bounds__(NT) k_tile_emit(Region R, long long tile0, const long long *run_base,
                                                   const long long *nl_base, long long *run_start, long long *run_end,
                                                   long long *run_line) {
-    const long long tile_start = (tile0 + blockIdx.x) * (long long)BLK;
-    const long long pos0 = tile_start + threadIdx.x * PER;
-    unsigned char c[PER];
-    load16(R.txt + pos0, c);
-    const bool prev_b = pos0 == 0 ? true : blank(R, pos0 - 1, R.txt[pos0 - 1]);
-    const bool next_b = blank(R, pos0 + PER, R.txt[pos0 + PER]);
-    bool b[PER];
-#pragma unroll
-    for (int j = 0; j < PER; ++j) b[j] = blank(R, pos0 + j, c[j]);
-    unsigned s = 0, e = 0, nl = 0;
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const bool pb = j ? b[j - 1] : prev_b;
-        const bool nb = j + 1 < PER ? b[j + 1] : next_b;
-        s += (!b[j] && pb) ? 1u : 0u;
-        e += (!b[j] && nb) ? 1u : 0u;
-        nl += (c[j] == '\n' && !(pos0 + j < R.begin || pos0 + j >= R.end)) ? 1u : 0u;
-    }
+    const long long pos0 = (tile0 + blockIdx.x) * (long long)BLK + threadIdx.x * PER;
+    const Bytes16 b = scan16(R, pos0);
+    unsigned S = starts16(b), E = ends16(b);
     unsigned long long tot;
     const unsigned long long off =
-        block_scan<NT>(s | ((unsigned long long)e << 20) | ((unsigned long long)nl << 40), tot);
-    // a run that covers the tile's first byte and the byte before it ended
-    // nowhere before this tile
-    const bool open = tile_start > 0 && !blank(R, tile_start - 1, R.txt[tile_start - 1]) &&
-                      !blank(R, tile_start, R.txt[tile_start]);
-    long long si = run_base[blockIdx.x] + (long long)(off & F20);
-    long long ei = run_base[blockIdx.x] - (open ? 1 : 0) + (long long)((off >> 20) & F20);
-    long long line = nl_base[blockIdx.x] + (long long)((off >> 40) & F20);
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const long long p = pos0 + j;
-        const bool pb = j ? b[j - 1] : prev_b;
-        const bool nb = j + 1 < PER ? b[j + 1] : next_b;
-        if (!b[j] && pb) {
-            run_start[si] = p;
-            run_line[si] = line;
-            ++si;
-        }
-        if (!b[j] && nb) {
-            run_end[ei] = p + 1;
-            ++ei;
-        }
-        if (c[j] == '\n' && p >= R.begin && p < R.end) ++line;
+        block_scan<NT>((unsigned)__popc(S) | ((unsigned long long)__popc(b.nl) << 20), tot);
+    const long long si0 = run_base[blockIdx.x] + (long long)(off & F20);
+    const long long line0 = nl_base[blockIdx.x] + (long long)((off >> 20) & F20);
+    const bool open = !b.prev_blank && !(b.blank & 1u);
+    long long si = si0, ei = si0 - (open ? 1 : 0);
+    while (S) {
+        const int j = __ffs(S) - 1;
+        S &= S - 1;
+        run_start[si] = pos0 + j;
+        run_line[si] = line0 + __popc(b.nl & ((1u << j) - 1u));
+        ++si;
+    }
+    while (E) {
+        const int j = __ffs(E) - 1;
+        E &= E - 1;
+        run_end[ei] = pos0 + j + 1;
+        ++ei;
     }
 }
 
@@ -297,16 +308,11 @@ __device__ __forceinline__ int tok_class(const Tokens &T, long long t) {
     return T.txt[T.start[t]] == '/' ? 2 : 1;
 }
 
+// Value tokens per block of NT tokens (one token per thread).
 __global__ void __launch_bounds__(NT) k_count_values(Tokens T, long long *block_sums) {
-    const long long i0 = blockIdx.x * (long long)BLK + threadIdx.x * PER;
-    unsigned cnt = 0;
-    for (int j = 0; j < PER; ++j) {
-        const long long t = i0 + j;
-        if (t < T.n) cnt += tok_class(T, t) == 1 ? 1u : 0u;
-    }
-    unsigned long long tot;
-    block_scan<NT>(cnt, tot);
-    if (threadIdx.x == 0) block_sums[blockIdx.x] = (long long)tot;
+    const long long t = blockIdx.x * (long long)NT + threadIdx.x;
+    const int n = __syncthreads_count(t < T.n && tok_class(T, t) == 1);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = n;
 }
 
 struct ValueOut {
@@ -320,57 +326,51 @@ struct ValueOut {
     long long *last_read;  // last token the reference's scanner would read
 };
 
-// Converts every value token whose index is below `size`.
+// Converts every value token whose index is below `size`, one token per
+// thread: a warp reads 32 neighbouring tokens of the text.
 __global__ void __launch_bounds__(NT) k_values(Tokens T, const long long *block_base, ValueOut O) {
-    const long long i0 = blockIdx.x * (long long)BLK + threadIdx.x * PER;
-    int cls[PER];
-    unsigned cnt = 0;
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const long long t = i0 + j;
-        cls[j] = t < T.n ? tok_class(T, t) : 0;
-        cnt += cls[j] == 1 ? 1u : 0u;
-    }
+    const long long t = blockIdx.x * (long long)NT + threadIdx.x;
+    const int cls = t < T.n ? tok_class(T, t) : 0;
     unsigned long long tot;
-    long long vi = block_base[blockIdx.x] + (long long)block_scan<NT>(cnt, tot);
-    long long last = -1;
-    for (int j = 0; j < PER; ++j) {
-        const long long t = i0 + j;
-        if (t >= T.n) break;
-        if (!T.first_comment || T.first_comment[T.line[t]] >= t) last = t;
-        if (cls[j] == 0) continue;
-        if (cls[j] == 2) {
-            if (vi < O.size) {
-                atomicMin(O.err_t, (unsigned long long)t);
-                atomicMin(O.err_vi, (unsigned long long)vi);
-            }
-            continue;
-        }
-        if (vi < O.size) {
-            const long long s = T.start[t];
-            const unsigned char *p = T.txt + s;
-            const int len = (int)(T.end[t] - s);
-            bool ok;
-            if (O.is_byte) {
-                int v;
-                ok = scan_int(p, len, v);
-                if (ok) {
-                    O.vals_b[vi] = (unsigned char)v;
-                    O.mask[vi] = v == O.undefined_i ? 0 : 1;
-                }
-            } else {
-                float v;
-                ok = scan_f32(p, len, v);
-                if (ok) O.vals_f[vi] = v;
-            }
-            if (!ok) {
-                atomicMin(O.err_t, (unsigned long long)t);
-                atomicMin(O.err_vi, (unsigned long long)vi);
-            }
-        }
-        ++vi;
+    const long long vi = block_base[blockIdx.x] + (long long)block_scan<NT>(cls == 1 ? 1u : 0u, tot);
+    if (cls == 0 || vi >= O.size) return;
+    if (cls == 2) {
+        atomicMin(O.err_t, (unsigned long long)t);
+        atomicMin(O.err_vi, (unsigned long long)vi);
+        return;
     }
-    if (last >= 0) atomicMax(O.last_read, last);
+    const long long s = T.start[t];
+    const unsigned char *p = T.txt + s;
+    const int len = (int)(T.end[t] - s);
+    // a token shorter than 255 bytes is a whole run, so a blank (or the
+    // padding after the file) follows it: the unbounded conversions apply
+    bool ok;
+    if (O.is_byte) {
+        int v;
+        ok = len < 255 ? scan_int<false>(p, len, v) : scan_int<true>(p, len, v);
+        if (ok) {
+            O.vals_b[vi] = (unsigned char)v;
+            O.mask[vi] = v == O.undefined_i ? 0 : 1;
+        }
+    } else {
+        float v;
+        ok = len < 255 ? scan_f32<false>(p, len, v) : scan_f32<true>(p, len, v);
+        if (ok) O.vals_f[vi] = v;
+    }
+    if (!ok) {
+        atomicMin(O.err_t, (unsigned long long)t);
+        atomicMin(O.err_vi, (unsigned long long)vi);
+    }
+}
+
+// The last token the reference's scanner reads: the last one that does not
+// follow a comment mark on its line (only asked for when values run out).
+__global__ void __launch_bounds__(NT) k_last_read(Tokens T, long long *last_read) {
+    const long long t = blockIdx.x * (long long)NT + threadIdx.x;
+    long long v = (t < T.n && (!T.first_comment || T.first_comment[T.line[t]] >= t)) ? t : -1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(FULL_MASK, v, o));
+    if ((threadIdx.x & 31) == 0 && v >= 0) atomicMax(last_read, v);
 }
 
 // A file with fewer values than asked: the reference's scanner keeps the
@@ -440,53 +440,43 @@ __device__ __forceinline__ int cell_line(const Cells &C, long long i, float &f, 
     return (int)(u >> 31) + ((u & 0x7fffffffu) >= 0x7f800000u ? 3 : 12) + 1;
 }
 
+// Text bytes per block of NT cells (one cell per thread).
 __global__ void __launch_bounds__(NT) k_count_text(Cells C, long long *block_sums, int *flags) {
-    const long long i0 = blockIdx.x * (long long)BLK + threadIdx.x * PER;
+    const long long i = blockIdx.x * (long long)NT + threadIdx.x;
     unsigned len = 0;
-    bool anybad = false;
-    for (int j = 0; j < PER; ++j) {
-        const long long i = i0 + j;
-        if (i >= C.n) break;
+    bool bad = false;
+    if (i < C.n) {
         float f;
         int d;
-        bool bad;
-        len += (unsigned)cell_line(C, i, f, d, bad);
-        anybad |= bad;
+        len = (unsigned)cell_line(C, i, f, d, bad);
     }
-    if (anybad) atomicOr(flags, FLAG_BAD_REMAP);
+    if (bad) atomicOr(flags, FLAG_BAD_REMAP);
     unsigned long long tot;
     block_scan<NT>(len, tot);
     if (threadIdx.x == 0) block_sums[blockIdx.x] = (long long)tot;
 }
 
+// One cell per thread; the block's lines are assembled in shared memory and
+// stored with consecutive threads on consecutive bytes.
 __global__ void __launch_bounds__(NT) k_format(Cells C, const long long *block_base, char *out) {
-    const long long i0 = blockIdx.x * (long long)BLK + threadIdx.x * PER;
-    int lens[PER];
-    unsigned len = 0;
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const long long i = i0 + j;
-        float f;
-        int d;
-        bool bad;
-        lens[j] = i < C.n ? cell_line(C, i, f, d, bad) : 0;
-        len += (unsigned)lens[j];
-    }
-    unsigned long long tot;
-    long long off = block_base[blockIdx.x] + (long long)block_scan<NT>(len, tot);
-    for (int j = 0; j < PER; ++j) {
-        const long long i = i0 + j;
-        if (i >= C.n) break;
+    __shared__ char text[NT * 16];
+    const long long i = blockIdx.x * (long long)NT + threadIdx.x;
+    char buf[16];
+    int k = 0;
+    if (i < C.n) {
         float f;
         int d;
         bool bad;
         cell_line(C, i, f, d, bad);
-        char buf[16];
-        const int k = C.is_byte ? format_d(d, buf) : format_E(f, buf);
-        buf[k] = '\n';
-        for (int q = 0; q <= k; ++q) out[off + q] = buf[q];
-        off += lens[j];
+        k = C.is_byte ? format_d(d, buf) : format_E(f, buf);
+        buf[k++] = '\n';
     }
+    unsigned long long tot;
+    const unsigned off = (unsigned)block_scan<NT>((unsigned)k, tot);
+    for (int q = 0; q < k; ++q) text[off + q] = buf[q];
+    __syncthreads();
+    char *dst = out + block_base[blockIdx.x];
+    for (unsigned q = threadIdx.x; q < (unsigned)tot; q += NT) dst[q] = text[q];
 }
 
 // ---- host side -------------------------------------------------------------
@@ -580,6 +570,31 @@ void read_file(int fd, char *dst, size_t n) {
         if (f) throw HpglError{HPGL_E_INVALID, "error reading the file"};
 }
 
+// Writes n bytes at offset `at` with a few threads.
+void write_file(int fd, const char *src, long long n, long long at) {
+    if (n <= 0) return;
+    const long long slice_min = 8ll << 20;
+    const int nth = (int)std::max<long long>(1, std::min<long long>(8, n / slice_min));
+    std::vector<std::thread> th;
+    std::vector<int> failed(nth, 0);
+    for (int k = 0; k < nth; ++k) {
+        th.emplace_back([&, k] {
+            long long a = n * k / nth, b = n * (k + 1) / nth;
+            while (a < b) {
+                const ssize_t r = pwrite(fd, src + a, (size_t)(b - a), (off_t)(at + a));
+                if (r <= 0) {
+                    failed[k] = 1;
+                    return;
+                }
+                a += r;
+            }
+        });
+    }
+    for (auto &t : th) t.join();
+    for (int f : failed)
+        if (f) throw HpglError{HPGL_E_INVALID, "error writing the file"};
+}
+
 // read_prop_name (read_inc_file.cpp:8-50): lines are read in pieces of up
 // to 1023 bytes, each followed by a skip of all blanks; the first line whose
 // first byte is a letter is the name, and data starts after it and the
@@ -656,22 +671,30 @@ Tokenized tokenize(IoContext &C, const char *filename, bool device, TextIoTiming
     cudaStream_t s = C.stream;
     auto t0 = std::chrono::steady_clock::now();
     unsigned char *h = (unsigned char *)C.host((size_t)n + 1);
-    read_file(fd, (char *)h, (size_t)n);
-    tm.ms_file = ms_since(t0);
     K.h = h;
     K.n = n;
+    if (!device) {
+        read_file(fd, (char *)h, (size_t)n);
+        tm.ms_file = ms_since(t0);
+        K.begin = skip_header(h, n);
+        return K;
+    }
+    // the whole file with a few threads, then one copy to the device, padded
+    // so that every tile reads whole 16-byte words past the end (a copy per
+    // chunk as chunks arrive measured slower: page-cache reads and the DMA
+    // share the host's memory bandwidth)
+    read_file(fd, (char *)h, (size_t)n);
+    tm.ms_file = ms_since(t0);
     K.begin = skip_header(h, n);
-    if (!device) return K;
-    // device copy, padded so that every tile reads whole 16-byte words
-    const long long tile0 = K.begin / BLK;
-    const long long ntiles = std::max<long long>(1, (n - tile0 * BLK + BLK - 1) / BLK);
-    const long long padded = (tile0 + ntiles) * BLK + BLK + 64;
+    const long long padded = n + 2 * BLK + 64;
     unsigned char *d_txt = C.text.get<unsigned char>((size_t)padded);
     t0 = std::chrono::steady_clock::now();
     TIO_CHECK(cudaMemcpyAsync(d_txt, h, (size_t)n, cudaMemcpyHostToDevice, s));
     TIO_CHECK(cudaMemsetAsync(d_txt + n, ' ', (size_t)(padded - n), s));
     TIO_CHECK(cudaStreamSynchronize(s));
     tm.ms_h2d = ms_since(t0);
+    const long long tile0 = K.begin / BLK;
+    const long long ntiles = std::max<long long>(1, (n - tile0 * BLK + BLK - 1) / BLK);
 
     TIO_CHECK(cudaEventRecord(C.ev0, s));
     const Region R{d_txt, K.begin, n};
@@ -814,7 +837,7 @@ void inc_read(const char *filename, bool is_byte, float undefined_f, int undefin
     O.err_vi = reinterpret_cast<unsigned long long *>(d_small + 5);
     O.last_read = d_small + 6;
     if (T.n > 0) {
-        const long long nb = (T.n + BLK - 1) / BLK;
+        const long long nb = (T.n + NT - 1) / NT;
         long long *d_blocks = C.blocks.get<long long>((size_t)nb);
         k_count_values<<<(unsigned)nb, NT, 0, s>>>(T, d_blocks);
         k_scan_blocks<<<1, 1024, 0, s>>>(d_blocks, nb, d_small + 3);
@@ -825,7 +848,12 @@ void inc_read(const char *filename, bool is_byte, float undefined_f, int undefin
     TIO_CHECK(cudaStreamSynchronize(s));
     const long long nvals = T.n > 0 ? hs[3] : 0;
     const unsigned long long err_t = (unsigned long long)hs[4], err_vi = (unsigned long long)hs[5];
-    const long long last_read = hs[6];
+    long long last_read = -1;
+    if (err_t == ~0ull && nvals < size && T.n > 0) {
+        k_last_read<<<grid_of(T.n, NT), NT, 0, s>>>(T, d_small + 6);
+        TIO_CHECK(cudaMemcpyAsync(&last_read, d_small + 6, sizeof(long long), cudaMemcpyDeviceToHost, s));
+        TIO_CHECK(cudaStreamSynchronize(s));
+    }
     const size_t elem = is_byte ? 1 : 4;
     void *out_vals = is_byte ? (void *)O.vals_b : (void *)O.vals_f;
     void *user_vals = is_byte ? (void *)data_b : (void *)data_f;
@@ -929,7 +957,7 @@ void prop_write(int format, bool is_byte, const char *filename, const char *name
         TIO_CHECK(cudaStreamSynchronize(s));
         tm.ms_h2d = ms_since(t0);
         TIO_CHECK(cudaEventRecord(C.ev0, s));
-        const long long nb = (size + BLK - 1) / BLK;
+        const long long nb = (size + NT - 1) / NT;
         long long *d_blocks = C.blocks.get<long long>((size_t)nb);
         long long *d_small = C.small.get<long long>(8);
         TIO_CHECK(cudaMemsetAsync(d_small, 0, 8 * sizeof(long long), s));
@@ -955,14 +983,24 @@ void prop_write(int format, bool is_byte, const char *filename, const char *name
         tm.ms_device = ms;
     }
     auto t0 = std::chrono::steady_clock::now();
-    FILE *f = fopen(filename, "w+");
-    if (!f)
+    // fopen(filename, "w+") of the reference, then the header, the lines
+    // (written by a few threads at their offsets) and the "/" line
+    const int fd = open(filename, O_RDWR | O_CREAT | O_TRUNC, 0666);
+    if (fd < 0)
         throw HpglError{HPGL_E_INVALID, std::string("open_file_checked: Can't open file '") + filename + "'."};
-    if (format == 1) fprintf(f, "HPGL saved GSLIB file\n%d\n", 1);
-    fprintf(f, "%s\n", name);
-    if (body > 0) fwrite(h, 1, (size_t)body, f);
-    if (format == 0) fprintf(f, "/\n");
-    fclose(f);
+    struct FdCloser {
+        int fd;
+        ~FdCloser() {
+            if (fd >= 0) close(fd);
+        }
+    } closer{fd};
+    const std::string head = std::string(format == 1 ? "HPGL saved GSLIB file\n1\n" : "") + name + "\n";
+    const std::string tail = format == 0 ? "/\n" : "";
+    write_file(fd, head.data(), (long long)head.size(), 0);
+    write_file(fd, h, body, (long long)head.size());
+    write_file(fd, tail.data(), (long long)tail.size(), (long long)head.size() + body);
+    close(fd);  // inside the timing: closing a freshly written file can take a while
+    closer.fd = -1;
     tm.ms_file = ms_since(t0);
     tm.bytes = body;
     tm.tokens = size;

@@ -193,9 +193,13 @@ long nt_fuzz_f32(unsigned long long seed, long count, int mode, char *report, in
         float a = -777.f, b = -777.f;
         const int ra = sscanf(tok.c_str(), "%f", &a) == 1 ? 1 : 0;
         const int rb = scan_f32((const unsigned char *)tok.data(), (int)tok.size(), b) ? 1 : 0;
-        if (ra != rb || (ra && f2u(a) != f2u(b))) {
+        // the unbounded variant, on the zero-terminated copy
+        float c = -777.f;
+        const int rc = scan_f32<false>((const unsigned char *)tok.c_str(), 0, c) ? 1 : 0;
+        if (ra != rb || (ra && f2u(a) != f2u(b)) || rc != rb || (rc && f2u(c) != f2u(b))) {
             char buf[400];
-            snprintf(buf, sizeof buf, "'%s' libc=%d:%08x mine=%d:%08x", tok.c_str(), ra, f2u(a), rb, f2u(b));
+            snprintf(buf, sizeof buf, "'%s' libc=%d:%08x mine=%d:%08x unbounded=%d:%08x", tok.c_str(), ra, f2u(a), rb,
+                     f2u(b), rc, f2u(c));
             if (bad < 10) note(report, cap, used, buf);
             ++bad;
         }
@@ -213,7 +217,9 @@ long nt_fuzz_int(unsigned long long seed, long count, char *report, int cap) {
         int a = -777, b = -777;
         const int ra = sscanf(tok.c_str(), "%d", &a) == 1 ? 1 : 0;
         const int rb = scan_int((const unsigned char *)tok.data(), (int)tok.size(), b) ? 1 : 0;
-        if (ra != rb || (ra && a != b)) {
+        int c = -777;
+        const int rc = scan_int<false>((const unsigned char *)tok.c_str(), 0, c) ? 1 : 0;
+        if (ra != rb || (ra && a != b) || rc != rb || (rc && c != b)) {
             char buf[400];
             snprintf(buf, sizeof buf, "'%s' libc=%d:%d mine=%d:%d", tok.c_str(), ra, a, rb, b);
             if (bad < 10) note(report, cap, used, buf);

@@ -26,6 +26,7 @@ EXPECTED_ERRORS = {
     "name_only": "load_floats_into_vector: Unexpected end of data.",
     "codes_bad": "load_floats_into_vector: Error parsing 'x' string.",
     "codes_minus": "load_floats_into_vector: Error parsing '-' string.",
+    "high_bytes": "load_floats_into_vector: Error parsing '\u00e9' string.",  # the token's bytes C3 A9
 }
 
 

@@ -93,6 +93,8 @@ def float_cases(d, seed=0):
         "0.000000000000000000000000000000000000000000000700649232162408535461864791644958065640130970938257885878534141944895541342930300743319094181060791015625",
         "340282356779733661637539395458142568448", "340282356779733661637539395458142568447",
         "16777217", "16777219", "9007199254740993", "1.17549435e-38", "0.99999999"]) + "\n", 10)
+    add("vt_ff_ws", "PORO\x0b\x0c\n1\x0b2\x0c3\r4\r\n\x0b5\x0c\n", 5)
+    add("high_bytes", b"PORO\n1.5\xa0 2\xff\xfe 3 \xc3\xa9 4\n", 4, ref_ok=False)
     add("undefined_nan", "PORO\n1 nan 2 -99 3\n", 5, undefined=float("nan"))
     return cases
 
