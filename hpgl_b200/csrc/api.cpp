@@ -2,6 +2,7 @@
 // (src/geo_bsd/hpgl/api.h, api.cpp) plus this build's additions, all declared
 // in include/hpgl.h.  Every entry point catches every error and records it
 // for hpgl_get_last_exception_message / hpgl_get_last_error.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -14,6 +15,7 @@
 #include "kernels.cuh"
 #include "plan.h"
 #include "textio.h"
+#include "variogram.h"
 
 using namespace hpgl_b200;
 
@@ -505,6 +507,66 @@ void hpgl_b200_io_last_timing(hpgl_b200_io_timing_t *out) {
     out->ms_total = t.ms_total;
     out->bytes = t.bytes;
     out->tokens = t.tokens;
+}
+
+// Experimental variograms and layer stacking (the reference's _cvariogram
+// library, api.h:91-141 there; variogram.cu).
+void fill_ellipsoid_directions(ellipsoid_t *ell, double azimuth, double dip, double rotation) {
+    guarded("fill_ellipsoid_directions", [&] {
+        if (!ell) throw HpglError{HPGL_E_INVALID, "ellipsoid is null"};
+        cv_fill_ellipsoid(ell, azimuth, dip, rotation);
+    });
+}
+
+void calc_variograms(variogram_search_template_t *templ, hard_data_t *data, float *result_covariations,
+                     int result_length, int percentToUse) {
+    guarded("calc_variograms", [&] {
+        if (!templ || !data || (!result_covariations && result_length > 0))
+            throw HpglError{HPGL_E_INVALID, "null argument"};
+        const int lags = std::min(templ->m_num_lags, result_length);
+        if (lags <= 0) return;
+        std::vector<double> sums(lags);
+        std::vector<unsigned long long> counts(lags);
+        cv_grid(*templ, *data, result_length, percentToUse, sums.data(), counts.data());
+        // variograms.cpp:411-414: sum / count / 2, NaN for a lag without pairs
+        for (int l = 0; l < lags; ++l) result_covariations[l] = (float)(sums[l] / (double)counts[l] / 2);
+    });
+}
+
+void calc_variograms_from_point_set(variogram_search_template_t *templ, cont_point_set_t *point_set,
+                                    float *result_covariations, int result_length) {
+    guarded("calc_variograms_from_point_set", [&] {
+        if (!templ || !point_set || (!result_covariations && result_length > 0))
+            throw HpglError{HPGL_E_INVALID, "null argument"};
+        const int lags = std::min(templ->m_num_lags, result_length);
+        if (lags <= 0) return;
+        std::vector<double> sums(lags);
+        std::vector<unsigned long long> counts(lags);
+        cv_points(*templ, *point_set, result_length, sums.data(), counts.data());
+        // variograms.cpp:495-500: 0 for a lag without pairs
+        for (int l = 0; l < lags; ++l)
+            result_covariations[l] = counts[l] == 0 ? 0.f : (float)(sums[l] / (double)counts[l] / 2);
+    });
+}
+
+void cvar_stack_layers(float_data_t *thick_layers, int *layer_markers, int layers_count, int nz, float scalez,
+                       int blank_value, float_data_t *result) {
+    guarded("cvar_stack_layers",
+            [&] { cv_stack_layers(thick_layers, layer_markers, layers_count, nz, scalez, blank_value, result); });
+}
+
+int hpgl_b200_variogram_stats(variogram_search_template_t *templ, hard_data_t *data, cont_point_set_t *points,
+                              int result_length, int percentToUse, double *sums, long long *counts) {
+    return guarded("hpgl_b200_variogram_stats", [&] {
+        if (!templ || !sums || !counts) throw HpglError{HPGL_E_INVALID, "null argument"};
+        const int lags = std::min(templ->m_num_lags, result_length);
+        if (lags <= 0) return;
+        std::vector<unsigned long long> c(lags);
+        if (points) cv_points(*templ, *points, result_length, sums, c.data());
+        else if (data) cv_grid(*templ, *data, result_length, percentToUse, sums, c.data());
+        else throw HpglError{HPGL_E_INVALID, "no data"};
+        for (int l = 0; l < lags; ++l) counts[l] = (long long)c[l];
+    });
 }
 
 void hpgl_sgs_simulation(hpgl_cont_masked_array_t *, hpgl_sgs_params_t *, hpgl_non_parametric_cdf_t *, double *,

@@ -37,3 +37,17 @@ gcc -O2 -ffp-contract=off -fPIC -c "$HERE/lapack_restated.c" -o "$OUT/obj/lapack
 for p in "${pids[@]}"; do wait "$p"; done
 g++ -shared -fopenmp -o "$OUT/libhpgl_ref.so" "$OUT"/obj/*.o
 echo "built $OUT/libhpgl_ref.so"
+
+# The experimental-variogram library (_cvariogram: variograms.cpp,
+# ellipsoid.cpp, stack_layers.cpp) as the reference builds it
+# (_cvariogram/SConstruct: no optimisation flags there; -O2 -ffp-contract=off
+# here as for the kriging sources), plus oracle/ref_cvar_shim.cpp.
+CV=$REF/geo_bsd/_cvariogram
+mkdir -p "$OUT/cvobj"
+CVFLAGS="-std=gnu++11 -O2 -ffp-contract=off -fPIC -w -DNDEBUG -I$CV"
+for f in variograms.cpp ellipsoid.cpp stack_layers.cpp; do
+    g++ $CVFLAGS -c "$CV/$f" -o "$OUT/cvobj/${f%.cpp}.o"
+done
+g++ $CVFLAGS -c "$HERE/ref_cvar_shim.cpp" -o "$OUT/cvobj/ref_cvar_shim.o"
+g++ -shared -o "$OUT/libcvariogram_ref.so" "$OUT"/cvobj/*.o
+echo "built $OUT/libcvariogram_ref.so"

@@ -553,3 +553,151 @@ def ref_write_prop(path, name, data, mask, undefined, fmt="inc", is_byte=False, 
             ref.hpgl_write_inc_file_float(_b(path), C.byref(arr), C.c_float(undefined), _b(name))
         else:
             ref.hpgl_write_gslib_cont_property(C.byref(arr), _b(path), _b(name), C.c_double(undefined))
+
+
+# ---- experimental variograms (_cvariogram) ---------------------------------------
+
+REF_CV_SO = os.path.join(HERE, "_ref", "libcvariogram_ref.so")
+
+
+class CvVector(C.Structure):
+    _fields_ = [("data", C.c_double * 3)]
+
+
+class CvEllipsoid(C.Structure):
+    _fields_ = [("direction1", CvVector), ("direction2", CvVector), ("direction3", CvVector), ("R1", C.c_double),
+                ("R2", C.c_double), ("R3", C.c_double)]
+
+
+class CvTemplate(C.Structure):
+    _fields_ = [("lag_width", C.c_double), ("lag_separation", C.c_double), ("tol_distance", C.c_double),
+                ("num_lags", C.c_int), ("first_lag_distance", C.c_double), ("ellipsoid", CvEllipsoid)]
+
+
+class CvHardData(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("mask", C.POINTER(C.c_ubyte)), ("data_shape", C.c_int * 3),
+                ("data_strides", C.c_int * 3), ("mask_shape", C.c_int * 3), ("mask_strides", C.c_int * 3)]
+
+
+class CvPointSet(C.Structure):
+    _fields_ = [("xs", C.POINTER(C.c_float)), ("ys", C.POINTER(C.c_float)), ("zs", C.POINTER(C.c_float)),
+                ("values", C.POINTER(C.c_float)), ("size", C.c_int)]
+
+
+class CvFloatData(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("shape", C.c_int * 3), ("strides", C.c_int * 3)]
+
+
+_ref_cv = None
+
+
+def reference_cv_available():
+    return os.path.exists(REF_CV_SO)
+
+
+def ref_cv():
+    global _ref_cv
+    if _ref_cv is None:
+        _ref_cv = C.CDLL(REF_CV_SO)
+        _ref_cv.ref_cvar_lag_areas.restype = C.c_longlong
+    return _ref_cv
+
+
+def cv_template(lag_width, lag_separation, tol_distance, num_lags, first_lag_distance, radii, angles):
+    """A search template with the restated fill_ellipsoid_directions."""
+    t = CvTemplate()
+    t.lag_width, t.lag_separation, t.tol_distance = lag_width, lag_separation, tol_distance
+    t.num_lags, t.first_lag_distance = num_lags, first_lag_distance
+    d = (C.c_double * 9)()
+    restated().oracle_fill_ellipsoid_directions(d, C.c_double(angles[0]), C.c_double(angles[1]),
+                                                C.c_double(angles[2]))
+    t.ellipsoid.direction1.data[:] = d[0:3]
+    t.ellipsoid.direction2.data[:] = d[3:6]
+    t.ellipsoid.direction3.data[:] = d[6:9]
+    t.ellipsoid.R1, t.ellipsoid.R2, t.ellipsoid.R3 = radii
+    return t
+
+
+def cv_hard_data(data, mask):
+    """(struct, keep-alive arrays) for a 3-D float32 property and uint8 mask
+    of any memory order (strides in elements)."""
+    data = np.asarray(data, dtype=np.float32)
+    mask = np.asarray(mask, dtype=np.uint8)
+    hd = CvHardData()
+    hd.data = _ptr(data, C.c_float)
+    hd.mask = _ptr(mask, C.c_ubyte)
+    hd.data_shape[:] = data.shape
+    hd.mask_shape[:] = mask.shape
+    hd.data_strides[:] = [s // data.itemsize for s in data.strides]
+    hd.mask_strides[:] = [s // mask.itemsize for s in mask.strides]
+    return hd, (data, mask)
+
+
+def variograms(templ, data, mask, percent=100, lags=None):
+    """Restated calc_variograms: dict of result (float32), seq_sums, exact_sums, counts."""
+    lib = restated()
+    n = templ.num_lags if lags is None else lags
+    hd, keep = cv_hard_data(data, mask)
+    out = {"result": np.zeros(n, np.float32), "seq_sums": np.zeros(n), "exact_sums": np.zeros(n),
+           "counts": np.zeros(n, np.int64)}
+    lib.oracle_calc_variograms(C.byref(templ), C.byref(hd), _ptr(out["result"], C.c_float),
+                               _ptr(out["seq_sums"], C.c_double), _ptr(out["exact_sums"], C.c_double),
+                               _ptr(out["counts"], C.c_longlong), n, percent)
+    return out
+
+
+def cv_point_set(xs, ys, zs, values):
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (xs, ys, zs, values)]
+    ps = CvPointSet(_ptr(arrs[0], C.c_float), _ptr(arrs[1], C.c_float), _ptr(arrs[2], C.c_float),
+                    _ptr(arrs[3], C.c_float), len(arrs[3]))
+    return ps, arrs
+
+
+def variograms_points(templ, xs, ys, zs, values, lags=None):
+    lib = restated()
+    n = templ.num_lags if lags is None else lags
+    ps, keep = cv_point_set(xs, ys, zs, values)
+    out = {"result": np.zeros(n, np.float32), "seq_sums": np.zeros(n), "exact_sums": np.zeros(n),
+           "counts": np.zeros(n, np.int64)}
+    lib.oracle_calc_variograms_points(C.byref(templ), C.byref(ps), _ptr(out["result"], C.c_float),
+                                      _ptr(out["seq_sums"], C.c_double), _ptr(out["exact_sums"], C.c_double),
+                                      _ptr(out["counts"], C.c_longlong), n)
+    return out
+
+
+def ref_variograms(templ, data, mask, lags=None):
+    """The reference's calc_variograms (percent 100)."""
+    n = templ.num_lags if lags is None else lags
+    hd, keep = cv_hard_data(data, mask)
+    res = np.zeros(n, np.float32)
+    ref_cv().calc_variograms(C.byref(templ), C.byref(hd), _ptr(res, C.c_float), n, 100)
+    return res
+
+
+def ref_variograms_points(templ, xs, ys, zs, values, lags=None):
+    n = templ.num_lags if lags is None else lags
+    ps, keep = cv_point_set(xs, ys, zs, values)
+    res = np.zeros(n, np.float32)
+    ref_cv().calc_variograms_from_point_set(C.byref(templ), C.byref(ps), _ptr(res, C.c_float), n)
+    return res
+
+
+def _float_data(a):
+    fd = CvFloatData()
+    fd.data = _ptr(a, C.c_float)
+    fd.shape[:] = list(a.shape) + [1] * (3 - a.ndim)
+    st = [s // a.itemsize for s in a.strides]
+    fd.strides[:] = st + [0] * (3 - a.ndim)
+    return fd
+
+
+def stack_layers(layers, markers, nz, scalez, blank_value, result, reference=False):
+    """stack_layers into `result` (3-D float32, modified in place)."""
+    arr = (CvFloatData * len(layers))(*[_float_data(l) for l in layers])
+    mk = (C.c_int * len(markers))(*markers)
+    res = _float_data(result)
+    if reference:
+        ref_cv().cvar_stack_layers(arr, mk, len(layers), nz, C.c_float(scalez), blank_value, C.byref(res))
+    else:
+        restated().oracle_stack_layers(arr, mk, len(layers), nz, C.c_float(scalez), blank_value, C.byref(res))
+    return result
