@@ -173,12 +173,16 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
-    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io"],
-                    help="inc_io: INC property file read/write (hpgl_b200/bench_io.py), one GPU")
+    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram"],
+                    help="inc_io: INC property file read/write (hpgl_b200/bench_io.py); variogram: experimental "
+                         "variograms (hpgl_b200/bench_variogram.py); one GPU")
     args = ap.parse_args()
     if args.workload == "inc_io":
         from hpgl_b200 import bench_io
         return bench_io.run(args, ROOT)
+    if args.workload == "variogram":
+        from hpgl_b200 import bench_variogram
+        return bench_variogram.run(args, ROOT)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)

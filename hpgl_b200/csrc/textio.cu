@@ -780,6 +780,11 @@ TextIoTiming last_io_timing() {
     return g_last_timing;
 }
 
+void set_last_io_timing(const TextIoTiming &t) {
+    std::lock_guard<std::mutex> lock(g_io_mutex);
+    g_last_timing = t;
+}
+
 long long inc_count(const char *filename, bool is_byte, TextIoTiming *timing) {
     (void)is_byte;
     if (!filename) throw HpglError{HPGL_E_INVALID, "file name is null"};

@@ -39,7 +39,8 @@ void prop_write(int format, bool is_byte, const char *filename, const char *name
                 const unsigned char *data_b, const unsigned char *mask, long long size, float undefined_f,
                 unsigned char undefined_b, const unsigned char *remap, int remap_count, TextIoTiming *timing);
 
-// Timing of the last inc_read / inc_count / prop_write call.
+// Timing of the last inc_read / inc_count / prop_write / variogram call.
 TextIoTiming last_io_timing();
+void set_last_io_timing(const TextIoTiming &t);
 
 }  // namespace hpgl_b200

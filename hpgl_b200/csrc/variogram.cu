@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -36,6 +37,7 @@
 #include "../../include/cvariogram.h"
 #include "../../include/hpgl.h"
 #include "engine.h"
+#include "textio.h"
 #include "variogram.h"
 
 namespace hpgl_b200 {
@@ -56,6 +58,7 @@ constexpr int NT = 256;
 struct CvT {
     double d1[3], d2[3], d3[3];
     double R2, R3, tol, width, sep, first;
+    double R2m, R3m;  // quick-reject bounds: |ss2| above R2m means s2 > 1 after rounding
     int lags;
 };
 
@@ -72,6 +75,10 @@ CvT cv_t(const variogram_search_template_t &t, int lags) {
     c.width = t.m_lag_width;
     c.sep = t.m_lag_separation;
     c.first = t.m_first_lag_distance;
+    // |ss2| >= R2 (1 + 2^-20) makes the rounded quotient ss2 / R2 exceed 1,
+    // so the tunnel test fails whatever s3 is
+    c.R2m = c.R2 > 0 ? c.R2 * (1.0 + 1.0 / 1048576.0) : HUGE_VAL;
+    c.R3m = c.R3 > 0 ? c.R3 * (1.0 + 1.0 / 1048576.0) : HUGE_VAL;
     c.lags = lags;
     return c;
 }
@@ -83,9 +90,13 @@ __device__ __forceinline__ double dot3(const double *d, double x, double y, doub
     return __dadd_rn(r, __dmul_rn(z, d[2]));
 }
 
-// is_in_tunnel (variograms.cpp:26-40)
+// is_in_tunnel (variograms.cpp:26-40).  Vectors far outside the tunnel's
+// cross-section, or behind it (ss1 < 0 with a non-negative tolerance), fail
+// before the divisions and the square root: the exact test would fail them
+// too (dist > 1, or tol * dist >= 0 > ss1).
 __device__ __forceinline__ bool in_tunnel(const CvT &T, double x, double y, double z) {
     const double ss1 = dot3(T.d1, x, y, z), ss2 = dot3(T.d2, x, y, z), ss3 = dot3(T.d3, x, y, z);
+    if (fabs(ss2) > T.R2m || fabs(ss3) > T.R3m || (T.tol >= 0.0 && ss1 < 0.0)) return false;
     const double s2 = __ddiv_rn(ss2, T.R2), s3 = __ddiv_rn(ss3, T.R3);
     const double dist = __dsqrt_rn(__dadd_rn(__dmul_rn(s2, s2), __dmul_rn(s3, s3)));
     return dist <= 1.0 && __dmul_rn(T.tol, dist) <= ss1;
@@ -431,18 +442,23 @@ __global__ void __launch_bounds__(NT) k_cv_points(CvT T, Points P, const double 
     }
 }
 
+// one warp per lag: the blocks' partials, lanes strided, then the xor tree
 __global__ void k_cv_points_sum(const Partial *part, long long nparts, int lags, double *lag_sum,
                                 unsigned long long *lag_n) {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (l >= lags) return;
     DD s{0.0, 0.0};
     unsigned long long n = 0;
-    for (long long p = 0; p < nparts; ++p) {
+    for (long long p = lane; p < nparts; p += 32) {
         s = dd_add(s, part[p * lags + l].hi, part[p * lags + l].lo);
         n += part[p * lags + l].n;
     }
-    lag_sum[l] = __dadd_rn(s.hi, s.lo);
-    lag_n[l] = n;
+    warp_reduce(s, n);
+    if (lane == 0) {
+        lag_sum[l] = __dadd_rn(s.hi, s.lo);
+        lag_n[l] = n;
+    }
 }
 
 // ---- layer stacking --------------------------------------------------------
@@ -481,6 +497,28 @@ __global__ void k_stack_layers(const Layer *layers, const int *markers, int nlay
 // ---- host ------------------------------------------------------------------
 
 std::mutex g_cv_mutex;
+
+// CUDA events around a call's kernels, and its wall time
+struct CallTiming {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    TextIoTiming t;
+    CallTiming() {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+    }
+    ~CallTiming() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+    void done(long long units) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) t.ms_device = ms;
+        t.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        t.tokens = units;
+        set_last_io_timing(t);
+    }
+};
 
 cudaStream_t cv_stream() {
     static cudaStream_t s = nullptr;
@@ -595,6 +633,7 @@ void cv_grid(const variogram_search_template_t &t, const hard_data_t &hd, int re
     std::lock_guard<std::mutex> lock(g_cv_mutex);
     cudaStream_t s = cv_stream();
     DevMem M;
+    CallTiming timing;
     double w[6];
     window_of(t, w);
     // loop bounds of the reference: int i2 = (int)min; i2 <= max
@@ -660,14 +699,17 @@ void cv_grid(const variogram_search_template_t &t, const hard_data_t &hd, int re
     unsigned long long *d_ln = M.alloc<unsigned long long>((size_t)lags);
     const long long blocks = noff * nchunks;
     if (blocks > 0x7fffffffLL) throw HpglError{HPGL_E_CAPACITY, "too many offsets for one launch"};
+    CV_CHECK(cudaEventRecord(timing.e0, s));
     k_cv_pairs<<<(unsigned)blocks, NT, 0, s>>>(G, d_offs, d_cells, ncells, (int)nchunks, chunk,
                                                std::max(0, percent), d_part);
     k_cv_offset_sums<<<(unsigned)((noff * 32 + NT - 1) / NT), NT, 0, s>>>(d_part, noff, (int)nchunks, d_osum);
     k_cv_lag_sums<<<lags, NT, 0, s>>>(d_offs, d_osum, noff, d_lsum, d_ln);
+    CV_CHECK(cudaEventRecord(timing.e1, s));
     CV_CHECK(cudaMemcpyAsync(sums, d_lsum, (size_t)lags * sizeof(double), cudaMemcpyDeviceToHost, s));
     CV_CHECK(cudaMemcpyAsync(counts, d_ln, (size_t)lags * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CV_CHECK(cudaStreamSynchronize(s));
     CV_CHECK(cudaGetLastError());
+    timing.done(noff * ncells);
 }
 
 void cv_points(const variogram_search_template_t &t, const cont_point_set_t &ps, int result_length, double *sums,
@@ -685,6 +727,7 @@ void cv_points(const variogram_search_template_t &t, const cont_point_set_t &ps,
     std::lock_guard<std::mutex> lock(g_cv_mutex);
     cudaStream_t s = cv_stream();
     DevMem M;
+    CallTiming timing;
     // lag windows (init_lag_list, variograms.cpp:140-151)
     std::vector<double> st(lags), en(lags);
     for (int l = 0; l < lags; ++l) {
@@ -713,12 +756,15 @@ void cv_points(const variogram_search_template_t &t, const cont_point_set_t &ps,
     Partial *d_part = M.alloc<Partial>((size_t)gx * gy * lags);
     double *d_lsum = M.alloc<double>((size_t)lags);
     unsigned long long *d_ln = M.alloc<unsigned long long>((size_t)lags);
+    CV_CHECK(cudaEventRecord(timing.e0, s));
     k_cv_points<<<dim3(gx, gy), NT, smem, s>>>(T, P, d_st, d_en, tiles_per_y, d_part);
-    k_cv_points_sum<<<(lags + 63) / 64, 64, 0, s>>>(d_part, (long long)gx * gy, lags, d_lsum, d_ln);
+    k_cv_points_sum<<<(lags * 32 + NT - 1) / NT, NT, 0, s>>>(d_part, (long long)gx * gy, lags, d_lsum, d_ln);
+    CV_CHECK(cudaEventRecord(timing.e1, s));
     CV_CHECK(cudaMemcpyAsync(sums, d_lsum, (size_t)lags * 8, cudaMemcpyDeviceToHost, s));
     CV_CHECK(cudaMemcpyAsync(counts, d_ln, (size_t)lags * 8, cudaMemcpyDeviceToHost, s));
     CV_CHECK(cudaStreamSynchronize(s));
     CV_CHECK(cudaGetLastError());
+    timing.done((long long)n * n);
 }
 
 void cv_stack_layers(const float_data_t *layers, const int *markers, int nlayers, int nz, float scalez, int blank,

@@ -459,7 +459,8 @@ long long hpgl_b200_search_template(const hpgl_ik_params_t *params, int *out_xyz
    caller size the buffers of hpgl_read_inc_file_float/_byte. */
 long long hpgl_b200_inc_count_values(const char *filename);
 
-/* Timings of the calling process's last INC/GSLIB call, milliseconds. */
+/* Timings of the calling process's last INC/GSLIB call (or variogram call:
+   ms_device = its kernels, tokens = candidate pairs), milliseconds. */
 typedef struct {
     double ms_file;   /* reading or writing the file on the host */
     double ms_h2d;    /* host -> device copies */
