@@ -127,3 +127,75 @@ def test_not_provided_entry_points_report(native_lib):
     L.hpgl_sgs_simulation(None, None, None, None, None)
     assert L.hpgl_get_last_error() == N.HPGL_E_UNSUPPORTED
     assert b"not provided" in L.hpgl_get_last_exception_message()
+
+
+# ---- the experimental-variogram ABI (include/cvariogram.h) -------------------------
+
+CV_HEADER = os.path.join(ROOT, "include", "cvariogram.h")
+REF_CV_API = "/root/reference/src/geo_bsd/_cvariogram/api.h"
+CV_STRUCTS = ["vector_t", "ellipsoid_t", "variogram_search_template_t", "cont_point_set_t", "hard_data_t",
+              "float_data_t"]
+
+
+def test_cvariogram_symbols_exported(native_lib):
+    text = re.sub(r"/\*.*?\*/", "", open(CV_HEADER).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\b([a-z_0-9]+)\s*\(", text)) - {"defined"})
+    for want in ("fill_ellipsoid_directions", "calc_variograms", "calc_variograms_from_point_set",
+                 "cvar_stack_layers", "hpgl_b200_variogram_stats"):
+        assert want in names
+    missing = [n for n in names if n not in exported_symbols(N.LIB_PATH)]
+    assert not missing, missing
+
+
+def _cv_layout(header):
+    lines = ['#include <cstdio>', '#include "%s"' % header, "int main() {"]
+    for s in CV_STRUCTS:
+        lines.append('printf("%s %%zu\\n", sizeof(struct %s));' % (s, s))
+    lines.append("return 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "l.cpp")
+        open(src, "w").write("\n".join(lines))
+        exe = os.path.join(d, "l")
+        subprocess.run(["g++", "-o", exe, src], check=True, capture_output=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    return dict(line.rsplit(" ", 1) for line in out.splitlines())
+
+
+def test_cvariogram_struct_layouts():
+    ours = _cv_layout(CV_HEADER)
+    from hpgl_b200 import cvariogram as CVP
+    assert int(ours["variogram_search_template_t"]) == C.sizeof(CVP.variogram_search_template_t)
+    assert int(ours["hard_data_t"]) == C.sizeof(CVP.hard_data_t)
+    assert int(ours["cont_point_set_t"]) == C.sizeof(CVP.cont_point_set_t)
+    assert int(ours["float_data_t"]) == C.sizeof(CVP.float_data_t)
+    if os.path.exists(REF_CV_API):
+        assert ours == _cv_layout(REF_CV_API)
+
+
+def test_ellipsoid_directions_on_the_host(native_lib):
+    from hpgl_b200 import cvariogram as CVP
+    from oracle import oracle as O
+    for angles in ((40.0, 50.0, 60.0), (320.0, 0.0, 0.0), (0.0, 90.0, 0.0)):
+        e = CVP.Ellipsoid(10, 20, 30, *angles).ell
+        t = O.cv_template(1, 1, 1, 1, 0, (10, 20, 30), angles)
+        for k in ("direction1", "direction2", "direction3"):
+            assert list(getattr(e, k).data) == list(getattr(t.ellipsoid, k).data)
+
+
+def test_file_and_variogram_calls_need_the_gpu(native_lib, tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from hpgl_b200 import cvariogram as CVP
+    from hpgl_b200.geo_bsd import geo
+    path = str(tmp_path / "p.inc")
+    with open(path, "w") as f:
+        f.write("PORO\n1 2 3\n/\n")
+    with pytest.raises(geo.HpglError) as e:
+        geo.load_cont_property(path, -99.0, (3, 1, 1))
+    assert e.value.code == N.HPGL_E_CUDA
+    t = CVP.VariogramSearchTemplate(1, 1, 0.5, 4, 0, CVP.Ellipsoid(10, 2, 2, 0, 0, 0))
+    v = np.ones((4, 4, 2), np.float32)
+    with pytest.raises(geo.HpglError) as e:
+        CVP.CalcVariograms(t, (v, np.ones(v.shape, np.uint8)))
+    assert e.value.code == N.HPGL_E_CUDA
