@@ -569,13 +569,60 @@ int hpgl_b200_variogram_stats(variogram_search_template_t *templ, hard_data_t *d
     });
 }
 
-void hpgl_sgs_simulation(hpgl_cont_masked_array_t *, hpgl_sgs_params_t *, hpgl_non_parametric_cdf_t *, double *,
-                         hpgl_ubyte_array_t *) {
-    guarded("hpgl_sgs_simulation", [&] { not_provided("sequential Gaussian simulation"); });
+// Sequential Gaussian simulation (api.cpp:409-469 of the reference).  The
+// property is simulated in place; a CDF transform is not provided.
+static hpgl_ik_params_t sgs_ik_params(const hpgl_sgs_params_t *p) {
+    hpgl_ik_params_t q;
+    memset(&q, 0, sizeof(q));
+    q.m_covariance_type = p->m_covariance_type;
+    for (int i = 0; i < 3; ++i) {
+        q.m_ranges[i] = p->m_ranges[i];
+        q.m_angles[i] = p->m_angles[i];
+        q.m_radiuses[i] = p->m_radiuses[i];
+    }
+    q.m_sill = p->m_sill;
+    q.m_nugget = p->m_nugget;
+    q.m_max_neighbours = p->m_max_neighbours;
+    return q;
 }
-void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *, hpgl_sgs_params_t *, hpgl_non_parametric_cdf_t *,
-                             hpgl_float_array_t *, hpgl_ubyte_array_t *) {
-    guarded("hpgl_sgs_lvm_simulation", [&] { not_provided("sequential Gaussian simulation"); });
+
+static void sgs_call(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
+                     const float *lvm_mean, hpgl_ubyte_array_t *simulation_mask) {
+    if (!data || !params) throw HpglError{HPGL_E_INVALID, "data or params are null"};
+    if (cdf) throw HpglError{HPGL_E_UNSUPPORTED, "CDF transforms are not provided by this build"};
+    const hpgl_ik_params_t q = sgs_ik_params(params);
+    hpgl_b200_job_t j = base_job(lvm_mean ? HPGL_KIND_LVM
+                                          : (params->m_kriging_kind == 1 ? HPGL_KIND_SK : HPGL_KIND_OK),
+                                 &data->m_shape);
+    j.values = data->m_data;
+    j.mask = data->m_mask;
+    j.mean = lvm_mean;
+    j.params = &q;
+    j.n_params = 1;
+    j.sequential = 1;
+    j.seed = params->m_seed;
+    j.simulation_mask = simulation_mask ? simulation_mask->m_data : nullptr;
+    hpgl_b200_result_t r;
+    memset(&r, 0, sizeof(r));
+    r.out_values = data->m_data;
+    r.out_mask = data->m_mask;
+    run("sequential Gaussian simulation", j, r);
+}
+
+void hpgl_sgs_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
+                         double *, hpgl_ubyte_array_t *simulation_mask) {
+    // the stationary mean argument is unused: simple kriging runs with mean 0
+    // (sequential_gaussian_simulation.cpp:39-41)
+    guarded("hpgl_sgs_simulation", [&] { sgs_call(data, params, cdf, nullptr, simulation_mask); });
+}
+
+void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params,
+                             hpgl_non_parametric_cdf_t *cdf, hpgl_float_array_t *means,
+                             hpgl_ubyte_array_t *simulation_mask) {
+    guarded("hpgl_sgs_lvm_simulation", [&] {
+        if (!means || !means->m_data) throw HpglError{HPGL_E_INVALID, "mean array is null"};
+        sgs_call(data, params, cdf, means->m_data, simulation_mask);
+    });
 }
 void hpgl_sis_simulation(hpgl_ind_masked_array_t *, hpgl_ik_params_t *, int, int, hpgl_ubyte_array_t *) {
     guarded("hpgl_sis_simulation", [&] { not_provided("sequential indicator simulation"); });

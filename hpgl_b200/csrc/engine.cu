@@ -21,6 +21,7 @@
 #include <thread>
 
 #include "engine.h"
+#include "sgs_host.h"
 #include "kernels.cuh"
 
 namespace hpgl_b200 {
@@ -95,6 +96,7 @@ struct Arena {
 
 struct JobState {
     hpgl_b200_job_t job;
+    long long sgs_batches = 0;
     int precision;
     long long size;
     int K;
@@ -162,6 +164,11 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     if (job.kind == KIND_IK && job.n_params > 255) invalid("too many categories");
     S.precision = job.precision >= 0 ? job.precision : g_precision;
     if (S.cok) S.precision = HPGL_PRECISION_FP64;  // cokriging is solved in the reference's order only
+    if (job.sequential) {
+        if (job.kind != KIND_OK && job.kind != KIND_SK && job.kind != KIND_LVM)
+            invalid("sequential simulation takes the kinds OK, SK and LVM");
+        S.precision = HPGL_PRECISION_FP64;  // each node's draw depends on its exact kriging
+    }
     if (S.precision != HPGL_PRECISION_FP64 && S.precision != HPGL_PRECISION_MIXED) invalid("unknown precision");
     S.K = job.kind == KIND_IK ? job.n_params : 1;
     std::vector<KrigingParams> kp;
@@ -185,7 +192,7 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     }
     try {
         for (auto &g : S.groups) {
-            build_plan(g.plan, job.kind, job.nx, job.ny, job.nz, kp[g.k0], job.mask, threads);
+            build_plan(g.plan, job.kind, job.nx, job.ny, job.nz, kp[g.k0], job.mask, threads, job.sequential != 0);
             S.nmax_all = std::max(S.nmax_all, g.plan.nmax);
         }
     } catch (const std::domain_error &e) {
@@ -226,9 +233,10 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     S.pk.resize(S.K);
     for (int k = 0; k < S.K; ++k) S.pk[k] = (float)kp[k].marginal_prob;
     S.sk_mean = 0;
-    if (job.kind == KIND_SK)
+    // sequential simulation krigs with mean 0 (sequential_gaussian_simulation.cpp:39-41)
+    if (job.kind == KIND_SK && !job.sequential)
         S.sk_mean = job.sk_automatic_mean ? informed_mean(job.values, job.mask, S.size) : job.sk_mean;
-    S.want_variance = res.variance != nullptr;
+    S.want_variance = res.variance != nullptr || job.sequential;
     S.want_weights = res.weights != nullptr;
     S.kriged = 0;
     if (cont) {
@@ -395,6 +403,9 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.out_codes = cont ? nullptr : at<uint8_t>(S, A.o_out_codes);
     J.out_mask = at<uint8_t>(S, A.o_out_mask);
     J.variance = S.want_variance ? at<double>(S, A.o_variance) : nullptr;
+    J.sim_values = cont ? at<float>(S, A.o_values) : nullptr;
+    J.sim_mask = at<uint8_t>(S, A.o_mask);
+    J.sim_bits = at<uint32_t>(S, g.o_bits);
     J.status = at<int8_t>(S, A.o_status);
     J.probs = cont ? nullptr : at<float>(S, A.o_probs);
     J.weights = S.want_weights ? at<double>(S, A.o_weights) : nullptr;
@@ -595,11 +606,21 @@ static void sync_arena(SyncContext &C, size_t bytes) {
     C.cap = bytes;
 }
 
+// Sequential Gaussian simulation (sequential_simulation.h:49-122): the host
+// schedule, then one launch per batch of nodes that do not see each other;
+// the property in the arena is simulated in place and copied out.
+static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::chrono::steady_clock::time_point t0);
+
 void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     auto t0 = std::chrono::steady_clock::now();
     JobState S;
     prepare(S, job, res);
     res.ms_plan = ms_since(t0);
+    if (job.sequential) {
+        std::lock_guard<std::mutex> lock(g_sync_mutex);
+        sgs_run(S, res, sync_ctx(), t0);
+        return;
+    }
     std::lock_guard<std::mutex> lock(g_sync_mutex);
     SyncContext &C = sync_ctx();
     auto t1 = std::chrono::steady_clock::now();
@@ -627,6 +648,80 @@ void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     download(S, res, cnt, C.stream);
     res.ms_d2h = ms_since(t2);
     res.ms_total = ms_since(t0);
+}
+
+static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::chrono::steady_clock::time_point t0) {
+    const hpgl_b200_job_t &job = S.job;
+    Group &g = S.groups[0];
+    const Plan &P = g.plan;
+    SgsSchedule sch;
+    try {
+        sgs_schedule(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, P.radii, 1 << 16, sch);
+    } catch (const std::domain_error &e) {
+        throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
+    }
+    res.ms_plan = ms_since(t0);
+    auto t1 = std::chrono::steady_clock::now();
+    cudaStream_t s = C.stream;
+    sync_arena(C, S.ar.total);
+    S.base = C.arena;
+    upload(S, s);
+    const size_t nsim = sch.nodes.size();
+    int *d_nodes = nullptr;
+    double *d_xp = nullptr;
+    if (nsim > 0) {
+        CUDA_CHECK(cudaMalloc(&d_nodes, nsim * sizeof(int)));
+        CUDA_CHECK(cudaMalloc(&d_xp, nsim * sizeof(double)));
+    }
+    struct Free {
+        void *a, *b;
+        ~Free() {
+            if (a) cudaFree(a);
+            if (b) cudaFree(b);
+        }
+    } free_guard{d_nodes, d_xp};
+    if (nsim > 0) {
+        CUDA_CHECK(cudaMemcpyAsync(d_nodes, sch.nodes.data(), nsim * sizeof(int), cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(d_xp, sch.xp.data(), nsim * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    res.ms_h2d = ms_since(t1);
+    cudaEvent_t e0, e1;
+    CUDA_CHECK(cudaEventCreate(&e0));
+    CUDA_CHECK(cudaEventCreate(&e1));
+    CUDA_CHECK(cudaEventRecord(e0, s));
+    DevJob J = make_devjob(S, g);
+    Counters *cnt = at<Counters>(S, S.ar.o_counters);
+    CUDA_CHECK(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
+    CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
+    launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
+    for (size_t b = 0; b + 1 < sch.batches.size(); ++b) {
+        const long long a = sch.batches[b], e = sch.batches[b + 1];
+        if (e > a) launch_sgs(J, g.dp, d_nodes + a, d_xp + a, (int)(e - a), s);
+    }
+    CUDA_CHECK(cudaGetLastError());
+    CUDA_CHECK(cudaEventRecord(e1, s));
+    Counters hc;
+    CUDA_CHECK(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    res.ms_device = ms;
+    if (hc.err)
+        throw HpglError{HPGL_E_INTERNAL, "device invariant violated (error bits " + std::to_string(hc.err) + ")"};
+    auto t2 = std::chrono::steady_clock::now();
+    const size_t n = (size_t)S.size;
+    CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, S.ar.o_values), n * 4, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaMemcpyAsync(res.out_mask, at<uint8_t>(S, S.ar.o_mask), n, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    res.ms_d2h = ms_since(t2);
+    res.systems = (long long)nsim;
+    res.systems_fp64 = (long long)nsim;
+    res.failures = 0;
+    res.ms_total = ms_since(t0);
+    S.sgs_batches = (long long)sch.batches.size() - 1;
 }
 
 static const char *top_kernel_name(int nmax, int precision, int schedule) {

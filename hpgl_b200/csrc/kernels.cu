@@ -308,6 +308,11 @@ void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *n
     else launch_solve64_mixed(J, P, s, blocks_per_sm);
 }
 
+void launch_sgs(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s) {
+    if (P.nmax <= 32) launch_sgs32(J, P, nodes, xp, count, s);
+    else launch_sgs64(J, P, nodes, xp, count, s);
+}
+
 long long persistent_grid(const void *fn, int threads, size_t smem, int blocks_per_sm, long long units) {
     // occupancy of each kernel is looked up once
     static std::mutex mu;

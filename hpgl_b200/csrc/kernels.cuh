@@ -114,6 +114,12 @@ struct DevJob {
     double cok_coef;             // cross covariance = coef * cross_table
     double cok_svar;             // secondary variance (the system's corner)
     float cok_m1, cok_m2;        // primary and secondary means (float, mean_t)
+    // sequential simulation: the property, its mask and the informed bits,
+    // written as nodes are simulated (the same buffers as values / mask /
+    // bits)
+    float *sim_values;
+    uint8_t *sim_mask;
+    uint32_t *sim_bits;
 };
 
 // Launch tuning of the per-node kernels: the schedule (separate template
@@ -144,6 +150,11 @@ void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *n
 void launch_ik_argmax(const DevJob &J, cudaStream_t s);
 // cokriging.cu: colocated simple cokriging of every node (after the template search)
 void launch_cokriging(const DevJob &J, const DevPlan &P, cudaStream_t s);
+// One batch of sequential simulation: nodes[i] (none inside another's search
+// box) kriged from the current informed set and set from the quantile xp[i].
+void launch_sgs(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s);
+void launch_sgs32(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s);
+void launch_sgs64(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm);

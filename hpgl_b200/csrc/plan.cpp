@@ -203,7 +203,7 @@ double informed_mean(const float *values, const uint8_t *mask, long long size) {
 }
 
 void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
-                int threads) {
+                int threads, bool sequential) {
     static const bool timing = getenv("HPGL_B200_PLAN_TIMING") != nullptr;
     auto t_last = std::chrono::steady_clock::now();
     auto lap = [&](const char *what) {
@@ -223,8 +223,8 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     // Ordinary kriging and cokriging use the model itself; cokriging searches
     // with neighbour_lookup_t alone (simple_cokriging_markI.cpp:201, no
     // clusterizer).
-    P.truncated = kind != KIND_OK && !kind_is_cokriging(kind);
-    P.clusterizer = !kind_is_cokriging(kind);
+    P.truncated = (kind != KIND_OK && !kind_is_cokriging(kind)) || sequential;
+    P.clusterizer = !kind_is_cokriging(kind) && !sequential;
     for (int i = 0; i < 3; ++i) P.radii[i] = p.radii[i];
     const int rx = p.radii[0], ry = p.radii[1], rz = p.radii[2];
 

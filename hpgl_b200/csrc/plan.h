@@ -85,8 +85,11 @@ struct Plan {
 void validate_params(const KrigingParams &p, int kind);
 
 // Builds the plan of one kind/params over the informed `mask` (size nx*ny*nz).
+// sequential: the covariance of sequential simulation (truncated at the radii
+// for every kind, precalculated_covariances_t in sequential_simulation.h:67)
+// and the template search alone (neighbour_lookup_t, no clusterizer).
 void build_plan(Plan &plan, int kind, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
-                int threads);
+                int threads, bool sequential = false);
 
 // C(v) of `p`'s model over the box +-B, laid out like Plan::table.
 void fill_cov_table(std::vector<double> &table, const int B[3], const KrigingParams &p, int threads);

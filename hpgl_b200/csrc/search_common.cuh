@@ -73,4 +73,54 @@ __device__ __forceinline__ int template_segment(const DevJob &J, const DevPlan &
     return base;
 }
 
+// neighbour_lookup_t::find (sugarbox_neighbour_lookup.h:35-61) for one node:
+// the warp tests 32 template entries at a time against the informed-bit rows
+// (lane t entry base + t, lanes in template order) and keeps the first
+// max_neighbours hits.  List and count go to J.nb / J.nbcount.
+__device__ __forceinline__ void template_node(const DevJob &J, const DevPlan &P, int node, int lane) {
+    int x, y, z;
+    node_xyz(J, node, x, y, z);
+    const int nmax = P.nmax;
+    int *out = J.nb + (long long)node * nmax;
+    int cnt = 0;
+    for (int tb = 0; tb < P.tmpl_len && cnt < nmax; tb += 32) {
+        const int t = tb + lane;
+        bool hit = false;
+        int delta = 0;
+        if (t < P.tmpl_len) {
+            const int4 e = __ldg(&P.tmpl[t]);
+            delta = e.w;
+            const int yy = y + e.y, zz = z + e.z;
+            if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
+                const int px = x + e.x;  // padded x of the target cell
+                hit = (J.bits[((long long)zz * J.ny + yy) * P.wpr + (px >> 5)] >> (px & 31)) & 1u;
+            }
+        }
+        const unsigned b = __ballot_sync(FULL_MASK, hit);
+        const int rank = __popc(b & ((1u << lane) - 1u));
+        if (hit && cnt + rank < nmax) out[cnt + rank] = node + delta;
+        cnt += __popc(b);
+    }
+    if (lane == 0) J.nbcount[node] = min(cnt, nmax);
+}
+
+// The simulated value of a kriged node (sequential_simulation.h:106-110,
+// gaussian_cdf_t::inverse in gaussian_distribution.h:49-66): xp, the
+// standard normal quantile of the node's draw, times sqrt(variance) plus the
+// kriged estimate; N(0, 1) when the kriging failed.  The node joins the
+// informed set.
+__device__ __forceinline__ void sgs_set(const DevJob &J, const DevPlan &P, int node, double xp) {
+    double v;
+    if (J.status[node] == ST_SUCCESS)
+        v = __dadd_rn(__dmul_rn(xp, __dsqrt_rn(J.variance[node])), (double)J.out_values[node]);
+    else
+        v = __dadd_rn(__dmul_rn(xp, 1.0), 0.0);
+    J.sim_values[node] = __double2float_rn(v);
+    J.sim_mask[node] = 1;
+    int x, y, z;
+    node_xyz(J, node, x, y, z);
+    const int px = x + P.px;
+    atomicOr(J.sim_bits + ((long long)z * J.ny + y) * P.wpr + (px >> 5), 1u << (px & 31));
+}
+
 }  // namespace hpgl_b200

@@ -618,7 +618,32 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_fused32(DevJob J, DevPlan P) {
 
 constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
 
+// A batch of sequential simulation (nodes of at most 32 neighbours): one warp
+// per node: template search, the exact FP64 system, the simulated value.
+__global__ void __launch_bounds__(WARPS32 * 32) k_sgs32(DevJob J, DevPlan P, const int *nodes, const double *xp,
+                                                        int count) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    for (int i = blockIdx.x * WARPS32 + warp; i < count; i += gridDim.x * WARPS32) {
+        const int node = nodes[i];
+        template_node(J, P, node, lane);
+        __syncwarp();
+        const NodeFetch f = fetch_node(J, P, node, lane);
+        exact32_node(J, P, S, f, lane);
+        __syncwarp();
+        if (lane == 0) sgs_set(J, P, node, xp[i]);
+        __syncwarp();
+    }
+}
+
 }  // namespace
+
+void launch_sgs32(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    const long long g = persistent_grid((const void *)k_sgs32, WARPS32 * 32, SMEM32, 0, (count + WARPS32 - 1) / WARPS32);
+    k_sgs32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, P, nodes, xp, count);
+}
 
 void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm) {
     const long long segs = (long long)P.nseg * J.ny * J.nz;

@@ -429,6 +429,27 @@ __device__ __forceinline__ bool exact64_node(const DevJob &J, const DevPlan &P, 
     return true;
 }
 
+// A batch of sequential simulation (33-64 neighbours): one warp per node.
+__global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs64(DevJob J, DevPlan P, const int *nodes, const double *xp,
+                                                              int count) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ int s_cs[N64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
+    __syncthreads();
+    Exact64Smem &S = reinterpret_cast<Exact64Smem *>(dyn_smem)[warp];
+    for (int i = blockIdx.x * WARPS64_BLOCK + warp; i < count; i += gridDim.x * WARPS64_BLOCK) {
+        const int node = nodes[i];
+        template_node(J, P, node, lane);
+        __syncwarp();
+        const NodeFetch f = fetch_node(J, P, node, lane);
+        exact64_node(J, P, S, s_cs, f, lane);
+        __syncwarp();
+        if (lane == 0) sgs_set(J, P, node, xp[i]);
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, DevPlan P, const int *list,
                                                                       const int *n_list) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -760,6 +781,13 @@ void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_lis
     const long long g = persistent_grid((const void *)k_solve_exact64, WARPS64_BLOCK * 32, SMEM64_EXACT,
                                         blocks_per_sm, (n_max + WARPS64_BLOCK - 1) / WARPS64_BLOCK);
     k_solve_exact64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, node_list, n_list);
+}
+
+void launch_sgs64(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    const long long g = persistent_grid((const void *)k_sgs64, WARPS64_BLOCK * 32, SMEM64_EXACT, 0,
+                                        (count + WARPS64_BLOCK - 1) / WARPS64_BLOCK);
+    k_sgs64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, nodes, xp, count);
 }
 
 void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s, int blocks_per_sm) {

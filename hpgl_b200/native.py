@@ -46,7 +46,8 @@ class Job(C.Structure):
                 ("precision", C.c_int),
                 ("secondary_values", C.POINTER(C.c_float)), ("secondary_mask", C.POINTER(C.c_ubyte)),
                 ("primary_mean", C.c_double), ("secondary_mean", C.c_double), ("secondary_variance", C.c_double),
-                ("correlation", C.c_double), ("secondary_cov", C.c_void_p)]
+                ("correlation", C.c_double), ("secondary_cov", C.c_void_p),
+                ("sequential", C.c_int), ("seed", C.c_longlong), ("simulation_mask", C.POINTER(C.c_ubyte))]
 
 
 class Result(C.Structure):
@@ -158,6 +159,12 @@ class _Prepared:
             if self.kind == "cok2":
                 self.scov = cov_struct(job["secondary_cov"])
                 j.secondary_cov = C.cast(C.pointer(self.scov), C.c_void_p)
+        if job.get("sequential"):
+            j.sequential = 1
+            j.seed = int(job.get("seed", 0))
+            sm = job.get("simulation_mask")
+            self.sim_mask = None if sm is None else np.ascontiguousarray(sm, dtype=np.uint8)
+            j.simulation_mask = _ptr(self.sim_mask, C.c_ubyte)
         self.job = j
         self.out = self.values.copy() if self.cont else self.codes.copy()
         self.out_mask = self.mask.copy()
@@ -214,6 +221,13 @@ def krige(job, precision=None, kind=None, dumps=False, sk_auto_mean=False, media
     if rc != 0:
         raise HpglError(rc, L.hpgl_get_last_exception_message().decode())
     return p.collect()
+
+
+def simulate(job, seed, kind=None, simulation_mask=None):
+    """Sequential Gaussian simulation of a cont job (kind "sk": mean 0, "ok",
+    or "lvm"); returns the dict of krige() with the simulated property."""
+    j = dict(job, sequential=True, seed=seed, simulation_mask=simulation_mask)
+    return krige(j, precision="fp64", kind=kind)
 
 
 def bench(job, precision="mixed", iters=5, warmup=3, flush_bytes=256 << 20, kind=None):

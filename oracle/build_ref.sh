@@ -5,8 +5,11 @@
 # reference checkout, into oracle/_ref/libhpgl_ref.so (git-ignored; it is
 # copied along with the working tree to the machine that runs the GPU tests).
 # Nothing from the reference is copied into this repository: the shim headers
-# in oracle/ref_shim/ stand in for boost and the CLAPACK headers, and
-# oracle/lapack_restated.c supplies dpotrf_/dpotrs_.
+# in oracle/ref_shim/ stand in for boost (boost::mt11213b restated from its
+# published parameters) and the CLAPACK headers, oracle/lapack_restated.c
+# supplies dpotrf_/dpotrs_, and oracle/gen_primes.py writes the prime table
+# the sequential simulation's path generator includes (primes.txt, missing
+# from the checkout: every prime in increasing order past 10^7).
 #
 # Flags: -O2 -fopenmp as the reference's release build (SConstruct:23-24),
 # with -ffp-contract=off instead of -march=native so that no a*b+c is fused.
@@ -19,22 +22,25 @@ if [ ! -d "$REF/geo_bsd/hpgl" ]; then
     exit 3
 fi
 mkdir -p "$OUT/obj"
-CXXFLAGS="-std=gnu++11 -O2 -fopenmp -ffp-contract=off -fPIC -w -DNDEBUG -I$HERE/ref_shim -I$REF/tnt_126 -I$REF/geo_bsd/hpgl"
+mkdir -p "$OUT/gen"
+[ -s "$OUT/gen/primes.txt" ] || python3 "$HERE/gen_primes.py" "$OUT/gen/primes.txt"
+CXXFLAGS="-std=gnu++11 -O2 -fopenmp -ffp-contract=off -fPIC -w -DNDEBUG -I$OUT/gen -I$HERE/ref_shim -I$REF/tnt_126 -I$REF/geo_bsd/hpgl"
 TUS="api.cpp api_helpers.cpp ordinary_kriging.cpp simple_kriging.cpp lvm_kriging.cpp indicator_kriging.cpp
 median_ik.cpp clusterizer.cpp covariance_field.cpp covariance_param.cpp neighbourhood_param.cpp ok_params.cpp
 sk_params_t.cpp ik_params.cpp calc_mean.cpp cdf_utils.cpp mean_provider.cpp output.cpp pretty_printer.cpp
 progress_reporter.cpp kriging_stats.cpp hpgl_exception.cpp sugarbox_grid.cpp set_thread_num.cpp
 property_writer.cpp read_inc_file.cpp simple_cokriging_markI.cpp sgs_params.cpp bs_assert.cpp logging.cpp
-gauss_solver.cpp load_property_from_file.cpp"
+gauss_solver.cpp load_property_from_file.cpp path_random_generator.cpp bs_random_generator.cpp
+sequential_gaussian_simulation.cpp sequential_indicator_simulation.cpp sample.cpp random_node_enumerator.cpp"
 pids=()
 for f in $TUS; do
     g++ $CXXFLAGS -c "$REF/geo_bsd/hpgl/$f" -o "$OUT/obj/${f%.cpp}.o" &
     pids+=($!)
 done
-g++ $CXXFLAGS -c "$HERE/ref_stubs.cpp" -o "$OUT/obj/ref_stubs.o" & pids+=($!)
 g++ $CXXFLAGS -c "$HERE/ref_dump.cpp" -o "$OUT/obj/ref_dump.o" & pids+=($!)
 gcc -O2 -ffp-contract=off -fPIC -c "$HERE/lapack_restated.c" -o "$OUT/obj/lapack_restated.o" & pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
+rm -f "$OUT/obj/ref_stubs.o"
 g++ -shared -fopenmp -o "$OUT/libhpgl_ref.so" "$OUT"/obj/*.o
 echo "built $OUT/libhpgl_ref.so"
 

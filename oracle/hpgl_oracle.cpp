@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -785,6 +786,172 @@ int oracle_krige(int kind, int nx, int ny, int nz, const float *values, const un
         }
         return 1;
     }
+}
+
+// ---- sequential Gaussian simulation --------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// path_random_generator.cpp:20-66: a full-period linear congruential walk
+// over [0, size).  The reference includes its prime table from primes.txt,
+// which its checkout lacks; init_rnd's asserts leave one reading of it, every
+// prime in increasing order past the grid size, which this restates.
+struct path_walk {
+    long long A = 1, C = 2, M = 1, R = 0;
+    path_walk(long long size, long long seed) {
+        M = size;
+        const long long lim = std::max<long long>(size, 3) + 1;
+        std::vector<char> comp((size_t)lim + 1, 0);
+        std::vector<long long> primes;
+        for (long long i = 2; i <= lim; ++i) {
+            if (comp[(size_t)i]) continue;
+            primes.push_back(i);
+            for (long long j = i * i; j <= lim; j += i) comp[(size_t)j] = 1;
+        }
+        for (long long p : primes) {
+            if (p > size) break;
+            if (size % p == 0) A *= p;
+        }
+        if (M % 4 == 0) A *= 2;
+        A += 1;
+        size_t idx = 0;
+        while (idx + 1 < primes.size() && primes[idx + 1] <= size / 3) ++idx;
+        for (long long k = (long long)idx; k >= 0; k--) {
+            C = primes[(size_t)k];
+            if (std::floor(double(size) / double(C)) != (double(size) / double(C))) break;
+        }
+        R = seed % size;
+    }
+    long long next() {
+        const long long r = R;
+        R = (A * R + C) % M;
+        return r;
+    }
+};
+
+// boost::mt11213b: the Mersenne Twister (Matsumoto and Nishimura, 1998) with
+// boost's published mt11213b parameters and the usual seeding.
+struct mt11213b {
+    enum { N = 351, M = 175, R = 19 };
+    uint32_t x[N];
+    int i = N;
+    explicit mt11213b(uint32_t s) {
+        x[0] = s;
+        for (int k = 1; k < N; ++k) x[k] = 1812433253u * (x[k - 1] ^ (x[k - 1] >> 30)) + (uint32_t)k;
+    }
+    uint32_t operator()() {
+        if (i >= N) {
+            const uint32_t upper = ~((1u << R) - 1u), lower = (1u << R) - 1u;
+            for (int k = 0; k < N; ++k) {
+                const uint32_t y = (x[k] & upper) | (x[(k + 1) % N] & lower);
+                x[k] = x[(k + M) % N] ^ (y >> 1) ^ ((y & 1u) ? 0xccab8ee7u : 0u);
+            }
+            i = 0;
+        }
+        uint32_t y = x[i++];
+        y ^= y >> 11;
+        y ^= (y << 7) & 0x31b6ab00u;
+        y ^= (y << 15) & 0xffe50000u;
+        y ^= y >> 17;
+        return y;
+    }
+    // mt_random_generator_t::operator()() (bs_random_generator.cpp:16-19)
+    double uniform() { return double((*this)()) / double(0xffffffffu); }
+};
+
+// gaussian_cdf_t::inverse (gaussian_distribution.h:49-66), Odeh and Evans's
+// rational approximation: the standard normal quantile of p.
+double gaussian_quantile(double p) {
+    const double ps[] = {-0.322232431088, -1.0, -0.342242088547, -0.0204231210245, -0.453642210148e-4};
+    const double qs[] = {0.0993484626060, 0.588581570495, 0.531103462366, 0.103537752850, 0.38560700634e-2};
+    const double p2 = (p > 0.5) ? (1 - p) : p;
+    const double y = std::sqrt(std::log(1 / (p2 * p2)));
+    double xp = y + ((((ps[4] * y + ps[3]) * y + ps[2]) * y + ps[1]) * y + ps[0]) /
+                        ((((qs[4] * y + qs[3]) * y + qs[2]) * y + qs[1]) * y + qs[0]);
+    if (p < 0.5) xp = -xp;
+    return xp;
+}
+
+// do_sequential_gausian_simulation (sequential_simulation.h:49-122) with
+// neighbour_lookup_t over the precalculated (radius-truncated) covariance:
+// nodes in the walk's order; each uninformed node inside the simulation mask
+// is kriged from the informed cells and the nodes simulated before it (SK with
+// mean 0, OK, or SK with the mean cube), and set to the Gaussian quantile of
+// the next draw with the kriged mean and variance (N(0, 1) when the kriging
+// fails).
+void sgs(const grid3 &g, float *values, unsigned char *mask, const oracle_params_t &p, bool ordinary,
+         const float *lvm, long long seed, const unsigned char *sim_mask, int *order, int *n_order) {
+    covariance cov(p, true);
+    const std::vector<int> tmpl = build_template(cov, p);
+    const int n_t = (int)tmpl.size() / 3;
+    const long long size = g.size();
+    path_walk path(size, seed);
+    mt11213b gen((uint32_t)seed);
+    int count = 0;
+    long long node = path.next();
+    for (long long counter = 0; counter < size; ++counter, node = path.next()) {
+        if (mask[node]) continue;
+        if (sim_mask && sim_mask[node] != 1) continue;
+        if (order) order[count] = (int)node;
+        ++count;
+        int center[3];
+        g.loc((int)node, center);
+        std::vector<int> nb, coords;
+        for (int t = 0; t < n_t && (int)nb.size() < p.max_neighbours; ++t) {
+            int pt[3] = {center[0] + tmpl[3 * t], center[1] + tmpl[3 * t + 1], center[2] + tmpl[3 * t + 2]};
+            const int idx = g.index(pt);
+            if (idx >= 0 && mask[idx]) nb.push_back(idx);
+        }
+        auto mean_at = [&](int i) -> float { return lvm ? lvm[i] : 0.0f; };
+        bool ok = false;
+        double variance = -1;
+        float mean = 0.f;
+        if (!nb.empty()) {
+            coords_of(g, nb, coords);
+            std::vector<double> w;
+            ok = kriging_weights(ordinary, center, coords, cov, w, variance);
+            if (ok) {
+                float result = mean_at((int)node);
+                for (size_t i = 0; i < nb.size(); ++i) result += (float)(w[i] * (values[nb[i]] - mean_at(nb[i])));
+                mean = result;
+            }
+        }
+        const double u = gen.uniform();
+        const double xp = gaussian_quantile(u);
+        const double value = ok ? xp * std::sqrt(variance) + (double)mean : xp * std::sqrt(1.0) + 0.0;
+        values[node] = (float)value;
+        mask[node] = 1;
+    }
+    if (n_order) *n_order = count;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Sequential Gaussian simulation in place on values / mask; `order`
+// (optional) receives the simulated nodes in simulation order.
+int oracle_sgs(int nx, int ny, int nz, float *values, unsigned char *mask, const oracle_params_t *p, int ordinary,
+               const float *lvm, long long seed, const unsigned char *sim_mask, int *order, int *n_order, char *err,
+               int err_len) {
+    try {
+        if (p->max_neighbours > 64) throw std::runtime_error("max_neighbours > 64 is not restated");
+        sgs(grid3{nx, ny, nz}, values, mask, *p, ordinary != 0, lvm, seed, sim_mask, order, n_order);
+        return 0;
+    } catch (const std::exception &e) {
+        if (err && err_len > 0) {
+            strncpy(err, e.what(), err_len - 1);
+            err[err_len - 1] = 0;
+        }
+        return 1;
+    }
+}
+
+// The standard normal quantiles of the first n draws of the generator.
+void oracle_sgs_draws(long long seed, long long n, double *xp) {
+    mt11213b gen((uint32_t)seed);
+    for (long long k = 0; k < n; ++k) xp[k] = gaussian_quantile(gen.uniform());
 }
 
 // The sorted search template as (dx,dy,dz) triples; returns its length or -1

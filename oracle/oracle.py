@@ -701,3 +701,81 @@ def stack_layers(layers, markers, nz, scalez, blank_value, result, reference=Fal
     else:
         restated().oracle_stack_layers(arr, mk, len(layers), nz, C.c_float(scalez), blank_value, C.byref(res))
     return result
+
+
+# ---- sequential Gaussian simulation --------------------------------------------
+
+class HpglSgsParams(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3), ("max_neighbours", C.c_int),
+                ("kriging_kind", C.c_int), ("seed", C.c_long), ("min_neighbours", C.c_int)]
+
+
+class HpglFloatArray(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("shape", HpglShape)]
+
+
+class HpglUbyteArray(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("shape", HpglShape)]
+
+
+def sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None):
+    """Restated sequential Gaussian simulation: (values, mask, order of the
+    simulated nodes)."""
+    lib = restated()
+    nx, ny, nz = job["shape"]
+    values = np.array(job["values"], dtype=np.float32)
+    mask = np.array(job["mask"], dtype=np.uint8)
+    order = np.zeros(values.size, dtype=np.int32)
+    n_order = C.c_int(0)
+    sm = None if sim_mask is None else np.ascontiguousarray(sim_mask, dtype=np.uint8)
+    lv = None if lvm is None else np.ascontiguousarray(lvm, dtype=np.float32)
+    err = C.create_string_buffer(512)
+    rc = lib.oracle_sgs(nx, ny, nz, _ptr(values, C.c_float), _ptr(mask, C.c_ubyte),
+                        C.byref(oracle_params(job["params"][0])), int(ordinary), _ptr(lv, C.c_float),
+                        C.c_longlong(seed), _ptr(sm, C.c_ubyte), _ptr(order, C.c_int), C.byref(n_order), err, 512)
+    if rc != 0:
+        raise RuntimeError("oracle: " + err.value.decode())
+    return values, mask, order[:n_order.value]
+
+
+def sgs_draws(seed, n):
+    """The standard normal quantiles of the first n draws (restated generator)."""
+    xp = np.zeros(n)
+    restated().oracle_sgs_draws(C.c_longlong(seed), C.c_longlong(n), _ptr(xp, C.c_double))
+    return xp
+
+
+def ref_sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None):
+    """The reference's hpgl_sgs_simulation / hpgl_sgs_lvm_simulation (no CDF
+    transform), compiled with oracle/ref_shim's boost::mt11213b and the
+    generated prime table."""
+    ref = reference()
+    nx, ny, nz = job["shape"]
+    sh = _shape((nx, ny, nz))
+    values = np.array(job["values"], dtype=np.float32)
+    mask = np.array(job["mask"], dtype=np.uint8)
+    arr = HpglContArray(_ptr(values, C.c_float), _ptr(mask, C.c_ubyte), sh)
+    p = job["params"][0]
+    q = HpglSgsParams()
+    q.covariance_type = p["cov_type"]
+    q.ranges[:] = p["ranges"]
+    q.angles[:] = p["angles"]
+    q.sill, q.nugget = p["sill"], p["nugget"]
+    q.radiuses[:] = p["radii"]
+    q.max_neighbours = p["max_neighbours"]
+    q.kriging_kind = 0 if ordinary else 1
+    q.seed = seed
+    q.min_neighbours = 0
+    sm_keep = None
+    smp = None
+    if sim_mask is not None:
+        sm_keep = np.ascontiguousarray(sim_mask, dtype=np.uint8)
+        smp = C.byref(HpglUbyteArray(_ptr(sm_keep, C.c_ubyte), sh))
+    if lvm is not None:
+        lv = np.ascontiguousarray(lvm, dtype=np.float32)
+        fa = HpglFloatArray(_ptr(lv, C.c_float), sh)
+        ref.hpgl_sgs_lvm_simulation(C.byref(arr), C.byref(q), None, C.byref(fa), smp)
+    else:
+        ref.hpgl_sgs_simulation(C.byref(arr), C.byref(q), None, None, smp)
+    return values, mask

@@ -124,9 +124,11 @@ def test_no_gpu_is_an_error_not_a_fallback(native_lib):
 
 def test_not_provided_entry_points_report(native_lib):
     L = native_lib
-    L.hpgl_sgs_simulation(None, None, None, None, None)
+    L.hpgl_sis_simulation(None, None, 0, 0, None)
     assert L.hpgl_get_last_error() == N.HPGL_E_UNSUPPORTED
     assert b"not provided" in L.hpgl_get_last_exception_message()
+    L.hpgl_sgs_simulation(None, None, None, None, None)
+    assert L.hpgl_get_last_error() == N.HPGL_E_INVALID
 
 
 # ---- the experimental-variogram ABI (include/cvariogram.h) -------------------------

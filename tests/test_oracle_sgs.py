@@ -1,0 +1,56 @@
+"""The CPU restatement of sequential Gaussian simulation (oracle/hpgl_oracle.cpp:
+random path, boost::mt11213b draws, Odeh-Evans quantile, kriging from the
+informed and already simulated nodes) against the reference's own sources
+compiled by oracle/build_ref.sh, whose missing pieces are supplied as
+oracle/ref_shim's boost::mt11213b and oracle/gen_primes.py's prime table."""
+
+import numpy as np
+import pytest
+
+from hpgl_b200 import workloads as W
+from oracle import oracle as O
+
+need_ref = pytest.mark.skipif(not O.reference_available(), reason="compiled reference not present")
+
+
+def _job(shape=(20, 18, 6), seed=4, n=12, cov=W.SPHERICAL):
+    j = W.ok_50x50x20(shape=shape, seed=seed)
+    j["params"] = [dict(j["params"][0], max_neighbours=n, cov_type=cov)]
+    return j
+
+
+@need_ref
+@pytest.mark.parametrize("ordinary", [False, True])
+@pytest.mark.parametrize("seed", [1, 7, 123456])
+def test_sgs_matches_reference(ordinary, seed):
+    job = _job()
+    v1, m1, order = O.sgs(job, ordinary=ordinary, seed=seed)
+    v2, m2 = O.ref_sgs(job, ordinary=ordinary, seed=seed)
+    assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32))
+    assert np.array_equal(m1, m2)
+    assert len(order) == int((job["mask"] == 0).sum())
+
+
+@need_ref
+def test_sgs_lvm_mask_and_exponential_match_reference():
+    job = _job(shape=(16, 14, 8), seed=9, n=20, cov=W.EXPONENTIAL)
+    rng = np.random.default_rng(3)
+    lvm = (0.1 * rng.normal(size=job["values"].size)).astype(np.float32)
+    sm = (rng.random(job["values"].size) < 0.6).astype(np.uint8)
+    v1, m1, _ = O.sgs(job, seed=5, sim_mask=sm, lvm=lvm)
+    v2, m2 = O.ref_sgs(job, seed=5, sim_mask=sm, lvm=lvm)
+    assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32)) and np.array_equal(m1, m2)
+
+
+def test_path_visits_every_node_once():
+    # the walk is a full-period LCG: the simulation order is a permutation of
+    # the uninformed nodes
+    job = _job(shape=(17, 11, 5), seed=2)
+    _, _, order = O.sgs(job, seed=99)
+    uninformed = np.nonzero(job["mask"] == 0)[0]
+    assert sorted(order.tolist()) == uninformed.tolist()
+
+
+def test_draws_are_standard_normal():
+    xp = O.sgs_draws(42, 200000)
+    assert abs(xp.mean()) < 0.01 and abs(xp.std() - 1) < 0.01
