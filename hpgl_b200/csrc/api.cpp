@@ -14,6 +14,7 @@
 #include "engine.h"
 #include "kernels.cuh"
 #include "plan.h"
+#include "sgs_host.h"
 #include "textio.h"
 #include "variogram.h"
 
@@ -184,6 +185,14 @@ void hpgl_b200_set_precision(int precision) {
     });
 }
 int hpgl_b200_get_precision(void) { return default_precision(); }
+
+void hpgl_b200_set_sim_window(int window) {
+    guarded("hpgl_b200_set_sim_window", [&] {
+        if (window == 0) window = 1 << 18;
+        if (window < 1 || window > (1 << 24)) throw HpglError{HPGL_E_INVALID, "window must be in [1, 2^24]"};
+        set_sim_window(window);
+    });
+}
 
 void hpgl_ordinary_kriging(hpgl_cont_masked_array_t *input_data, hpgl_ok_params_t *params,
                            hpgl_cont_masked_array_t *output_data) {
@@ -569,8 +578,11 @@ int hpgl_b200_variogram_stats(variogram_search_template_t *templ, hard_data_t *d
     });
 }
 
-// Sequential Gaussian simulation (api.cpp:409-469 of the reference).  The
-// property is simulated in place; a CDF transform is not provided.
+// Sequential Gaussian simulation (api.cpp:409-469 of the reference), in
+// place on the property.  With a CDF the informed values (and the LVM mean
+// cube) are normal-score transformed first and every informed value is
+// transformed back at the end (sequential_gaussian_simulation.cpp:32-35,
+// 72-73, 97-103, 119-123).
 static hpgl_ik_params_t sgs_ik_params(const hpgl_sgs_params_t *p) {
     hpgl_ik_params_t q;
     memset(&q, 0, sizeof(q));
@@ -589,7 +601,21 @@ static hpgl_ik_params_t sgs_ik_params(const hpgl_sgs_params_t *p) {
 static void sgs_call(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
                      const float *lvm_mean, hpgl_ubyte_array_t *simulation_mask) {
     if (!data || !params) throw HpglError{HPGL_E_INVALID, "data or params are null"};
-    if (cdf) throw HpglError{HPGL_E_UNSUPPORTED, "CDF transforms are not provided by this build"};
+    if (!data->m_data || !data->m_mask) throw HpglError{HPGL_E_INVALID, "property arrays are null"};
+    const long long n = volume(&data->m_shape);
+    NonParametricCdf c{nullptr, nullptr, 0};
+    std::vector<float> gaussian_mean;
+    if (cdf) {
+        if (!cdf->m_values || !cdf->m_probs || cdf->m_size <= 0)
+            throw HpglError{HPGL_E_INVALID, "the CDF has no values"};
+        c = NonParametricCdf{cdf->m_values, cdf->m_probs, cdf->m_size};
+        cdf_to_gaussian(c, data->m_data, data->m_data, data->m_mask, n, host_threads());
+        if (lvm_mean) {
+            gaussian_mean.resize((size_t)n);
+            cdf_to_gaussian(c, lvm_mean, gaussian_mean.data(), nullptr, n, host_threads());
+            lvm_mean = gaussian_mean.data();
+        }
+    }
     const hpgl_ik_params_t q = sgs_ik_params(params);
     hpgl_b200_job_t j = base_job(lvm_mean ? HPGL_KIND_LVM
                                           : (params->m_kriging_kind == 1 ? HPGL_KIND_SK : HPGL_KIND_OK),
@@ -607,6 +633,7 @@ static void sgs_call(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, 
     r.out_values = data->m_data;
     r.out_mask = data->m_mask;
     run("sequential Gaussian simulation", j, r);
+    if (cdf) gaussian_to_cdf(c, data->m_data, data->m_mask, n, host_threads());
 }
 
 void hpgl_sgs_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,

@@ -7,6 +7,7 @@
 // at once, each on its own stream with an arena from the stream-ordered pool
 // (cudaMallocAsync), admitted against an HBM budget.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -41,6 +42,8 @@ static int env_precision() {
 static int g_precision = env_precision();
 int default_precision() { return g_precision; }
 void set_default_precision(int p) { g_precision = p; }
+static std::atomic<int> g_sim_window{1 << 18};
+void set_sim_window(int window) { g_sim_window = window; }
 
 static double ms_since(std::chrono::steady_clock::time_point t) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
@@ -96,7 +99,6 @@ struct Arena {
 
 struct JobState {
     hpgl_b200_job_t job;
-    long long sgs_batches = 0;
     int precision;
     long long size;
     int K;
@@ -654,36 +656,63 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     const hpgl_b200_job_t &job = S.job;
     Group &g = S.groups[0];
     const Plan &P = g.plan;
-    SgsSchedule sch;
+    SimPath path;
+    std::vector<double> xp;
     try {
-        sgs_schedule(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, P.radii, 1 << 16, sch);
+        sim_path(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, path);
     } catch (const std::domain_error &e) {
         throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
     }
+    gaussian_quantiles(path.u, xp, host_threads());
     res.ms_plan = ms_since(t0);
     auto t1 = std::chrono::steady_clock::now();
     cudaStream_t s = C.stream;
     sync_arena(C, S.ar.total);
     S.base = C.arena;
     upload(S, s);
-    const size_t nsim = sch.nodes.size();
-    int *d_nodes = nullptr;
-    double *d_xp = nullptr;
-    if (nsim > 0) {
-        CUDA_CHECK(cudaMalloc(&d_nodes, nsim * sizeof(int)));
-        CUDA_CHECK(cudaMalloc(&d_xp, nsim * sizeof(double)));
-    }
+    const long long nsim = (long long)path.nodes.size();
+    const int window = g_sim_window.load();
+    const size_t bits_bytes = ((size_t)P.wpr * P.ny * P.nz + 2) * 4;
+    // scratch: control, path, quantiles, ranks, pending bits, window buffers, flags
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += align_up(bytes ? bytes : 1);
+        return o;
+    };
+    const size_t o_ctl = take(sizeof(SgsCtl)), o_nodes = take((size_t)nsim * 4), o_xp = take((size_t)nsim * 8),
+                 o_rank = take((size_t)S.size * 4), o_pend = take(bits_bytes), o_blocker = take((size_t)nsim * 4),
+                 o_done = take((size_t)nsim), o_w0 = take((size_t)window * 4), o_w1 = take((size_t)window * 4),
+                 o_ok = take((size_t)window);
+    unsigned char *scratch = nullptr;
+    CUDA_CHECK(cudaMalloc(&scratch, off));
     struct Free {
-        void *a, *b;
-        ~Free() {
-            if (a) cudaFree(a);
-            if (b) cudaFree(b);
-        }
-    } free_guard{d_nodes, d_xp};
+        void *p;
+        ~Free() { cudaFree(p); }
+    } free_guard{scratch};
+    SgsState G;
+    G.ctl = reinterpret_cast<SgsCtl *>(scratch + o_ctl);
+    G.nodes = reinterpret_cast<const int *>(scratch + o_nodes);
+    G.xp = reinterpret_cast<const double *>(scratch + o_xp);
+    G.rank_of = reinterpret_cast<const int *>(scratch + o_rank);
+    G.pend = reinterpret_cast<uint32_t *>(scratch + o_pend);
+    G.blocker = reinterpret_cast<int *>(scratch + o_blocker);
+    G.done = scratch + o_done;
+    G.win0 = reinterpret_cast<int *>(scratch + o_w0);
+    G.win1 = reinterpret_cast<int *>(scratch + o_w1);
+    G.ok = scratch + o_ok;
+    SgsCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.window = window;
+    hc.total = nsim;
+    CUDA_CHECK(cudaMemcpyAsync(G.ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
     if (nsim > 0) {
-        CUDA_CHECK(cudaMemcpyAsync(d_nodes, sch.nodes.data(), nsim * sizeof(int), cudaMemcpyHostToDevice, s));
-        CUDA_CHECK(cudaMemcpyAsync(d_xp, sch.xp.data(), nsim * sizeof(double), cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(scratch + o_nodes, path.nodes.data(), (size_t)nsim * 4, cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(scratch + o_xp, xp.data(), (size_t)nsim * 8, cudaMemcpyHostToDevice, s));
     }
+    CUDA_CHECK(cudaMemsetAsync(G.pend, 0, bits_bytes, s));
+    CUDA_CHECK(cudaMemsetAsync(G.blocker, 0xff, (size_t)nsim * 4, s));
+    CUDA_CHECK(cudaMemsetAsync(G.done, 0, (size_t)nsim, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     res.ms_h2d = ms_since(t1);
     cudaEvent_t e0, e1;
@@ -695,33 +724,47 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     CUDA_CHECK(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
     CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
     launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
-    for (size_t b = 0; b + 1 < sch.batches.size(); ++b) {
-        const long long a = sch.batches[b], e = sch.batches[b + 1];
-        if (e > a) launch_sgs(J, g.dp, d_nodes + a, d_xp + a, (int)(e - a), s);
+    launch_sgs_ranks(J, G, nsim, s);
+    long long round = 0;
+    if (nsim > 0) {
+        // every round commits at least the pending node of lowest rank
+        launch_sgs_admit(J, g.dp, G, 1, s);
+        int chunk = 4;
+        for (;;) {
+            for (int c = 0; c < chunk; ++c, ++round) launch_sgs_round(J, g.dp, G, (int)(round & 1), s);
+            CUDA_CHECK(cudaGetLastError());
+            CUDA_CHECK(cudaMemcpyAsync(&hc, G.ctl, sizeof(hc), cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaStreamSynchronize(s));
+            if (hc.next >= hc.total && hc.count[round & 1] == 0) break;
+            if (round > nsim + 64) throw HpglError{HPGL_E_INTERNAL, "sequential simulation made no progress"};
+            chunk = std::min(chunk * 2, 64);
+        }
     }
-    CUDA_CHECK(cudaGetLastError());
     CUDA_CHECK(cudaEventRecord(e1, s));
-    Counters hc;
-    CUDA_CHECK(cudaMemcpyAsync(&hc, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    Counters hcnt;
+    CUDA_CHECK(cudaMemcpyAsync(&hcnt, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     res.ms_device = ms;
-    if (hc.err)
-        throw HpglError{HPGL_E_INTERNAL, "device invariant violated (error bits " + std::to_string(hc.err) + ")"};
+    if (hcnt.err)
+        throw HpglError{HPGL_E_INTERNAL, "device invariant violated (error bits " + std::to_string(hcnt.err) + ")"};
+    if (nsim > 0 && hc.commits != nsim)
+        throw HpglError{HPGL_E_INTERNAL, "sequential simulation committed " + std::to_string(hc.commits) + " of " +
+                                             std::to_string(nsim) + " nodes"};
     auto t2 = std::chrono::steady_clock::now();
     const size_t n = (size_t)S.size;
     CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, S.ar.o_values), n * 4, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaMemcpyAsync(res.out_mask, at<uint8_t>(S, S.ar.o_mask), n, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     res.ms_d2h = ms_since(t2);
-    res.systems = (long long)nsim;
-    res.systems_fp64 = (long long)nsim;
+    res.systems = hc.tries;
+    res.systems_fp64 = hc.tries;
     res.failures = 0;
     res.ms_total = ms_since(t0);
-    S.sgs_batches = (long long)sch.batches.size() - 1;
+    res.rounds = hc.rounds;
 }
 
 static const char *top_kernel_name(int nmax, int precision, int schedule) {

@@ -39,5 +39,7 @@ void server_destroy(void *h);
 
 int default_precision();
 void set_default_precision(int p);
+// Window of the speculative simulation rounds (pending nodes per round).
+void set_sim_window(int window);
 
 }  // namespace hpgl_b200

@@ -4,6 +4,7 @@
 //   k_search_template  bit-sliced walk of the sorted search template
 //   k_search_cluster   clusterizer gather, covariance filter, reference sort
 //   k_ik_argmax        most probable category
+//   k_sgs_*            bookkeeping of the speculative simulation rounds
 // Paths cited are relative to the reference's src/geo_bsd/hpgl/.
 #include <algorithm>
 #include <climits>
@@ -308,9 +309,123 @@ void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *n
     else launch_solve64_mixed(J, P, s, blocks_per_sm);
 }
 
-void launch_sgs(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s) {
-    if (P.nmax <= 32) launch_sgs32(J, P, nodes, xp, count, s);
-    else launch_sgs64(J, P, nodes, xp, count, s);
+// ---------------------------------------------------------------------------
+// Speculative sequential simulation: path ranks, commits and admissions (the
+// rounds' kriging is k_sgs_try32 / k_sgs_try64).
+
+__global__ void k_sgs_rank_init(DevJob J, int *rank_of) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < J.size) rank_of[i] = J.mask[i] ? -1 : INT_MAX;
+}
+
+__global__ void k_sgs_rank_path(const int *nodes, int *rank_of, long long nsim) {
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r < nsim) rank_of[nodes[r]] = (int)r;
+}
+
+__device__ __forceinline__ void sgs_bit(const DevJob &J, const DevPlan &P, int node, long long &w, uint32_t &bit) {
+    int x, y, z;
+    node_xyz(J, node, x, y, z);
+    const int px = x + P.px;
+    w = ((long long)z * J.ny + y) * P.wpr + (px >> 5);
+    bit = 1u << (px & 31);
+}
+
+// Commits the nodes of window buffer `cur` that the round kept (informed bit
+// set, pending bit cleared, done) and moves the others to the other buffer
+// (one counter update per warp).  The last block to finish (a ticket
+// counter, no waiting) tops the window up to its size and records the
+// admission that k_sgs_admit carries out.
+__global__ void __launch_bounds__(256) k_sgs_commit(DevJob J, DevPlan P, SgsState G, int cur) {
+    SgsCtl *ctl = G.ctl;
+    const int count = *(volatile int *)&ctl->count[cur];
+    const int *win = cur ? G.win1 : G.win0;
+    int *nxt = cur ? G.win0 : G.win1;
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += stride) {
+        const int i = base + lane;
+        int rank = -1;
+        bool keep = false;
+        if (i < count) {
+            rank = win[i];
+            if (G.ok[i]) {
+                long long w;
+                uint32_t bit;
+                sgs_bit(J, P, G.nodes[rank], w, bit);
+                atomicOr(J.sim_bits + w, bit);
+                atomicAnd(G.pend + w, ~bit);
+                G.done[rank] = 1;
+            } else {
+                keep = true;
+            }
+        }
+        const unsigned km = __ballot_sync(FULL_MASK, keep);
+        int slot0 = 0;
+        if (lane == 0 && km) slot0 = atomicAdd(&ctl->count[cur ^ 1], __popc(km));
+        slot0 = __shfl_sync(FULL_MASK, slot0, 0);
+        if (keep) nxt[slot0 + __popc(km & ((1u << lane) - 1u))] = rank;
+    }
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&ctl->blocks_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    const int kept = atomicAdd(&ctl->count[cur ^ 1], 0);
+    long long add = (long long)ctl->window - kept;
+    if (add < 0) add = 0;
+    if (add > ctl->total - ctl->next) add = ctl->total - ctl->next;
+    ctl->admit_base = kept;
+    ctl->admit = add;
+    ctl->next += add;
+    ctl->count[cur ^ 1] = kept + (int)add;
+    ctl->count[cur] = 0;
+    if (count > 0) {
+        ctl->rounds += 1;
+        ctl->commits += count - kept;
+    }
+    ctl->blocks_done = 0;
+}
+
+// Appends the admitted path ranks to window buffer `buf` and marks them
+// pending.
+__global__ void __launch_bounds__(256) k_sgs_admit(DevJob J, DevPlan P, SgsState G, int buf) {
+    const SgsCtl *ctl = G.ctl;
+    const long long add = ctl->admit, base = ctl->admit_base, first = ctl->next - add;
+    int *win = buf ? G.win1 : G.win0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < add;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int rank = (int)(first + k);
+        win[base + k] = rank;
+        long long w;
+        uint32_t bit;
+        sgs_bit(J, P, G.nodes[rank], w, bit);
+        atomicOr(G.pend + w, bit);
+    }
+}
+
+void launch_sgs_ranks(const DevJob &J, const SgsState &G, long long nsim, cudaStream_t s) {
+    int *rank_of = const_cast<int *>(G.rank_of);
+    k_sgs_rank_init<<<(unsigned)((J.size + 255) / 256), 256, 0, s>>>(J, rank_of);
+    if (nsim > 0) k_sgs_rank_path<<<(unsigned)((nsim + 255) / 256), 256, 0, s>>>(G.nodes, rank_of, nsim);
+}
+
+static void sgs_commit_admit(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
+    const unsigned blocks = (unsigned)sm_count() * 4;
+    k_sgs_commit<<<blocks, 256, 0, s>>>(J, P, G, cur);
+    k_sgs_admit<<<blocks, 256, 0, s>>>(J, P, G, cur ^ 1);
+}
+
+void launch_sgs_admit(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
+    sgs_commit_admit(J, P, G, cur, s);
+}
+
+void launch_sgs_round(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
+    if (P.nmax <= 32) launch_sgs_try32(J, P, G, cur, s);
+    else launch_sgs_try64(J, P, G, cur, s);
+    sgs_commit_admit(J, P, G, cur, s);
 }
 
 long long persistent_grid(const void *fn, int threads, size_t smem, int blocks_per_sm, long long units) {

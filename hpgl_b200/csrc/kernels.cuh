@@ -150,11 +150,44 @@ void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *n
 void launch_ik_argmax(const DevJob &J, cudaStream_t s);
 // cokriging.cu: colocated simple cokriging of every node (after the template search)
 void launch_cokriging(const DevJob &J, const DevPlan &P, cudaStream_t s);
-// One batch of sequential simulation: nodes[i] (none inside another's search
-// box) kriged from the current informed set and set from the quantile xp[i].
-void launch_sgs(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s);
-void launch_sgs32(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s);
-void launch_sgs64(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s);
+// Sequential simulation in speculative rounds.  The path's nodes enter, in
+// path order, a window of pending nodes.  Each round krigs pending nodes
+// from the committed nodes of lower path rank (informed bits, rank_of); a
+// node commits unless the part of its search template that the search read
+// holds a pending node of lower rank -- a committed node has then seen
+// exactly the nodes the sequential order gives it, so the result is the
+// sequential one.  A node that did not commit records that pending node
+// (its blocker) and is not tried again before the blocker commits.  The
+// pending node of lowest rank always commits, so every round makes progress.
+struct SgsCtl {
+    int count[2];           // pending nodes in window buffer 0 / 1
+    int window;             // window size (pending nodes per round)
+    unsigned blocks_done;   // commit kernel: blocks finished
+    long long next;         // next path rank to admit
+    long long total;        // path length
+    long long admit_base;   // window slot of the first admitted node
+    long long admit;        // nodes admitted by the pending admission
+    long long rounds, tries, commits;
+};
+struct SgsState {
+    SgsCtl *ctl;
+    const int *nodes;       // path order
+    const double *xp;       // per path rank: the draw's standard normal quantile
+    const int *rank_of;     // per node: -1 informed, path rank, or INT_MAX
+    uint32_t *pend;         // pending bits, laid out like the informed bits
+    int *blocker;           // per path rank: the pending rank that blocked it, or -1
+    uint8_t *done;          // per path rank: committed
+    int *win0, *win1;       // window buffers (path ranks)
+    uint8_t *ok;            // per window slot: the node committed this round
+};
+// rank_of from the mask and the path
+void launch_sgs_ranks(const DevJob &J, const SgsState &G, long long nsim, cudaStream_t s);
+// one round: try the pending nodes of window buffer `cur`, commit, admit
+void launch_sgs_round(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
+void launch_sgs_try32(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
+void launch_sgs_try64(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
+// the first admission (window buffer 0 from an empty buffer 1)
+void launch_sgs_admit(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm);

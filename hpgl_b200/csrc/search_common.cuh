@@ -104,12 +104,80 @@ __device__ __forceinline__ void template_node(const DevJob &J, const DevPlan &P,
     if (lane == 0) J.nbcount[node] = min(cnt, nmax);
 }
 
+// neighbour_lookup_t::find for one node of a speculative simulation round
+// (path rank `rank`): as template_node, over the committed nodes of lower
+// rank (informed bit set and rank_of below `rank`; informed data have rank
+// -1).  Returns -1 when the search completed, else the rank of the first
+// pending node of lower rank met before the point where the search would
+// stop: in the sequential order that node would have been simulated and
+// seen, so nothing of this search is kept.  The bits and ranks are read-only
+// while a round's nodes are tried.
+__device__ __forceinline__ int template_node_spec(const DevJob &J, const DevPlan &P, const SgsState &G, int node,
+                                                  int rank, int lane) {
+    int x, y, z;
+    node_xyz(J, node, x, y, z);
+    const int nmax = P.nmax;
+    int *out = J.nb + (long long)node * nmax;
+    int cnt = 0;
+    for (int tb = 0; tb < P.tmpl_len && cnt < nmax; tb += 32) {
+        const int t = tb + lane;
+        bool hit = false, conflict = false;
+        int delta = 0, r = -1;
+        if (t < P.tmpl_len) {
+            const int4 e = __ldg(&P.tmpl[t]);
+            delta = e.w;
+            const int yy = y + e.y, zz = z + e.z;
+            if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
+                const int px = x + e.x;  // padded x of the target cell
+                const long long w = ((long long)zz * J.ny + yy) * P.wpr + (px >> 5);
+                const uint32_t bit = 1u << (px & 31);
+                const bool inf = (__ldg(J.bits + w) & bit) != 0;
+                const bool pen = (__ldg(G.pend + w) & bit) != 0;
+                if (inf || pen) {  // set bits only inside the grid
+                    r = __ldg(G.rank_of + node + delta);
+                    hit = inf && r < rank;
+                    conflict = pen && r < rank;
+                }
+            }
+        }
+        const unsigned b = __ballot_sync(FULL_MASK, hit);
+        const unsigned c = __ballot_sync(FULL_MASK, conflict);
+        if (c) {
+            const int first = __ffs(c) - 1;
+            const int blocker = __shfl_sync(FULL_MASK, r, first);
+            if (cnt + __popc(b & ((1u << first) - 1u)) < nmax) return blocker;
+        }
+        const int pos = __popc(b & ((1u << lane) - 1u));
+        if (hit && cnt + pos < nmax) out[cnt + pos] = node + delta;
+        cnt += __popc(b);
+    }
+    if (lane == 0) J.nbcount[node] = min(cnt, nmax);
+    return -1;
+}
+
+// The pending entries of a round, 32 per warp: lane l holds entry base + l;
+// entries whose blocker has not committed are left alone.  Returns the mask
+// of lanes whose node is tried this round; the others' ok flags are cleared.
+__device__ __forceinline__ unsigned sgs_lanes_to_try(const SgsState &G, const int *win, int count, int base,
+                                                     int lane, int &rank) {
+    const int i = base + lane;
+    bool tr = false;
+    rank = -1;
+    if (i < count) {
+        rank = win[i];
+        const int b = G.blocker[rank];
+        tr = b < 0 || G.done[b];
+        if (!tr) G.ok[i] = 0;
+    }
+    return __ballot_sync(FULL_MASK, tr);
+}
+
 // The simulated value of a kriged node (sequential_simulation.h:106-110,
 // gaussian_cdf_t::inverse in gaussian_distribution.h:49-66): xp, the
 // standard normal quantile of the node's draw, times sqrt(variance) plus the
 // kriged estimate; N(0, 1) when the kriging failed.  The node joins the
-// informed set.
-__device__ __forceinline__ void sgs_set(const DevJob &J, const DevPlan &P, int node, double xp) {
+// informed set when its round commits.
+__device__ __forceinline__ void sgs_value(const DevJob &J, int node, double xp) {
     double v;
     if (J.status[node] == ST_SUCCESS)
         v = __dadd_rn(__dmul_rn(xp, __dsqrt_rn(J.variance[node])), (double)J.out_values[node]);
@@ -117,10 +185,6 @@ __device__ __forceinline__ void sgs_set(const DevJob &J, const DevPlan &P, int n
         v = __dadd_rn(__dmul_rn(xp, 1.0), 0.0);
     J.sim_values[node] = __double2float_rn(v);
     J.sim_mask[node] = 1;
-    int x, y, z;
-    node_xyz(J, node, x, y, z);
-    const int px = x + P.px;
-    atomicOr(J.sim_bits + ((long long)z * J.ny + y) * P.wpr + (px >> 5), 1u << (px & 31));
 }
 
 }  // namespace hpgl_b200

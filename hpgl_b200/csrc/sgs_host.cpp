@@ -1,4 +1,4 @@
-// Host schedule of sequential Gaussian simulation.
+// Host side of sequential simulation.
 //
 // Path (path_random_generator.cpp:20-66): a linear congruential walk x ->
 // (A x + C) mod size from x0 = seed mod size, A = 1 + the product of the
@@ -8,21 +8,26 @@
 // checkout lacks; init_rnd's asserts leave one reading of that table (every
 // prime in increasing order past the grid size), restated here with a sieve.
 //
-// Draws (bs_random_generator.cpp, sample.h:14-17): boost::mt11213b seeded
-// with the seed, one 32-bit output per simulated node divided by 2^32 - 1,
-// turned into the standard normal quantile of Odeh and Evans's rational
-// approximation (gaussian_distribution.h:49-66) with the C library's log and
-// sqrt -- the GPU multiplies it by the kriging standard deviation and adds the
-// kriged mean, as gaussian_cdf_t::inverse does.
+// Draws (bs_random_generator.cpp, sample.h:14-17, sample.cpp:8-21):
+// boost::mt11213b seeded with the seed, one 32-bit output per simulated node
+// divided by 2^32 - 1.  Gaussian simulation turns it into the standard
+// normal quantile of Odeh and Evans's rational approximation
+// (gaussian_distribution.h:49-66) with the C library's log and sqrt -- the GPU
+// multiplies it by the kriging standard deviation and adds the kriged mean,
+// as gaussian_cdf_t::inverse does; indicator simulation compares it with the
+// cumulative category probabilities.
 //
-// Batches: the nodes of one batch are outside each other's search boxes, so
-// none can be a neighbour of another and simulating them at once gives the
-// sequential result.  A grid of cells of the box's size holds the current
-// batch's nodes; a node is checked against the 27 cells around its own.
+// Normal-score transforms (sequential_gaussian_simulation.cpp:32-35, 72-73,
+// 97-103, 119-123): the caller's CDF interpolated in float
+// (non_parametric_cdf.h:185-260) and the standard normal CDF of Abramowitz and
+// Stegun 26.2.17 (gaussian_distribution.h:22-47).  They run here, over the
+// host threads, because the C library's log and exp define their bits.
 #include "sgs_host.h"
 
+#include <algorithm>
 #include <cmath>
 #include <stdexcept>
+#include <thread>
 
 namespace hpgl_b200 {
 
@@ -103,12 +108,68 @@ double quantile(double p) {
 
 }  // namespace
 
-void sgs_schedule(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed,
-                  const int radii[3], long long max_batch, SgsSchedule &out) {
+namespace {
+
+template <typename F>
+void parallel_for(long long n, int threads, F f) {
+    const long long chunk = 1 << 16;
+    const int t = (int)std::max<long long>(1, std::min<long long>(threads, (n + chunk - 1) / chunk));
+    if (t <= 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const long long per = (n + t - 1) / t;
+    for (int k = 0; k < t; ++k) {
+        const long long a = k * per, b = std::min(n, a + per);
+        if (a < b) pool.emplace_back([=] { f(a, b); });
+    }
+    for (auto &th : pool) th.join();
+}
+
+// non_parametric_cdf_2_t::operator() (non_parametric_cdf.h:202-228): float
+// interpolation between the bracketing values.
+float npcdf_prob(const NonParametricCdf &c, float value) {
+    const float *it = std::lower_bound(c.values, c.values + c.size, value);
+    if (it == c.values + c.size) return c.probs[c.size - 1];
+    if (it == c.values) return c.probs[0];
+    const long long i2 = it - c.values, i1 = i2 - 1;
+    const float x1 = c.values[i1], x2 = c.values[i2], y1 = c.probs[i1], y2 = c.probs[i2];
+    return y1 + (y2 - y1) / (x2 - x1) * (value - x1);
+}
+
+// non_parametric_cdf_2_t::inverse (non_parametric_cdf.h:230-257).
+float npcdf_inverse(const NonParametricCdf &c, float prob) {
+    if (c.size <= 0) return 0;
+    const float *it = std::lower_bound(c.probs, c.probs + c.size, prob);
+    if (it == c.probs) return c.values[0];
+    if (it == c.probs + c.size) return c.values[c.size - 1];
+    const long long i2 = it - c.probs, i1 = i2 - 1;
+    const float x1 = c.values[i1], x2 = c.values[i2], y1 = c.probs[i1], y2 = c.probs[i2];
+    return x1 + (x2 - x1) / (y2 - y1) * (prob - y1);
+}
+
+// gaussian_cdf_t::operator() with mean 0 and variance 1
+// (gaussian_distribution.h:22-41).
+double gaussian_prob(double x) {
+    const double p = 0.2316419;
+    const double b[] = {0.319381530, -0.356563782, 1.781477937, -1.821255978, 1.330274429};
+    double sx = (x - 0.0) / std::sqrt(1.0);
+    const bool neg = sx < 0;
+    if (neg) sx = -sx;
+    const double t = 1 / (1 + p * sx);
+    const double zx = 1 / std::sqrt(2 * 3.14159265358) * std::exp(-sx * sx / 2);
+    double result = 1 - zx * ((((b[4] * t + b[3]) * t + b[2]) * t + b[1]) * t + b[0]) * t;
+    if (neg) result = 1 - result;
+    return result;
+}
+
+}  // namespace
+
+void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out) {
     const long long size = (long long)nx * ny * nz;
     out.nodes.clear();
-    out.xp.clear();
-    out.batches.clear();
+    out.u.clear();
     if (size <= 0) return;
     if (size > 10000000LL)
         throw std::domain_error("the simulation path is defined for grids of at most 10^7 nodes");
@@ -120,50 +181,36 @@ void sgs_schedule(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *si
         out.nodes.push_back((int)node);
     }
     Mt11213b gen((uint32_t)seed);
-    out.xp.resize(out.nodes.size());
-    for (size_t k = 0; k < out.nodes.size(); ++k) out.xp[k] = quantile(double(gen.next()) / double(0xffffffffu));
-    // batches
-    const int bx = radii[0] + 1, by = radii[1] + 1, bz = radii[2] + 1;
-    const int cx = nx / bx + 1, cy = ny / by + 1, cz = nz / bz + 1;
-    std::vector<long long> stamp((size_t)cx * cy * cz, -1);
-    std::vector<std::vector<int>> cell((size_t)cx * cy * cz);
-    long long batch = 0, in_batch = 0;
-    out.batches.push_back(0);
-    for (size_t k = 0; k < out.nodes.size(); ++k) {
-        const int nd = out.nodes[k];
-        const int x = nd % nx, y = nd / nx % ny, z = nd / nx / ny;
-        const int gx = x / bx, gy = y / by, gz = z / bz;
-        bool conflict = in_batch >= max_batch;
-        for (int dz = -1; dz <= 1 && !conflict; ++dz)
-            for (int dy = -1; dy <= 1 && !conflict; ++dy)
-                for (int dx = -1; dx <= 1 && !conflict; ++dx) {
-                    const int ax = gx + dx, ay = gy + dy, az = gz + dz;
-                    if (ax < 0 || ay < 0 || az < 0 || ax >= cx || ay >= cy || az >= cz) continue;
-                    const size_t c = ((size_t)az * cy + ay) * cx + ax;
-                    if (stamp[c] != batch) continue;
-                    for (int o : cell[c]) {
-                        const int ox = o % nx, oy = o / nx % ny, oz = o / nx / ny;
-                        if (std::abs(ox - x) <= radii[0] && std::abs(oy - y) <= radii[1] &&
-                            std::abs(oz - z) <= radii[2]) {
-                            conflict = true;
-                            break;
-                        }
-                    }
-                }
-        if (conflict) {
-            ++batch;
-            in_batch = 0;
-            out.batches.push_back((long long)k);
+    out.u.resize(out.nodes.size());
+    for (size_t k = 0; k < out.nodes.size(); ++k) out.u[k] = double(gen.next()) / double(0xffffffffu);
+}
+
+void gaussian_quantiles(const std::vector<double> &u, std::vector<double> &xp, int threads) {
+    xp.resize(u.size());
+    parallel_for((long long)u.size(), threads, [&](long long a, long long b) {
+        for (long long k = a; k < b; ++k) xp[(size_t)k] = quantile(u[(size_t)k]);
+    });
+}
+
+void cdf_to_gaussian(const NonParametricCdf &cdf, const float *in, float *out, const uint8_t *mask, long long n,
+                     int threads) {
+    parallel_for(n, threads, [&](long long a, long long b) {
+        for (long long i = a; i < b; ++i) {
+            if (mask && !mask[i]) continue;
+            const double P = npcdf_prob(cdf, in[i]);
+            out[i] = (float)(quantile(P) * std::sqrt(1.0) + 0.0);
         }
-        const size_t c = ((size_t)gz * cy + gy) * cx + gx;
-        if (stamp[c] != batch) {
-            stamp[c] = batch;
-            cell[c].clear();
+    });
+}
+
+void gaussian_to_cdf(const NonParametricCdf &cdf, float *values, const uint8_t *mask, long long n, int threads) {
+    parallel_for(n, threads, [&](long long a, long long b) {
+        for (long long i = a; i < b; ++i) {
+            if (!mask[i]) continue;
+            const double P = gaussian_prob(values[i]);
+            values[i] = npcdf_inverse(cdf, (float)P);
         }
-        cell[c].push_back(nd);
-        ++in_batch;
-    }
-    out.batches.push_back((long long)out.nodes.size());
+    });
 }
 
 }  // namespace hpgl_b200

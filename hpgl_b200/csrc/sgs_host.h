@@ -1,23 +1,40 @@
-// Host schedule of sequential Gaussian simulation (sgs_host.cpp): the
-// reference's random path over the grid, its random draws, and the batches
-// of path-consecutive nodes that the GPU can simulate at once.
+// Host side of sequential simulation (sgs_host.cpp): the reference's random
+// path over the grid, its random draws, and the normal-score transforms of
+// sequential Gaussian simulation.
 #pragma once
 #include <cstdint>
 #include <vector>
 
 namespace hpgl_b200 {
 
-struct SgsSchedule {
-    std::vector<int> nodes;         // simulated nodes in path order
-    std::vector<double> xp;         // standard normal quantile of each node's draw
-    std::vector<long long> batches; // batch b = nodes[batches[b], batches[b+1])
+struct SimPath {
+    std::vector<int> nodes;  // simulated nodes in path order
+    std::vector<double> u;   // the draw of each simulated node, in [0, 1]
 };
 
-// nodes: the path's uninformed nodes inside `sim_mask` (all when null);
-// batches: maximal runs in which no node lies inside another's search box
-// (|dx| <= rx, |dy| <= ry, |dz| <= rz), so that each node sees exactly the
-// nodes simulated before it on the path, at most `max_batch` nodes.
-void sgs_schedule(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed,
-                  const int radii[3], long long max_batch, SgsSchedule &out);
+// The path's uninformed nodes inside `sim_mask` (all when null: a node is
+// simulated when sim_mask[node] == 1) in path order, with the generator's
+// draws in the same order.  Throws std::domain_error above 10^7 nodes.
+void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out);
+
+// xp[k] = the standard normal quantile of u[k] (gaussian_cdf_t::inverse).
+void gaussian_quantiles(const std::vector<double> &u, std::vector<double> &xp, int threads);
+
+// A caller's non-parametric CDF (hpgl_non_parametric_cdf_t): `size` values in
+// increasing order and their cumulative probabilities.
+struct NonParametricCdf {
+    const float *values;
+    const float *probs;
+    long long size;
+};
+
+// Normal-score transform (cdf_utils.h:12-25 with non_parametric_cdf_2_t as
+// the source and the standard normal as the target): out[i] =
+// N^-1(F(in[i])) for the nodes with mask[i] != 0 (every node when mask is
+// null); out may be in.
+void cdf_to_gaussian(const NonParametricCdf &cdf, const float *in, float *out, const uint8_t *mask, long long n,
+                     int threads);
+// The back transform: values[i] = F^-1(N(values[i])) where mask[i] != 0.
+void gaussian_to_cdf(const NonParametricCdf &cdf, float *values, const uint8_t *mask, long long n, int threads);
 
 }  // namespace hpgl_b200

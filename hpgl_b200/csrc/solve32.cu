@@ -618,31 +618,46 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_fused32(DevJob J, DevPlan P) {
 
 constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
 
-// A batch of sequential simulation (nodes of at most 32 neighbours): one warp
-// per node: template search, the exact FP64 system, the simulated value.
-__global__ void __launch_bounds__(WARPS32 * 32) k_sgs32(DevJob J, DevPlan P, const int *nodes, const double *xp,
-                                                        int count) {
+// One speculative round of sequential simulation (at most 32 neighbours):
+// one warp per pending node of window buffer `cur`: the template search with
+// conflict detection, the exact FP64 system and the simulated value.
+__global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P, SgsState G, int cur) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
-    for (int i = blockIdx.x * WARPS32 + warp; i < count; i += gridDim.x * WARPS32) {
-        const int node = nodes[i];
-        template_node(J, P, node, lane);
-        __syncwarp();
-        const NodeFetch f = fetch_node(J, P, node, lane);
-        exact32_node(J, P, S, f, lane);
-        __syncwarp();
-        if (lane == 0) sgs_set(J, P, node, xp[i]);
-        __syncwarp();
+    const int count = G.ctl->count[cur];
+    const int *win = cur ? G.win1 : G.win0;
+    for (int base = (blockIdx.x * WARPS32 + warp) * 32; base < count; base += gridDim.x * WARPS32 * 32) {
+        int my_rank;
+        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
+        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
+            const int node = G.nodes[rank];
+            const int blocker = template_node_spec(J, P, G, node, rank, lane);
+            __syncwarp();
+            if (blocker < 0) {
+                const NodeFetch f = fetch_node(J, P, node, lane);
+                exact32_node(J, P, S, f, lane);
+                __syncwarp();
+                if (lane == 0) sgs_value(J, node, G.xp[rank]);
+            }
+            if (lane == 0) {
+                G.ok[base + l] = blocker < 0;
+                if (blocker >= 0) G.blocker[rank] = blocker;
+            }
+            __syncwarp();
+        }
     }
 }
 
 }  // namespace
 
-void launch_sgs32(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s) {
-    if (count <= 0) return;
-    const long long g = persistent_grid((const void *)k_sgs32, WARPS32 * 32, SMEM32, 0, (count + WARPS32 - 1) / WARPS32);
-    k_sgs32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, P, nodes, xp, count);
+void launch_sgs_try32(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
+    const long long g = persistent_grid((const void *)k_sgs_try32, WARPS32 * 32, SMEM32, 0, 1LL << 30);
+    k_sgs_try32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, P, G, cur);
 }
 
 void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm) {

@@ -429,24 +429,40 @@ __device__ __forceinline__ bool exact64_node(const DevJob &J, const DevPlan &P, 
     return true;
 }
 
-// A batch of sequential simulation (33-64 neighbours): one warp per node.
-__global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs64(DevJob J, DevPlan P, const int *nodes, const double *xp,
-                                                              int count) {
+// One speculative round of sequential simulation (33-64 neighbours): one
+// warp per pending node of window buffer `cur`.
+__global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs_try64(DevJob J, DevPlan P, SgsState G, int cur) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ int s_cs[N64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Exact64Smem &S = reinterpret_cast<Exact64Smem *>(dyn_smem)[warp];
-    for (int i = blockIdx.x * WARPS64_BLOCK + warp; i < count; i += gridDim.x * WARPS64_BLOCK) {
-        const int node = nodes[i];
-        template_node(J, P, node, lane);
-        __syncwarp();
-        const NodeFetch f = fetch_node(J, P, node, lane);
-        exact64_node(J, P, S, s_cs, f, lane);
-        __syncwarp();
-        if (lane == 0) sgs_set(J, P, node, xp[i]);
-        __syncwarp();
+    const int count = G.ctl->count[cur];
+    const int *win = cur ? G.win1 : G.win0;
+    for (int base = (blockIdx.x * WARPS64_BLOCK + warp) * 32; base < count; base += gridDim.x * WARPS64_BLOCK * 32) {
+        int my_rank;
+        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
+        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
+            const int node = G.nodes[rank];
+            const int blocker = template_node_spec(J, P, G, node, rank, lane);
+            __syncwarp();
+            if (blocker < 0) {
+                const NodeFetch f = fetch_node(J, P, node, lane);
+                exact64_node(J, P, S, s_cs, f, lane);
+                __syncwarp();
+                if (lane == 0) sgs_value(J, node, G.xp[rank]);
+            }
+            if (lane == 0) {
+                G.ok[base + l] = blocker < 0;
+                if (blocker >= 0) G.blocker[rank] = blocker;
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -783,11 +799,9 @@ void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_lis
     k_solve_exact64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, node_list, n_list);
 }
 
-void launch_sgs64(const DevJob &J, const DevPlan &P, const int *nodes, const double *xp, int count, cudaStream_t s) {
-    if (count <= 0) return;
-    const long long g = persistent_grid((const void *)k_sgs64, WARPS64_BLOCK * 32, SMEM64_EXACT, 0,
-                                        (count + WARPS64_BLOCK - 1) / WARPS64_BLOCK);
-    k_sgs64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, nodes, xp, count);
+void launch_sgs_try64(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
+    const long long g = persistent_grid((const void *)k_sgs_try64, WARPS64_BLOCK * 32, SMEM64_EXACT, 0, 1LL << 30);
+    k_sgs_try64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, G, cur);
 }
 
 void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s, int blocks_per_sm) {

@@ -1,4 +1,6 @@
-"""Python-3 drop-in for the kriging entry points of the reference's
-``geo_bsd`` package (geo_bsd/geo.py), running on the B200 library."""
+"""Python-3 drop-in for the entry points of the reference's ``geo_bsd``
+package (geo_bsd/geo.py, sgs.py, cdf.py), running on the B200 library."""
 
+from .cdf import *  # noqa: F401,F403
 from .geo import *  # noqa: F401,F403
+from .sgs import *  # noqa: F401,F403

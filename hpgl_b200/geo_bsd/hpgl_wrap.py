@@ -1,7 +1,7 @@
 """ctypes layer of the kriging entry points: the C structs of the library's
 ABI (include/hpgl.h, same layouts as the reference's api.h:18-153) and the
 argument/return types of each call, following the reference's
-geo_bsd/hpgl_wrap.py:18-311 for the kriging path.  Loads hpgl_b200/hpgl.so;
+geo_bsd/hpgl_wrap.py:18-311.  Loads hpgl_b200/hpgl.so;
 there is no fallback when it is missing."""
 
 import ctypes as C
@@ -27,6 +27,19 @@ class _HPGL_IND_MASKED_ARRAY(C.Structure):
                 ("indicator_count", C.c_int)]
 
 
+class _HPGL_KRIGING_KIND:
+    ordinary = 0
+    simple = 1
+
+
+class _HPGL_UBYTE_ARRAY(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("shape", _HPGL_SHAPE)]
+
+
+class _HPGL_FLOAT_ARRAY(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_float)), ("shape", _HPGL_SHAPE)]
+
+
 _KRIGING_FIELDS = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
                    ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3),
                    ("max_neighbours", C.c_int)]
@@ -46,6 +59,14 @@ class _HPGL_MEDIAN_IK_PARAMS(C.Structure):
 
 class _HPGL_IK_PARAMS(C.Structure):
     _fields_ = _KRIGING_FIELDS + [("marginal_prob", C.c_double)]
+
+
+class _HPGL_SGS_PARAMS(C.Structure):
+    _fields_ = _KRIGING_FIELDS + [("kriging_kind", C.c_int), ("seed", C.c_long), ("min_neighbours", C.c_int)]
+
+
+class hpgl_non_parametric_cdf_t(C.Structure):
+    _fields_ = [("values", C.POINTER(C.c_float)), ("probs", C.POINTER(C.c_float)), ("size", C.c_longlong)]
 
 
 class _HPGL_COV_PARAMS(C.Structure):
@@ -118,6 +139,22 @@ _hpgl_so.hpgl_simple_cokriging_mark2.restype = None
 _hpgl_so.hpgl_simple_cokriging_mark2.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_CONT_MASKED_ARRAY),
                                                  C.POINTER(_HPGL_COKRIGING_M2_PARAMS),
                                                  C.POINTER(_HPGL_CONT_MASKED_ARRAY)]
+
+_hpgl_so.hpgl_sgs_simulation.restype = None
+_hpgl_so.hpgl_sgs_simulation.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_SGS_PARAMS),
+                                         C.POINTER(hpgl_non_parametric_cdf_t), C.POINTER(C.c_double),
+                                         C.POINTER(_HPGL_UBYTE_ARRAY)]
+_hpgl_so.hpgl_sgs_lvm_simulation.restype = None
+_hpgl_so.hpgl_sgs_lvm_simulation.argtypes = [C.POINTER(_HPGL_CONT_MASKED_ARRAY), C.POINTER(_HPGL_SGS_PARAMS),
+                                             C.POINTER(hpgl_non_parametric_cdf_t), C.POINTER(_HPGL_FLOAT_ARRAY),
+                                             C.POINTER(_HPGL_UBYTE_ARRAY)]
+_hpgl_so.hpgl_sis_simulation.restype = None
+_hpgl_so.hpgl_sis_simulation.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.POINTER(_HPGL_IK_PARAMS), C.c_int,
+                                         C.c_int, C.POINTER(_HPGL_UBYTE_ARRAY)]
+_hpgl_so.hpgl_sis_simulation_lvm.restype = None
+_hpgl_so.hpgl_sis_simulation_lvm.argtypes = [C.POINTER(_HPGL_IND_MASKED_ARRAY), C.POINTER(_HPGL_IK_PARAMS),
+                                             C.POINTER(_HPGL_FLOAT_ARRAY), C.c_int, C.c_int,
+                                             C.POINTER(_HPGL_UBYTE_ARRAY), C.c_int]
 
 _hpgl_so.hpgl_read_inc_file_float.restype = None
 _hpgl_so.hpgl_read_inc_file_float.argtypes = [C.c_char_p, C.c_float, C.c_int, NC.ndpointer(dtype=numpy.float32, flags=_F),

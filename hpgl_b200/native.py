@@ -58,7 +58,7 @@ class Result(C.Structure):
                 ("probs", C.POINTER(C.c_float)), ("nb_stride", C.c_int),
                 ("systems", C.c_longlong), ("systems_fp64", C.c_longlong), ("failures", C.c_longlong),
                 ("ms_plan", C.c_double), ("ms_h2d", C.c_double), ("ms_device", C.c_double),
-                ("ms_d2h", C.c_double), ("ms_total", C.c_double)]
+                ("ms_d2h", C.c_double), ("ms_total", C.c_double), ("rounds", C.c_longlong)]
 
 
 class Bench(C.Structure):
@@ -208,7 +208,7 @@ class _Prepared:
         out["out"] = self.out
         out["out_mask"] = self.out_mask
         out["cap"] = self.cap
-        for k in ("systems", "systems_fp64", "ms_plan", "ms_h2d", "ms_device", "ms_d2h", "ms_total"):
+        for k in ("systems", "systems_fp64", "ms_plan", "ms_h2d", "ms_device", "ms_d2h", "ms_total", "rounds"):
             out[k] = getattr(r, k)
         return out
 

@@ -266,6 +266,14 @@ int hpgl_get_last_error(void);
 void hpgl_b200_set_precision(int precision);
 int hpgl_b200_get_precision(void);
 
+/* Sequential simulation runs in speculative rounds: the pending nodes of a
+   window of the random path are kriged at once, and a node commits when no
+   pending node of lower path rank lies in the part of its search template
+   that the search read, so the result is the sequential one.  `window` is
+   the number of pending nodes (0: the default 2^18); results do not depend
+   on it. */
+void hpgl_b200_set_sim_window(int window);
+
 /* Kriging kinds of hpgl_b200_job_t. */
 #define HPGL_KIND_OK 0
 #define HPGL_KIND_SK 1
@@ -341,6 +349,7 @@ typedef struct hpgl_b200_result_t {
     double ms_device;             /* device work, CUDA events */
     double ms_d2h;
     double ms_total;              /* wall time of the call */
+    long long rounds;             /* sequential simulation: speculative rounds */
 } hpgl_b200_result_t;
 
 /* Runs one job on the GPU.  Returns 0 or an HPGL_E_* code (message via

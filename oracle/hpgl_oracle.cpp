@@ -873,6 +873,43 @@ double gaussian_quantile(double p) {
     return xp;
 }
 
+// non_parametric_cdf_2_t (non_parametric_cdf.h:185-260): a caller's CDF of
+// increasing values and cumulative probabilities, read and inverted by float
+// linear interpolation between the bracketing entries (the first / last
+// entry outside them).
+struct np_cdf {
+    const float *v, *p;
+    long long n;
+    float prob(float value) const {
+        const float *it = std::lower_bound(v, v + n, value);
+        if (it == v + n) return p[n - 1];
+        if (it == v) return p[0];
+        const long long b = it - v, a = b - 1;
+        return p[a] + (p[b] - p[a]) / (v[b] - v[a]) * (value - v[a]);
+    }
+    float inverse(float prob) const {
+        if (n <= 0) return 0;
+        const float *it = std::lower_bound(p, p + n, prob);
+        if (it == p) return v[0];
+        if (it == p + n) return v[n - 1];
+        const long long b = it - p, a = b - 1;
+        return v[a] + (v[b] - v[a]) / (p[b] - p[a]) * (prob - p[a]);
+    }
+};
+
+// gaussian_cdf_t::operator() (gaussian_distribution.h:22-41), Abramowitz and
+// Stegun 26.2.17, mean 0 and variance 1.
+double gaussian_cdf(double x) {
+    const double b[] = {0.319381530, -0.356563782, 1.781477937, -1.821255978, 1.330274429};
+    double sx = (x - 0.0) / std::sqrt(1.0);
+    const bool neg = sx < 0;
+    if (neg) sx = -sx;
+    const double t = 1 / (1 + 0.2316419 * sx);
+    const double zx = 1 / std::sqrt(2 * 3.14159265358) * std::exp(-sx * sx / 2);
+    const double r = 1 - zx * ((((b[4] * t + b[3]) * t + b[2]) * t + b[1]) * t + b[0]) * t;
+    return neg ? 1 - r : r;
+}
+
 // do_sequential_gausian_simulation (sequential_simulation.h:49-122) with
 // neighbour_lookup_t over the precalculated (radius-truncated) covariance:
 // nodes in the walk's order; each uninformed node inside the simulation mask
@@ -945,6 +982,27 @@ int oracle_sgs(int nx, int ny, int nz, float *values, unsigned char *mask, const
             err[err_len - 1] = 0;
         }
         return 1;
+    }
+}
+
+// Normal-score transforms of sequential Gaussian simulation (cdf_utils.h:12-50):
+// direction 0 maps values through the CDF to the standard normal quantile
+// (transform_cdf_p / transform_cdf_ptr from non_parametric_cdf_2_t to
+// gaussian_cdf_t), direction 1 back (gaussian_cdf_t to the CDF's inverse,
+// the probability passed as float).  Only nodes with mask != 0 (every node
+// when mask is null); out may be in.
+void oracle_cdf_transform(const float *in, float *out, const unsigned char *mask, long long n, const float *cdf_values,
+                          const float *cdf_probs, long long cdf_size, int direction) {
+    const np_cdf c{cdf_values, cdf_probs, cdf_size};
+    for (long long i = 0; i < n; ++i) {
+        if (mask && !mask[i]) continue;
+        if (direction == 0) {
+            const double P = c.prob(in[i]);
+            out[i] = (float)(gaussian_quantile(P) * std::sqrt(1.0) + 0.0);
+        } else {
+            const double P = gaussian_cdf(in[i]);
+            out[i] = c.inverse((float)P);
+        }
     }
 }
 

@@ -711,6 +711,10 @@ class HpglSgsParams(C.Structure):
                 ("kriging_kind", C.c_int), ("seed", C.c_long), ("min_neighbours", C.c_int)]
 
 
+class HpglNonParametricCdf(C.Structure):
+    _fields_ = [("values", C.POINTER(C.c_float)), ("probs", C.POINTER(C.c_float)), ("size", C.c_longlong)]
+
+
 class HpglFloatArray(C.Structure):
     _fields_ = [("data", C.POINTER(C.c_float)), ("shape", HpglShape)]
 
@@ -719,13 +723,32 @@ class HpglUbyteArray(C.Structure):
     _fields_ = [("data", C.POINTER(C.c_ubyte)), ("shape", HpglShape)]
 
 
-def sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None):
+def cdf_transform(values, cdf, direction, mask=None):
+    """Normal-score transform of a float32 array through a (values, probs)
+    CDF: direction 0 to the standard normal, 1 back (restated)."""
+    cv = np.ascontiguousarray(cdf[0], dtype=np.float32)
+    cp = np.ascontiguousarray(cdf[1], dtype=np.float32)
+    out = np.array(values, dtype=np.float32)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    restated().oracle_cdf_transform(_ptr(out, C.c_float), _ptr(out, C.c_float), _ptr(m, C.c_ubyte),
+                                    C.c_longlong(out.size), _ptr(cv, C.c_float), _ptr(cp, C.c_float),
+                                    C.c_longlong(cv.size), int(direction))
+    return out
+
+
+def sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None, cdf=None):
     """Restated sequential Gaussian simulation: (values, mask, order of the
-    simulated nodes)."""
+    simulated nodes).  `cdf` = (values, probs): the normal-score transforms
+    around it (sequential_gaussian_simulation.cpp:32-35, 72-73, 97-103,
+    119-123)."""
     lib = restated()
     nx, ny, nz = job["shape"]
     values = np.array(job["values"], dtype=np.float32)
     mask = np.array(job["mask"], dtype=np.uint8)
+    if cdf is not None:
+        values = cdf_transform(values, cdf, 0, mask)
+        if lvm is not None:
+            lvm = cdf_transform(lvm, cdf, 0)
     order = np.zeros(values.size, dtype=np.int32)
     n_order = C.c_int(0)
     sm = None if sim_mask is None else np.ascontiguousarray(sim_mask, dtype=np.uint8)
@@ -736,6 +759,8 @@ def sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None):
                         C.c_longlong(seed), _ptr(sm, C.c_ubyte), _ptr(order, C.c_int), C.byref(n_order), err, 512)
     if rc != 0:
         raise RuntimeError("oracle: " + err.value.decode())
+    if cdf is not None:
+        values = cdf_transform(values, cdf, 1, mask)
     return values, mask, order[:n_order.value]
 
 
@@ -746,10 +771,10 @@ def sgs_draws(seed, n):
     return xp
 
 
-def ref_sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None):
-    """The reference's hpgl_sgs_simulation / hpgl_sgs_lvm_simulation (no CDF
-    transform), compiled with oracle/ref_shim's boost::mt11213b and the
-    generated prime table."""
+def ref_sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None, cdf=None):
+    """The reference's hpgl_sgs_simulation / hpgl_sgs_lvm_simulation, compiled
+    with oracle/ref_shim's boost::mt11213b and the generated prime table;
+    `cdf` = (values, probs) or None."""
     ref = reference()
     nx, ny, nz = job["shape"]
     sh = _shape((nx, ny, nz))
@@ -772,10 +797,15 @@ def ref_sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None):
     if sim_mask is not None:
         sm_keep = np.ascontiguousarray(sim_mask, dtype=np.uint8)
         smp = C.byref(HpglUbyteArray(_ptr(sm_keep, C.c_ubyte), sh))
+    cdfp = None
+    if cdf is not None:
+        cv = np.ascontiguousarray(cdf[0], dtype=np.float32)
+        cp = np.ascontiguousarray(cdf[1], dtype=np.float32)
+        cdfp = C.byref(HpglNonParametricCdf(_ptr(cv, C.c_float), _ptr(cp, C.c_float), cv.size))
     if lvm is not None:
         lv = np.ascontiguousarray(lvm, dtype=np.float32)
         fa = HpglFloatArray(_ptr(lv, C.c_float), sh)
-        ref.hpgl_sgs_lvm_simulation(C.byref(arr), C.byref(q), None, C.byref(fa), smp)
+        ref.hpgl_sgs_lvm_simulation(C.byref(arr), C.byref(q), cdfp, C.byref(fa), smp)
     else:
-        ref.hpgl_sgs_simulation(C.byref(arr), C.byref(q), None, None, smp)
+        ref.hpgl_sgs_simulation(C.byref(arr), C.byref(q), cdfp, None, smp)
     return values, mask

@@ -77,3 +77,80 @@ def test_sgs_reference_entry_point(native_lib):
     assert native_lib.hpgl_get_last_error() == 0
     v, m, _ = O.sgs(job, ordinary=True, seed=555)
     assert _same(values, v) and np.array_equal(mask, m)
+
+
+def _calc_cdf(values, mask):
+    v = np.asarray(values, np.float32)[np.asarray(mask) != 0]
+    u, c = np.unique(v, return_counts=True)
+    size = u.size - 1 if u.size > 1 else u.size
+    return u[:size], np.cumsum(c[:size] / float(v.size)).astype(np.float32)
+
+
+def _geo(job):
+    from hpgl_b200.geo_bsd import geo
+    nx, ny, nz = job["shape"]
+    p = job["params"][0]
+    cov = geo.CovarianceModel(type=p["cov_type"], ranges=p["ranges"], angles=p["angles"], sill=p["sill"],
+                              nugget=p["nugget"])
+    prop = geo.ContProperty(np.asfortranarray(np.reshape(job["values"], (nx, ny, nz), order="F")),
+                            np.asfortranarray(np.reshape(job["mask"], (nx, ny, nz), order="F")))
+    return geo, geo.SugarboxGrid(nx, ny, nz), prop, cov
+
+
+@pytest.mark.parametrize("kriging_type", ["sk", "ok"])
+def test_sgs_simulation_with_cdf(native_lib, kriging_type):
+    from hpgl_b200.geo_bsd import sgs
+    from hpgl_b200.geo_bsd.cdf import calc_cdf
+    job = _job((22, 20, 8), seed=13)
+    geo, grid, prop, cov = _geo(job)
+    cdf = calc_cdf(prop)
+    out = sgs.sgs_simulation(prop, grid, cdf, job["params"][0]["radii"], 12, cov, 4242, kriging_type=kriging_type)
+    # the wrapper normalises the covariance to sill - nugget = 1 (sill 1, nugget 0 here: unchanged)
+    v, m, _ = O.sgs(job, ordinary=kriging_type == "ok", seed=4242, cdf=(cdf.values, cdf.probs))
+    assert _same(out.data.ravel(order="F"), v) and np.array_equal(out.mask.ravel(order="F"), m)
+
+
+def test_sgs_simulation_lvm_cdf_and_mask(native_lib):
+    from hpgl_b200.geo_bsd import sgs
+    job = _job((20, 16, 8), seed=14, n=20, radii=(10, 10, 5))
+    geo, grid, prop, cov = _geo(job)
+    rng = np.random.default_rng(21)
+    mean = np.asfortranarray((0.3 * rng.normal(size=prop.data.shape)).astype(np.float32))
+    sm = np.asfortranarray((rng.random(prop.data.shape) < 0.5).astype(np.uint8))
+    cdf = _calc_cdf(job["values"], job["mask"])
+    out = sgs.sgs_simulation((prop.data, prop.mask), grid, (prop.data, prop.mask), (10, 10, 5), 20, cov, 99,
+                             mean=mean, mask=sm)
+    v, m, _ = O.sgs(job, seed=99, lvm=mean.ravel(order="F"), sim_mask=sm.ravel(order="F"), cdf=cdf)
+    assert _same(out.data.ravel(order="F"), v) and np.array_equal(out.mask.ravel(order="F"), m)
+
+
+def test_unconditional_simulation(native_lib):
+    from hpgl_b200.geo_bsd import sgs
+    job = _job((24, 22, 6), seed=15, radii=(8, 8, 4))
+    geo, grid, prop, cov = _geo(job)
+    out = sgs.sgs_simulation(prop, grid, None, (8, 8, 4), 12, cov, 7, use_harddata=False)
+    empty = dict(job, values=np.zeros_like(job["values"]), mask=np.zeros_like(job["mask"]))
+    v, m, _ = O.sgs(empty, seed=7)
+    assert _same(out.data.ravel(order="F"), v) and np.array_equal(out.mask.ravel(order="F"), m)
+
+
+def test_window_bounds_do_not_change_results(native_lib):
+    # 166 x 141 x 40 cube, 1 % informed, radii 20, 12 neighbours: the result
+    # is the sequential one whatever the speculative window, and the rounds
+    # are few compared with the nodes
+    job = _job((166, 141, 40), seed=16, n=12, cov=W.EXPONENTIAL, radii=(20, 20, 20))
+    rng = np.random.default_rng(2)
+    job["mask"] = (rng.random(job["values"].size) < 0.01).astype(np.uint8)
+    runs = []
+    try:
+        for window in (0, 512, 1 << 20):
+            native_lib.hpgl_b200_set_sim_window(window)
+            assert native_lib.hpgl_get_last_error() == 0
+            r = N.simulate(job, 3439275, kind="sk")
+            runs.append(r)
+    finally:
+        native_lib.hpgl_b200_set_sim_window(0)
+    for r in runs[1:]:
+        assert _same(r["out"], runs[0]["out"]) and np.array_equal(r["out_mask"], runs[0]["out_mask"])
+    assert runs[0]["rounds"] < 1000
+    assert int(runs[0]["out_mask"].sum()) == job["values"].size

@@ -54,3 +54,43 @@ def test_path_visits_every_node_once():
 def test_draws_are_standard_normal():
     xp = O.sgs_draws(42, 200000)
     assert abs(xp.mean()) < 0.01 and abs(xp.std() - 1) < 0.01
+
+
+def _calc_cdf(values, mask):
+    v = np.asarray(values, np.float32)[np.asarray(mask) != 0]
+    u, c = np.unique(v, return_counts=True)
+    size = u.size - 1 if u.size > 1 else u.size
+    return u[:size], np.cumsum(c[:size] / float(v.size)).astype(np.float32)
+
+
+@need_ref
+@pytest.mark.parametrize("ordinary", [False, True])
+def test_sgs_cdf_transform_matches_reference(ordinary):
+    job = _job(seed=11)
+    cdf = _calc_cdf(job["values"], job["mask"])
+    v1, m1, _ = O.sgs(job, ordinary=ordinary, seed=3, cdf=cdf)
+    v2, m2 = O.ref_sgs(job, ordinary=ordinary, seed=3, cdf=cdf)
+    assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32)) and np.array_equal(m1, m2)
+
+
+@need_ref
+def test_sgs_lvm_cdf_matches_reference():
+    job = _job(shape=(16, 14, 8), seed=12)
+    rng = np.random.default_rng(5)
+    lvm = (0.1 * rng.normal(size=job["values"].size)).astype(np.float32)
+    cdf = _calc_cdf(job["values"], job["mask"])
+    v1, m1, _ = O.sgs(job, seed=8, lvm=lvm, cdf=cdf)
+    v2, m2 = O.ref_sgs(job, seed=8, lvm=lvm, cdf=cdf)
+    assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32)) and np.array_equal(m1, m2)
+
+
+def test_cdf_transform_round_trip_is_close():
+    # the back transform undoes the forward one up to the interpolation's
+    # float rounding (a property of the restated transforms, not of the data)
+    rng = np.random.default_rng(1)
+    vals = np.sort(rng.normal(size=200).astype(np.float32))
+    cdf = (vals[:-1], np.cumsum(np.full(199, 1 / 200.0)).astype(np.float32))
+    x = vals[10:150]
+    g = O.cdf_transform(x, cdf, 0)
+    back = O.cdf_transform(g, cdf, 1)
+    assert np.allclose(back, x, atol=2e-3)
