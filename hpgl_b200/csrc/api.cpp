@@ -100,9 +100,6 @@ void run(const char *name, hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     log_line(buf);
 }
 
-void not_provided(const char *what) {
-    throw HpglError{HPGL_E_UNSUPPORTED, std::string(what) + " is not provided by this build (kriging path only)"};
-}
 }  // namespace
 
 namespace {
@@ -651,12 +648,53 @@ void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *
         sgs_call(data, params, cdf, means->m_data, simulation_mask);
     });
 }
-void hpgl_sis_simulation(hpgl_ind_masked_array_t *, hpgl_ik_params_t *, int, int, hpgl_ubyte_array_t *) {
-    guarded("hpgl_sis_simulation", [&] { not_provided("sequential indicator simulation"); });
+// Sequential indicator simulation (api.cpp:517-580 of the reference), in
+// place on the codes: one params entry per category; the LVM form takes a
+// mean cube per category and, with use_correlograms, the correlogram
+// weights (sequential_indicator_simulation.cpp:150-181).
+static void sis_call(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, int indicator_count, int seed,
+                     const hpgl_float_array_t *means, hpgl_ubyte_array_t *simulation_mask, int use_correlograms) {
+    if (!data || !params) throw HpglError{HPGL_E_INVALID, "data or params are null"};
+    if (!data->m_data || !data->m_mask) throw HpglError{HPGL_E_INVALID, "property arrays are null"};
+    if (indicator_count < 1 || indicator_count > 255) throw HpglError{HPGL_E_INVALID, "invalid indicator count"};
+    hpgl_b200_job_t j = base_job(HPGL_KIND_IK, &data->m_shape);
+    j.codes = data->m_data;
+    j.mask = data->m_mask;
+    j.params = params;
+    j.n_params = indicator_count;
+    j.sequential = 1;
+    j.seed = seed;
+    j.simulation_mask = simulation_mask ? simulation_mask->m_data : nullptr;
+    std::vector<const float *> cubes;
+    if (means) {
+        const long long n = volume(&data->m_shape);
+        for (int k = 0; k < indicator_count; ++k) {
+            if (!means[k].m_data) throw HpglError{HPGL_E_INVALID, "mean array is null"};
+            if (volume(&means[k].m_shape) != n) throw HpglError{HPGL_E_INVALID, "mean array size differs"};
+            cubes.push_back(means[k].m_data);
+        }
+        j.category_means = cubes.data();
+        j.correlogram = use_correlograms != 0;
+    }
+    hpgl_b200_result_t r;
+    memset(&r, 0, sizeof(r));
+    r.out_codes = data->m_data;
+    r.out_mask = data->m_mask;
+    run("sequential indicator simulation", j, r);
 }
-void hpgl_sis_simulation_lvm(hpgl_ind_masked_array_t *, hpgl_ik_params_t *, hpgl_float_array_t *, int, int,
-                             hpgl_ubyte_array_t *, int) {
-    guarded("hpgl_sis_simulation_lvm", [&] { not_provided("sequential indicator simulation"); });
+
+void hpgl_sis_simulation(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, int indicator_count, int seed,
+                         hpgl_ubyte_array_t *simulation_mask) {
+    guarded("hpgl_sis_simulation",
+            [&] { sis_call(data, params, indicator_count, seed, nullptr, simulation_mask, 0); });
+}
+void hpgl_sis_simulation_lvm(hpgl_ind_masked_array_t *data, hpgl_ik_params_t *params, hpgl_float_array_t *mean_data,
+                             int indicator_count, int seed, hpgl_ubyte_array_t *simulation_mask,
+                             int use_correlograms) {
+    guarded("hpgl_sis_simulation_lvm", [&] {
+        if (!mean_data) throw HpglError{HPGL_E_INVALID, "mean arrays are null"};
+        sis_call(data, params, indicator_count, seed, mean_data, simulation_mask, use_correlograms);
+    });
 }
 // hpgl_simple_cokriging_mark1/2 (api.cpp:587-713 of the reference): the
 // three arrays must have the same size (the reference raises otherwise).

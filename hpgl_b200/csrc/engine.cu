@@ -109,6 +109,7 @@ struct JobState {
     double sk_mean;
     int nmax_all;
     bool want_variance, want_weights;
+    bool sis_lvm = false;
     long long kriged;
     // cokriging
     bool cok = false;
@@ -167,9 +168,12 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     S.precision = job.precision >= 0 ? job.precision : g_precision;
     if (S.cok) S.precision = HPGL_PRECISION_FP64;  // cokriging is solved in the reference's order only
     if (job.sequential) {
-        if (job.kind != KIND_OK && job.kind != KIND_SK && job.kind != KIND_LVM)
-            invalid("sequential simulation takes the kinds OK, SK and LVM");
+        if (job.kind != KIND_OK && job.kind != KIND_SK && job.kind != KIND_LVM && job.kind != KIND_IK)
+            invalid("sequential simulation takes the kinds OK, SK, LVM and IK");
         S.precision = HPGL_PRECISION_FP64;  // each node's draw depends on its exact kriging
+        if (job.kind == KIND_IK && job.category_means)
+            for (int k = 0; k < job.n_params; ++k)
+                if (!job.category_means[k]) invalid("category mean cube is null");
     }
     if (S.precision != HPGL_PRECISION_FP64 && S.precision != HPGL_PRECISION_MIXED) invalid("unknown precision");
     S.K = job.kind == KIND_IK ? job.n_params : 1;
@@ -196,6 +200,16 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
         for (auto &g : S.groups) {
             build_plan(g.plan, job.kind, job.nx, job.ny, job.nz, kp[g.k0], job.mask, threads, job.sequential != 0);
             S.nmax_all = std::max(S.nmax_all, g.plan.nmax);
+        }
+        if (job.sequential && job.kind == KIND_IK) {
+            // indicator simulation searches every category's template over
+            // one set of informed bits: one padding for all
+            int px = 0;
+            for (auto &g : S.groups) px = std::max(px, g.plan.px);
+            for (auto &g : S.groups) {
+                g.plan.px = px;
+                g.plan.wpr = g.plan.nseg + 2 * (px / 32) + 2;
+            }
         }
     } catch (const std::domain_error &e) {
         throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
@@ -238,7 +252,7 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     // sequential simulation krigs with mean 0 (sequential_gaussian_simulation.cpp:39-41)
     if (job.kind == KIND_SK && !job.sequential)
         S.sk_mean = job.sk_automatic_mean ? informed_mean(job.values, job.mask, S.size) : job.sk_mean;
-    S.want_variance = res.variance != nullptr || job.sequential;
+    S.want_variance = res.variance != nullptr || (job.sequential && cont);
     S.want_weights = res.weights != nullptr;
     S.kriged = 0;
     if (cont) {
@@ -259,7 +273,8 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     A.o_mask = take(n);
     A.o_values = cont ? take(n * 4) : 0;
     A.o_codes = cont ? 0 : take(n);
-    A.o_mean = job.kind == KIND_LVM ? take(n * 4) : 0;
+    S.sis_lvm = job.sequential && job.kind == KIND_IK && job.category_means;
+    A.o_mean = job.kind == KIND_LVM ? take(n * 4) : (S.sis_lvm ? take(n * S.K * 4) : 0);
     A.o_out_values = cont ? take(n * 4) : 0;
     A.o_out_codes = cont ? 0 : take(n);
     A.o_out_mask = take(n);
@@ -321,6 +336,10 @@ static void upload(JobState &S, cudaStream_t s) {
         CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_codes), job.codes, n, cudaMemcpyHostToDevice, s));
     if (job.kind == KIND_LVM)
         CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_mean), job.mean, n * 4, cudaMemcpyHostToDevice, s));
+    if (S.sis_lvm)
+        for (int k = 0; k < S.K; ++k)
+            CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_mean) + (size_t)k * n, job.category_means[k], n * 4,
+                                       cudaMemcpyHostToDevice, s));
     CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_pk), S.pk.data(), S.K * 4, cudaMemcpyHostToDevice, s));
     if (S.cok) {
         CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_svalues), job.secondary_values, n * 4, cudaMemcpyHostToDevice, s));
@@ -391,7 +410,7 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.values = cont ? at<float>(S, A.o_values) : nullptr;
     J.codes = cont ? nullptr : at<uint8_t>(S, A.o_codes);
     J.mask = at<uint8_t>(S, A.o_mask);
-    J.mean = job.kind == KIND_LVM ? at<float>(S, A.o_mean) : nullptr;
+    J.mean = (job.kind == KIND_LVM || S.sis_lvm) ? at<float>(S, A.o_mean) : nullptr;
     J.bits = at<uint32_t>(S, g.o_bits);
     J.K = S.K;
     J.k0 = g.k0;
@@ -408,6 +427,10 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.sim_values = cont ? at<float>(S, A.o_values) : nullptr;
     J.sim_mask = at<uint8_t>(S, A.o_mask);
     J.sim_bits = at<uint32_t>(S, g.o_bits);
+    J.sim_codes = cont ? nullptr : at<uint8_t>(S, A.o_codes);
+    J.sis_lvm = S.sis_lvm ? 1 : 0;
+    J.sis_corr = job.correlogram ? 1 : 0;
+    J.nb_stride = S.nmax_all;
     J.status = at<int8_t>(S, A.o_status);
     J.probs = cont ? nullptr : at<float>(S, A.o_probs);
     J.weights = S.want_weights ? at<double>(S, A.o_weights) : nullptr;
@@ -662,8 +685,12 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
         sim_path(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, path);
     } catch (const std::domain_error &e) {
         throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
+    } catch (const std::invalid_argument &e) {
+        throw HpglError{HPGL_E_INVALID, e.what()};
     }
-    gaussian_quantiles(path.u, xp, host_threads());
+    const bool indicator = job.kind == KIND_IK;
+    if (indicator) xp = path.u;  // sample() compares the draw itself
+    else gaussian_quantiles(path.u, xp, host_threads());
     res.ms_plan = ms_since(t0);
     auto t1 = std::chrono::steady_clock::now();
     cudaStream_t s = C.stream;
@@ -701,11 +728,29 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     G.win0 = reinterpret_cast<int *>(scratch + o_w0);
     G.win1 = reinterpret_cast<int *>(scratch + o_w1);
     G.ok = scratch + o_ok;
+    // indicator simulation: every category's plan (a category shares its
+    // group's)
+    DevPlan *d_plans = nullptr;
+    std::vector<DevPlan> cat_plans;
+    if (indicator) {
+        for (auto &gr : S.groups)
+            for (int k = gr.k0; k < gr.k1; ++k) cat_plans.push_back(gr.dp);
+        CUDA_CHECK(cudaMalloc(&d_plans, cat_plans.size() * sizeof(DevPlan)));
+    }
+    struct FreePlans {
+        void *p;
+        ~FreePlans() {
+            if (p) cudaFree(p);
+        }
+    } free_plans{d_plans};
     SgsCtl hc;
     memset(&hc, 0, sizeof(hc));
     hc.window = window;
     hc.total = nsim;
     CUDA_CHECK(cudaMemcpyAsync(G.ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
+    if (indicator)
+        CUDA_CHECK(cudaMemcpyAsync(d_plans, cat_plans.data(), cat_plans.size() * sizeof(DevPlan),
+                                   cudaMemcpyHostToDevice, s));
     if (nsim > 0) {
         CUDA_CHECK(cudaMemcpyAsync(scratch + o_nodes, path.nodes.data(), (size_t)nsim * 4, cudaMemcpyHostToDevice, s));
         CUDA_CHECK(cudaMemcpyAsync(scratch + o_xp, xp.data(), (size_t)nsim * 8, cudaMemcpyHostToDevice, s));
@@ -731,7 +776,10 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
         launch_sgs_admit(J, g.dp, G, 1, s);
         int chunk = 4;
         for (;;) {
-            for (int c = 0; c < chunk; ++c, ++round) launch_sgs_round(J, g.dp, G, (int)(round & 1), s);
+            for (int c = 0; c < chunk; ++c, ++round) {
+                if (indicator) launch_sis_round(J, g.dp, d_plans, S.nmax_all <= 32 ? 0 : 1, G, (int)(round & 1), s);
+                else launch_sgs_round(J, g.dp, G, (int)(round & 1), s);
+            }
             CUDA_CHECK(cudaGetLastError());
             CUDA_CHECK(cudaMemcpyAsync(&hc, G.ctl, sizeof(hc), cudaMemcpyDeviceToHost, s));
             CUDA_CHECK(cudaStreamSynchronize(s));
@@ -756,7 +804,10 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
                                              std::to_string(nsim) + " nodes"};
     auto t2 = std::chrono::steady_clock::now();
     const size_t n = (size_t)S.size;
-    CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, S.ar.o_values), n * 4, cudaMemcpyDeviceToHost, s));
+    if (indicator)
+        CUDA_CHECK(cudaMemcpyAsync(res.out_codes, at<uint8_t>(S, S.ar.o_codes), n, cudaMemcpyDeviceToHost, s));
+    else
+        CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, S.ar.o_values), n * 4, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaMemcpyAsync(res.out_mask, at<uint8_t>(S, S.ar.o_mask), n, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     res.ms_d2h = ms_since(t2);

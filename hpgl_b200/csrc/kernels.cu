@@ -422,6 +422,13 @@ void launch_sgs_admit(const DevJob &J, const DevPlan &P, const SgsState &G, int 
     sgs_commit_admit(J, P, G, cur, s);
 }
 
+void launch_sis_round(const DevJob &J, const DevPlan &P0, const DevPlan *plans, int family, const SgsState &G,
+                      int cur, cudaStream_t s) {
+    if (family == 0) launch_sis_try32(J, plans, G, cur, s);
+    else launch_sis_try64(J, plans, G, cur, s);
+    sgs_commit_admit(J, P0, G, cur, s);
+}
+
 void launch_sgs_round(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
     if (P.nmax <= 32) launch_sgs_try32(J, P, G, cur, s);
     else launch_sgs_try64(J, P, G, cur, s);

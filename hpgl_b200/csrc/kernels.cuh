@@ -120,6 +120,14 @@ struct DevJob {
     float *sim_values;
     uint8_t *sim_mask;
     uint32_t *sim_bits;
+    // sequential indicator simulation: the codes written as nodes are
+    // simulated (the same buffer as codes), per-category mean cubes in
+    // `mean` (K x size) instead of pk, the correlogram weights, and the
+    // stride of the neighbour lists (the largest max_neighbours)
+    uint8_t *sim_codes;
+    int sis_lvm;
+    int sis_corr;
+    int nb_stride;
 };
 
 // Launch tuning of the per-node kernels: the schedule (separate template
@@ -188,6 +196,13 @@ void launch_sgs_try32(const DevJob &J, const DevPlan &P, const SgsState &G, int 
 void launch_sgs_try64(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
 // the first admission (window buffer 0 from an empty buffer 1)
 void launch_sgs_admit(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
+// sequential indicator simulation: one round over window buffer `cur` with
+// the categories' plans (device array of K); family 0 when every category
+// has at most 32 neighbours
+void launch_sis_round(const DevJob &J, const DevPlan &P0, const DevPlan *plans, int family, const SgsState &G,
+                      int cur, cudaStream_t s);
+void launch_sis_try32(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s);
+void launch_sis_try64(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm);

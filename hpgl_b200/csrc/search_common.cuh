@@ -107,18 +107,19 @@ __device__ __forceinline__ void template_node(const DevJob &J, const DevPlan &P,
 // neighbour_lookup_t::find for one node of a speculative simulation round
 // (path rank `rank`): as template_node, over the committed nodes of lower
 // rank (informed bit set and rank_of below `rank`; informed data have rank
-// -1).  Returns -1 when the search completed, else the rank of the first
+// -1); the list goes to `out`, its length to `count`.  Returns -1 when the
+// search completed, else the rank of the first
 // pending node of lower rank met before the point where the search would
 // stop: in the sequential order that node would have been simulated and
 // seen, so nothing of this search is kept.  The bits and ranks are read-only
 // while a round's nodes are tried.
 __device__ __forceinline__ int template_node_spec(const DevJob &J, const DevPlan &P, const SgsState &G, int node,
-                                                  int rank, int lane) {
+                                                  int rank, int lane, int *out, int &count) {
     int x, y, z;
     node_xyz(J, node, x, y, z);
     const int nmax = P.nmax;
-    int *out = J.nb + (long long)node * nmax;
     int cnt = 0;
+    count = 0;
     for (int tb = 0; tb < P.tmpl_len && cnt < nmax; tb += 32) {
         const int t = tb + lane;
         bool hit = false, conflict = false;
@@ -151,7 +152,7 @@ __device__ __forceinline__ int template_node_spec(const DevJob &J, const DevPlan
         if (hit && cnt + pos < nmax) out[cnt + pos] = node + delta;
         cnt += __popc(b);
     }
-    if (lane == 0) J.nbcount[node] = min(cnt, nmax);
+    count = min(cnt, nmax);
     return -1;
 }
 
@@ -185,6 +186,51 @@ __device__ __forceinline__ void sgs_value(const DevJob &J, int node, double xp) 
         v = __dadd_rn(__dmul_rn(xp, 1.0), 0.0);
     J.sim_values[node] = __double2float_rn(v);
     J.sim_mask[node] = 1;
+}
+
+// Sequential indicator simulation helpers (sequential_indicator_simulation.cpp).
+
+// The mean of category k at a node: the category's mean cube, or its
+// marginal probability (mean_t, float).
+__device__ __forceinline__ float sis_mean(const DevJob &J, int k, long long node) {
+    return J.sis_lvm ? J.mean[(long long)k * J.size + node] : J.pk[k];
+}
+
+// sigma = sqrt(m (1 - m)) of an indicator mean, a mean of exactly 0 or 1
+// moved by 1e-5 (corellogramed_weights_3, my_kriging_weights.h:275-305).
+__device__ __forceinline__ double sis_sigma(float mean) {
+    double m = (double)mean;
+    if (m == 0) m = __dadd_rn(m, 0.00001);
+    if (m == 1) m = __dsub_rn(m, 0.00001);
+    return __dsqrt_rn(__dmul_rn(m, __dsub_rn(1.0, m)));
+}
+
+// sample (sample.cpp:8-21): the first category whose running sum of the
+// float probabilities (in double) exceeds u times their total; the last one
+// otherwise.
+__device__ __forceinline__ int sis_sample(const float *probs, int n, double u) {
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) sum = __dadd_rn(sum, (double)probs[i]);
+    const double s = __dmul_rn(u, sum);
+    double p = 0.0;
+    for (int i = 0; i < n; ++i) {
+        p = __dadd_rn(p, (double)probs[i]);
+        if (s < p) return i;
+    }
+    return n - 1;
+}
+
+// Records the outcome of one tried node: its code (and mask) once every
+// category's search completed, else its blocker.
+__device__ __forceinline__ void sis_finish(const DevJob &J, const SgsState &G, int node, int rank, int slot,
+                                           int blocker) {
+    if (blocker < 0) {
+        J.sim_codes[node] = (uint8_t)sis_sample(J.probs + (long long)node * J.K, J.K, G.xp[rank]);
+        J.sim_mask[node] = 1;
+    } else {
+        G.blocker[rank] = blocker;
+    }
+    G.ok[slot] = blocker < 0;
 }
 
 }  // namespace hpgl_b200

@@ -57,7 +57,11 @@ struct Path {
             C = primes[(size_t)k];
             if (std::floor(double(size) / double(C)) != (double(size) / double(C))) break;
         }
-        R = seed % size;
+        // path_random_generator_t(int size, int seed) takes the seed as int;
+        // a negative one makes the walk leave the grid
+        const int s32 = (int)(uint32_t)seed;
+        if (s32 < 0) throw std::invalid_argument("the simulation path is undefined for a negative seed");
+        R = s32 % size;
     }
     long long next() {
         const long long r = R;

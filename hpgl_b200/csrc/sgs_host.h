@@ -14,7 +14,9 @@ struct SimPath {
 
 // The path's uninformed nodes inside `sim_mask` (all when null: a node is
 // simulated when sim_mask[node] == 1) in path order, with the generator's
-// draws in the same order.  Throws std::domain_error above 10^7 nodes.
+// draws in the same order.  Throws std::domain_error above 10^7 nodes and
+// std::invalid_argument when the seed, as the int the path takes, is
+// negative.
 void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out);
 
 // xp[k] = the standard normal quantile of u[k] (gaussian_cdf_t::inverse).

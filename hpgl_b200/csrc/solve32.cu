@@ -261,10 +261,14 @@ __device__ __forceinline__ bool copy_informed(const DevJob &J, const NodeFetch &
 __device__ __noinline__ double dsqrt_rn(double a) { return __dsqrt_rn(a); }
 __device__ __noinline__ double drcp_rn(double a) { return __drcp_rn(a); }
 
-// Solves and writes the outputs of one system.  Lane k gathers column k of
-// the upper triangle straight into registers.
-__device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane,
-                                             const NodeData &d) {
+// Factorises and solves one system (weights of row `lane` in w); returns the
+// status.  Lane k gathers column k of the upper triangle straight into
+// registers.  CORR scales entry (i, k) by sg_k sg_i, sg the lanes' sigma
+// (corellogramed_weights_3, my_kriging_weights.h:308-317; b is scaled by the
+// caller).
+template <bool CORR>
+__device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, SysSmem &S, int lane, const NodeData &d,
+                                          double sg, double &w_out) {
     constexpr int LD = 34;
     const int n = d.n;
     const bool ordinary = J.kind == 0;
@@ -274,8 +278,12 @@ __device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, 
         // A(i, lane) = C(x_i - x_lane) for i <= lane (my_kriging_weights.h:53)
         const int ix = __shfl_sync(FULL_MASK, d.ox, i), iy = __shfl_sync(FULL_MASK, d.oy, i);
         const int iz = __shfl_sync(FULL_MASK, d.oz, i), il = __shfl_sync(FULL_MASK, d.lin, i);
+        const double si = CORR ? __shfl_sync(FULL_MASK, sg, i) : 0.0;
         c[i] = 0.0;
-        if (i <= lane && lane < n) c[i] = cov_lin(P, ix - d.ox, iy - d.oy, iz - d.oz, il - d.lin, J.err);
+        if (i <= lane && lane < n) {
+            c[i] = cov_lin(P, ix - d.ox, iy - d.oy, iz - d.oz, il - d.lin, J.err);
+            if (CORR) c[i] = __dmul_rn(c[i], __dmul_rn(sg, si));
+        }
     }
     // DPOTF2 'U': column j, ajj = a_jj - sum_{i<j} a_ij^2; a_jk += -sum a_ij a_ik;
     // a_jk *= 1/ajj.  Finished entries U(j,k) go to S.A (column k at k*34)
@@ -375,6 +383,17 @@ __device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, 
             w = xa;
         }
     }
+    w_out = w;
+    return status;
+}
+
+// Solves and writes the outputs of one system.
+__device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane,
+                                             const NodeData &d) {
+    const int n = d.n;
+    const bool ordinary = J.kind == 0;
+    double w;
+    const int status = exact_core<false>(J, P, S, lane, d, 0.0, w);
     double variance = -1.0;
     if (J.variance && status == ST_SUCCESS) {
         // c0 - p_0 - p_1 - ... (my_kriging_weights.h): subtracting p is adding -p
@@ -636,7 +655,9 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P,
             todo &= todo - 1;
             const int rank = __shfl_sync(FULL_MASK, my_rank, l);
             const int node = G.nodes[rank];
-            const int blocker = template_node_spec(J, P, G, node, rank, lane);
+            int cnt;
+            const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
+            if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
             __syncwarp();
             if (blocker < 0) {
                 const NodeFetch f = fetch_node(J, P, node, lane);
@@ -653,11 +674,113 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Sequential indicator simulation (do_sis, sequential_indicator_simulation.cpp:23-116).
+
+// Row `lane` of category k's system: dv = indicator - mean of the neighbour
+// (float, combiner.h:18-22), b = C(x_lane - x0), scaled by sg sgc with the
+// correlogram weights (sg: the neighbour's sigma).
+__device__ __forceinline__ NodeData sis_load32(const DevJob &J, const DevPlan &P, SysSmem &S, int node,
+                                               const int *list, int n, int k, double sgc, int lane, double &sg) {
+    NodeData d;
+    d.n = n;
+    int x0, y0, z0;
+    node_xyz(J, node, x0, y0, z0);
+    d.dv = 0.f;
+    d.code = -1;
+    d.b = 0.0;
+    sg = 0.0;
+    int ox = 0, oy = 0, oz = 0;
+    if (lane < n) {
+        const int cell = list[lane];
+        int qx, qy, qz;
+        node_xyz(J, cell, qx, qy, qz);
+        ox = qx - x0;
+        oy = qy - y0;
+        oz = qz - z0;
+        const float m = sis_mean(J, k, cell);
+        d.dv = __fsub_rn(J.codes[cell] == k ? 1.f : 0.f, m);
+        d.b = cov_at(P, ox, oy, oz, J.err);
+        if (J.sis_corr) {
+            sg = sis_sigma(m);
+            d.b = __dmul_rn(d.b, __dmul_rn(sg, sgc));
+        }
+    }
+    d.ox = ox;
+    d.oy = oy;
+    d.oz = oz;
+    d.lin = oz * P.syx + oy * P.sx + ox;
+    S.nb[lane] = make_int4(ox, oy, oz, d.lin);
+    __syncwarp();
+    return d;
+}
+
+// One speculative round of sequential indicator simulation (every category
+// at most 32 neighbours): one warp per pending node, the categories in
+// order; per category the template search with conflict detection, the
+// simple kriging system (correlogram-scaled with the mean cubes when asked)
+// and the probability m_c + sum w_i (ind_i - m_i) accumulated in double
+// (kriging_interpolation.h:228-265 with a double result), the mean when the
+// kriging fails.  Two categories krige category 0 only and take 1 - p for
+// the other (median SIS).  The code is drawn from the float probabilities.
+__global__ void __launch_bounds__(WARPS32 * 32) k_sis_try32(DevJob J, const DevPlan *plans, SgsState G, int cur) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    const int count = G.ctl->count[cur];
+    const int *win = cur ? G.win1 : G.win0;
+    const int cats = J.K == 2 ? 1 : J.K;
+    for (int base = (blockIdx.x * WARPS32 + warp) * 32; base < count; base += gridDim.x * WARPS32 * 32) {
+        int my_rank;
+        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
+        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
+            const int node = G.nodes[rank];
+            int *list = J.nb + (long long)node * J.nb_stride;
+            float *probs = J.probs + (long long)node * J.K;
+            int blocker = -1;
+            for (int k = 0; k < cats; ++k) {
+                const DevPlan &P = plans[k];
+                int cnt;
+                blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
+                if (blocker >= 0) break;
+                __syncwarp();
+                const float mc = sis_mean(J, k, node);
+                double prob = (double)mc;
+                if (cnt > 0) {
+                    const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
+                    double sg, w;
+                    const NodeData d = sis_load32(J, P, S, node, list, cnt, k, sgc, lane, sg);
+                    const int status = J.sis_corr ? exact_core<true>(J, P, S, lane, d, sg, w)
+                                                  : exact_core<false>(J, P, S, lane, d, 0.0, w);
+                    if (status == ST_SUCCESS)
+                        prob = seq_dsum((double)mc, __dmul_rn(w, (double)d.dv), cnt, S.vd, lane);
+                }
+                if (lane == 0) {
+                    probs[k] = __double2float_rn(prob);
+                    if (J.K == 2) probs[1] = __double2float_rn(__dsub_rn(1.0, prob));
+                }
+                __syncwarp();
+            }
+            if (lane == 0) sis_finish(J, G, node, rank, base + l, blocker);
+            __syncwarp();
+        }
+    }
+}
+
 }  // namespace
 
 void launch_sgs_try32(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
     const long long g = persistent_grid((const void *)k_sgs_try32, WARPS32 * 32, SMEM32, 0, 1LL << 30);
     k_sgs_try32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, P, G, cur);
+}
+
+void launch_sis_try32(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s) {
+    const long long g = persistent_grid((const void *)k_sis_try32, WARPS32 * 32, SMEM32, 0, 1LL << 30);
+    k_sis_try32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, plans, G, cur);
 }
 
 void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm) {

@@ -213,8 +213,10 @@ __device__ __forceinline__ double pair_cov64(const DevJob &J, const DevPlan &P, 
 // triangle into the skewed packed layout, in column order, 32 at a time
 // (pairs[p] = i | k << 8); lanes stay converged and the gathers of 8 pairs
 // are issued together.  Columns from n on are left as they are.
+template <bool CORR>
 __device__ __forceinline__ void build_packed(const DevJob &J, const DevPlan &P, double *U, const int4 *nb,
-                                             const int *cs, const uint16_t *pairs, int n, int lane) {
+                                             const int *cs, const uint16_t *pairs, int n, int lane,
+                                             const double *sg) {
     const int npairs = n * (n - 1) / 2;
     for (int p0 = 0; p0 < npairs; p0 += 256) {
         double v[8];
@@ -228,6 +230,7 @@ __device__ __forceinline__ void build_packed(const DevJob &J, const DevPlan &P, 
                 const int ik = __ldg(pairs + p);
                 const int i = ik & 0xff, k = ik >> 8;
                 v[e] = pair_cov64(J, P, nb[i], nb[k]);
+                if (CORR) v[e] = __dmul_rn(v[e], __dmul_rn(sg[k], sg[i]));
                 dst[e] = cs[k] + i;
             }
         }
@@ -238,12 +241,17 @@ __device__ __forceinline__ void build_packed(const DevJob &J, const DevPlan &P, 
     __syncwarp();
 }
 
-__device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs,
-                               const uint16_t *pairs, int node, int lane, const Node64 &d) {
+// Factorises and solves one system (weights of rows lane, lane + 32 in w0,
+// w1); returns the status.  CORR scales entry (i, k) by sg[k] sg[i]
+// (corellogramed_weights_3, my_kriging_weights.h:308-317; b is scaled by
+// the caller).
+template <bool CORR>
+__device__ int exact64_core(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs, const uint16_t *pairs,
+                            int lane, const Node64 &d, const double *sg, double &w0_out, double &w1_out) {
     const int n = d.n;
     const bool ordinary = J.kind == 0;
     double *U = S.U;
-    build_packed(J, P, U, S.nb, cs, pairs, n, lane);
+    build_packed<CORR>(J, P, U, S.nb, cs, pairs, n, lane, sg);
     const int k0 = lane, k1 = lane + 32;  // the lane's columns in the factorisation
     const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0), the table's centre
     // diagonal slots and pads of the lane's columns are zero until their step
@@ -294,7 +302,7 @@ __device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S
         // every lane has read column j's diagonal slot before it is written
         __syncwarp();
         const double tj = __shfl_sync(FULL_MASK, lo ? t0 : t1, owner);
-        const double ajj = __dsub_rn(a_diag, tj);
+        const double ajj = __dsub_rn(CORR ? __dmul_rn(a_diag, __dmul_rn(sg[j], sg[j])) : a_diag, tj);
         if (!(ajj > 0.0)) {
             info = j + 1;
             break;
@@ -404,6 +412,18 @@ __device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S
             w1 = xa1;
         }
     }
+    w0_out = w0;
+    w1_out = w1;
+    return status;
+}
+
+__device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs,
+                               const uint16_t *pairs, int node, int lane, const Node64 &d) {
+    const int n = d.n;
+    const bool ordinary = J.kind == 0;
+    const int n0 = n < 32 ? n : 32;
+    double w0, w1;
+    const int status = exact64_core<false>(J, P, S, cs, pairs, lane, d, nullptr, w0, w1);
     double variance = -1.0;
     if (J.variance && status == ST_SUCCESS) {
         double v = P.c0;
@@ -449,7 +469,9 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs_try64(DevJob J, DevP
             todo &= todo - 1;
             const int rank = __shfl_sync(FULL_MASK, my_rank, l);
             const int node = G.nodes[rank];
-            const int blocker = template_node_spec(J, P, G, node, rank, lane);
+            int cnt;
+            const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
+            if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
             __syncwarp();
             if (blocker < 0) {
                 const NodeFetch f = fetch_node(J, P, node, lane);
@@ -595,7 +617,7 @@ __device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, 
         return;
     }
     const int n = d.n;
-    build_packed(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane);
+    build_packed<false>(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane, nullptr);
     // Rows lane and lane + 32 of the unit-diagonal system A / C(0),
     // identity beyond n.
     float2 m0[32], m1[32];
@@ -789,6 +811,106 @@ __global__ void __launch_bounds__(32) k_fused64(DevJob J, DevPlan P) {
 constexpr size_t SMEM64_EXACT = sizeof(Exact64Smem) * WARPS64_BLOCK;
 constexpr size_t SMEM64_MIXED = sizeof(Mixed64Smem);
 
+// ---------------------------------------------------------------------------
+// Sequential indicator simulation with categories of up to 64 neighbours
+// (the 32-neighbour kernel's rules, k_sis_try32 in solve32.cu).
+
+struct Sis64Smem {
+    Exact64Smem e;
+    double sg[N64];  // the rows' sigma (correlogram weights)
+};
+
+__device__ __forceinline__ Node64 sis_load64(const DevJob &J, const DevPlan &P, Sis64Smem &S, int node,
+                                             const int *list, int n, int k, double sgc, int lane) {
+    Node64 d;
+    d.n = n;
+    int x0, y0, z0;
+    node_xyz(J, node, x0, y0, z0);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int row = lane + 32 * r;
+        d.dv[r] = 0.f;
+        d.code[r] = -1;
+        d.b[r] = 0.0;
+        double sg = 0.0;
+        int4 o = make_int4(0, 0, 0, 0);
+        if (row < n) {
+            const int cell = list[row];
+            int qx, qy, qz;
+            node_xyz(J, cell, qx, qy, qz);
+            o.x = qx - x0;
+            o.y = qy - y0;
+            o.z = qz - z0;
+            o.w = o.z * P.syx + o.y * P.sx + o.x;
+            const float m = sis_mean(J, k, cell);
+            d.dv[r] = __fsub_rn(J.codes[cell] == k ? 1.f : 0.f, m);
+            d.b[r] = cov_lin(P, o.x, o.y, o.z, o.w, J.err);
+            if (J.sis_corr) {
+                sg = sis_sigma(m);
+                d.b[r] = __dmul_rn(d.b[r], __dmul_rn(sg, sgc));
+            }
+        }
+        S.e.nb[row] = o;
+        S.sg[row] = sg;
+    }
+    __syncwarp();
+    return d;
+}
+
+__global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sis_try64(DevJob J, const DevPlan *plans, SgsState G, int cur) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ int s_cs[N64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
+    __syncthreads();
+    Sis64Smem &S = reinterpret_cast<Sis64Smem *>(dyn_smem)[warp];
+    const int count = G.ctl->count[cur];
+    const int *win = cur ? G.win1 : G.win0;
+    const int cats = J.K == 2 ? 1 : J.K;
+    for (int base = (blockIdx.x * WARPS64_BLOCK + warp) * 32; base < count; base += gridDim.x * WARPS64_BLOCK * 32) {
+        int my_rank;
+        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
+        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
+            const int node = G.nodes[rank];
+            int *list = J.nb + (long long)node * J.nb_stride;
+            float *probs = J.probs + (long long)node * J.K;
+            int blocker = -1;
+            for (int k = 0; k < cats; ++k) {
+                const DevPlan &P = plans[k];
+                int cnt;
+                blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
+                if (blocker >= 0) break;
+                __syncwarp();
+                const float mc = sis_mean(J, k, node);
+                double prob = (double)mc;
+                if (cnt > 0) {
+                    const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
+                    const Node64 d = sis_load64(J, P, S, node, list, cnt, k, sgc, lane);
+                    double w0, w1;
+                    const int status =
+                        J.sis_corr ? exact64_core<true>(J, P, S.e, s_cs, g_pairs64.v, lane, d, S.sg, w0, w1)
+                                   : exact64_core<false>(J, P, S.e, s_cs, g_pairs64.v, lane, d, nullptr, w0, w1);
+                    if (status == ST_SUCCESS) {
+                        const double t0 = __dmul_rn(w0, (double)d.dv[0]), t1 = __dmul_rn(w1, (double)d.dv[1]);
+                        prob = rows_dsum((double)mc, t0, t1, cnt);
+                    }
+                }
+                if (lane == 0) {
+                    probs[k] = __double2float_rn(prob);
+                    if (J.K == 2) probs[1] = __double2float_rn(__dsub_rn(1.0, prob));
+                }
+                __syncwarp();
+            }
+            if (lane == 0) sis_finish(J, G, node, rank, base + l, blocker);
+            __syncwarp();
+        }
+    }
+}
+
 }  // namespace
 
 void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
@@ -802,6 +924,12 @@ void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_lis
 void launch_sgs_try64(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
     const long long g = persistent_grid((const void *)k_sgs_try64, WARPS64_BLOCK * 32, SMEM64_EXACT, 0, 1LL << 30);
     k_sgs_try64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, G, cur);
+}
+
+void launch_sis_try64(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s) {
+    const size_t smem = sizeof(Sis64Smem) * WARPS64_BLOCK;
+    const long long g = persistent_grid((const void *)k_sis_try64, WARPS64_BLOCK * 32, smem, 0, 1LL << 30);
+    k_sis_try64<<<(unsigned)g, WARPS64_BLOCK * 32, smem, s>>>(J, plans, G, cur);
 }
 
 void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s, int blocks_per_sm) {

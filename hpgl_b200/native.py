@@ -47,7 +47,8 @@ class Job(C.Structure):
                 ("secondary_values", C.POINTER(C.c_float)), ("secondary_mask", C.POINTER(C.c_ubyte)),
                 ("primary_mean", C.c_double), ("secondary_mean", C.c_double), ("secondary_variance", C.c_double),
                 ("correlation", C.c_double), ("secondary_cov", C.c_void_p),
-                ("sequential", C.c_int), ("seed", C.c_longlong), ("simulation_mask", C.POINTER(C.c_ubyte))]
+                ("sequential", C.c_int), ("seed", C.c_longlong), ("simulation_mask", C.POINTER(C.c_ubyte)),
+                ("category_means", C.POINTER(C.POINTER(C.c_float))), ("correlogram", C.c_int)]
 
 
 class Result(C.Structure):
@@ -165,6 +166,13 @@ class _Prepared:
             sm = job.get("simulation_mask")
             self.sim_mask = None if sm is None else np.ascontiguousarray(sm, dtype=np.uint8)
             j.simulation_mask = _ptr(self.sim_mask, C.c_ubyte)
+            cm = job.get("category_means")
+            if cm is not None:
+                self.cat_means = [np.ascontiguousarray(a, dtype=np.float32) for a in cm]
+                self.cat_ptrs = (C.POINTER(C.c_float) * len(self.cat_means))(
+                    *[_ptr(a, C.c_float) for a in self.cat_means])
+                j.category_means = C.cast(self.cat_ptrs, C.POINTER(C.POINTER(C.c_float)))
+                j.correlogram = int(bool(job.get("correlogram", False)))
         self.job = j
         self.out = self.values.copy() if self.cont else self.codes.copy()
         self.out_mask = self.mask.copy()
@@ -228,6 +236,15 @@ def simulate(job, seed, kind=None, simulation_mask=None):
     or "lvm"); returns the dict of krige() with the simulated property."""
     j = dict(job, sequential=True, seed=seed, simulation_mask=simulation_mask)
     return krige(j, precision="fp64", kind=kind)
+
+
+def simulate_indicator(job, seed, simulation_mask=None, category_means=None, correlogram=False):
+    """Sequential indicator simulation of an IK job (codes, mask, one params
+    entry per category with marginal_prob); `category_means`: optional mean
+    cubes per category (with the correlogram weights when asked)."""
+    j = dict(job, sequential=True, seed=seed, simulation_mask=simulation_mask, category_means=category_means,
+             correlogram=correlogram)
+    return krige(j, precision="fp64", kind="ik")
 
 
 def bench(job, precision="mixed", iters=5, warmup=3, flush_bytes=256 << 20, kind=None):

@@ -308,12 +308,18 @@ typedef struct hpgl_b200_job_t {
     double secondary_variance;    /* Markov model I: variance of the secondary */
     double correlation;           /* correlation coefficient of the two */
     const hpgl_cov_params_t *secondary_cov;  /* Markov model II: secondary covariance */
-    /* sequential Gaussian simulation (kinds OK, SK with mean 0, LVM): the
-       uninformed nodes inside `simulation_mask` (all when NULL) are simulated
-       along the reference's random path for `seed`; always FP64 */
+    /* sequential simulation: Gaussian (kinds OK, SK with mean 0, LVM) or
+       indicator (kind IK, one params entry per category): the uninformed
+       nodes inside `simulation_mask` (all when NULL) are simulated along the
+       reference's random path for `seed`; always FP64 */
     int sequential;
     long long seed;
     const unsigned char *simulation_mask;
+    /* sequential indicator simulation: optional per-category mean cubes
+       (n_params pointers) in place of the marginal probabilities, and the
+       correlogram weights for them */
+    const float *const *category_means;
+    int correlogram;
 } hpgl_b200_job_t;
 
 /* Outputs of hpgl_b200_krige.  out_values (cont) or out_codes (IK) and

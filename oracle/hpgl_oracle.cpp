@@ -821,7 +821,10 @@ struct path_walk {
             C = primes[(size_t)k];
             if (std::floor(double(size) / double(C)) != (double(size) / double(C))) break;
         }
-        R = seed % size;
+        // path_random_generator_t(int size, int seed): the seed arrives as int
+        const int s32 = (int)(uint32_t)seed;
+        if (s32 < 0) throw std::runtime_error("the path is undefined for a negative seed");
+        R = s32 % size;
     }
     long long next() {
         const long long r = R;
@@ -963,6 +966,108 @@ void sgs(const grid3 &g, float *values, unsigned char *mask, const oracle_params
     if (n_order) *n_order = count;
 }
 
+// corellogramed_weights_3 (my_kriging_weights.h:257-363): simple kriging of
+// the system scaled by the indicator standard deviations sigma =
+// sqrt(m (1 - m)) of the neighbours' and the centre's means (a mean of
+// exactly 0 or 1 moved by 1e-5): A(i,j) = C(x_i, x_j) (s_i s_j), b_i =
+// C(x_i, x0) (s_i s_c); the weights are not rescaled.
+bool correlogram_weights(const int *center, float center_mean, const std::vector<int> &coords,
+                         const std::vector<float> &means, const covariance &cov, std::vector<double> &w) {
+    const int n = (int)coords.size() / 3;
+    w.assign(n, 0.0);
+    if (n <= 0) return false;
+    auto sigma = [](double m) {
+        if (m == 0) m += 0.00001;
+        if (m == 1) m -= 0.00001;
+        return std::sqrt(m * (1 - m));
+    };
+    const double sc = sigma(center_mean);
+    std::vector<double> sg(n), A((size_t)n * n), b(n);
+    for (int i = 0; i < n; ++i) sg[i] = sigma(means[i]);
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) A[(size_t)i * n + j] = cov(&coords[3 * i], &coords[3 * j]) * (sg[i] * sg[j]);
+        b[i] = cov(&coords[3 * i], center) * (sg[i] * sc);
+    }
+    const int info = oracle_dpotf2_upper(n, A.data(), n);
+    for (int i = 0; i < n; ++i) w[i] = b[i];
+    oracle_dpotrs_upper(n, 1, A.data(), n, w.data(), n);
+    return info == 0;
+}
+
+// do_sis (sequential_indicator_simulation.cpp:23-116): along the random path
+// each uninformed node inside the simulation mask gets, per category k, the
+// simple-kriged probability of code k from the informed and already
+// simulated nodes (kriging_interpolation.h:228-265 with the category's
+// radius-truncated covariance and template search; the estimate
+// m_c + sum w_i (ind_i - m_i) accumulated in double; the mean, p_k or the
+// category's mean cube, when the kriging fails); two categories krige
+// category 0 only and take 1 - p for the other.  The code is drawn from the
+// float probabilities (sample.cpp:8-21).
+void sis(const grid3 &g, unsigned char *codes, unsigned char *mask, const oracle_params_t *p, int K,
+         const float *const *lvm, bool corr, long long seed, const unsigned char *sim_mask) {
+    std::vector<covariance> covs;
+    std::vector<std::vector<int>> tmpls;
+    for (int k = 0; k < K; ++k) {
+        covs.emplace_back(p[k], true);
+        tmpls.push_back(build_template(covs.back(), p[k]));
+    }
+    const long long size = g.size();
+    path_walk path(size, seed);
+    mt11213b gen((uint32_t)seed);
+    long long node = path.next();
+    for (long long counter = 0; counter < size; ++counter, node = path.next()) {
+        if (mask[node]) continue;
+        if (sim_mask && sim_mask[node] != 1) continue;
+        int center[3];
+        g.loc((int)node, center);
+        std::vector<float> probs;
+        const int cats = K == 2 ? 1 : K;
+        for (int k = 0; k < cats; ++k) {
+            const std::vector<int> &tm = tmpls[k];
+            std::vector<int> nb, coords;
+            for (size_t t = 0; t < tm.size() / 3 && (int)nb.size() < p[k].max_neighbours; ++t) {
+                int pt[3] = {center[0] + tm[3 * t], center[1] + tm[3 * t + 1], center[2] + tm[3 * t + 2]};
+                const int idx = g.index(pt);
+                if (idx >= 0 && mask[idx]) nb.push_back(idx);
+            }
+            const float pk = (float)p[k].marginal_prob;
+            auto mean_at = [&](long long i) -> float { return lvm ? lvm[k][i] : pk; };
+            double prob = lvm ? (double)lvm[k][node] : (double)pk;
+            if (!nb.empty()) {
+                coords_of(g, nb, coords);
+                std::vector<float> means(nb.size());
+                for (size_t i = 0; i < nb.size(); ++i) means[i] = mean_at(nb[i]);
+                std::vector<double> w;
+                double variance;
+                const bool ok = corr ? correlogram_weights(center, mean_at(node), coords, means, covs[k], w)
+                                     : kriging_weights(false, center, coords, covs[k], w, variance);
+                if (ok) {
+                    double r = (float)mean_at(node);
+                    for (size_t i = 0; i < nb.size(); ++i)
+                        r += w[i] * (float)((codes[nb[i]] == k ? 1 : 0) - means[i]);
+                    prob = r;
+                }
+            }
+            probs.push_back((float)prob);
+            if (K == 2) probs.push_back((float)(1 - prob));
+        }
+        double sum = 0.0;
+        for (float q : probs) sum += q;
+        const double s = gen.uniform() * sum;
+        double acc = 0;
+        int code = (int)probs.size() - 1;
+        for (size_t i = 0; i < probs.size(); ++i) {
+            acc += probs[i];
+            if (s < acc) {
+                code = (int)i;
+                break;
+            }
+        }
+        codes[node] = (unsigned char)code;
+        mask[node] = 1;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1003,6 +1108,24 @@ void oracle_cdf_transform(const float *in, float *out, const unsigned char *mask
             const double P = gaussian_cdf(in[i]);
             out[i] = c.inverse((float)P);
         }
+    }
+}
+
+// Sequential indicator simulation in place on codes / mask; `lvm` (optional)
+// holds K mean cubes, `corr` selects the correlogram weights.
+int oracle_sis(int nx, int ny, int nz, unsigned char *codes, unsigned char *mask, const oracle_params_t *p, int K,
+               const float *const *lvm, int corr, long long seed, const unsigned char *sim_mask, char *err,
+               int err_len) {
+    try {
+        if (K < 2) throw std::runtime_error("at least two categories");
+        sis(grid3{nx, ny, nz}, codes, mask, p, K, lvm, corr != 0, seed, sim_mask);
+        return 0;
+    } catch (const std::exception &e) {
+        if (err && err_len > 0) {
+            strncpy(err, e.what(), err_len - 1);
+            err[err_len - 1] = 0;
+        }
+        return 1;
     }
 }
 

@@ -809,3 +809,79 @@ def ref_sgs(job, ordinary=False, seed=1, sim_mask=None, lvm=None, cdf=None):
     else:
         ref.hpgl_sgs_simulation(C.byref(arr), C.byref(q), cdfp, None, smp)
     return values, mask
+
+
+def _ik_param_array(params):
+    arr = (OracleParams * len(params))()
+    for i, p in enumerate(params):
+        arr[i] = oracle_params(p)
+    return arr
+
+
+def sis(shape, codes, mask, params, seed=1, sim_mask=None, lvm=None, correlogram=False):
+    """Restated sequential indicator simulation: (codes, mask).  `params`:
+    one dict per category (with marginal_prob); `lvm`: K mean cubes."""
+    nx, ny, nz = shape
+    c = np.array(codes, dtype=np.uint8)
+    m = np.array(mask, dtype=np.uint8)
+    K = len(params)
+    sm = None if sim_mask is None else np.ascontiguousarray(sim_mask, dtype=np.uint8)
+    keep = []
+    lv = None
+    if lvm is not None:
+        keep = [np.ascontiguousarray(a, dtype=np.float32) for a in lvm]
+        lv = (C.POINTER(C.c_float) * K)(*[_ptr(a, C.c_float) for a in keep])
+    err = C.create_string_buffer(512)
+    rc = restated().oracle_sis(nx, ny, nz, _ptr(c, C.c_ubyte), _ptr(m, C.c_ubyte), _ik_param_array(params), K, lv,
+                               int(correlogram), C.c_longlong(seed), _ptr(sm, C.c_ubyte), err, 512)
+    if rc != 0:
+        raise RuntimeError("oracle: " + err.value.decode())
+    return c, m
+
+
+class HpglIndMaskedArray(C.Structure):
+    _fields_ = [("data", C.POINTER(C.c_ubyte)), ("mask", C.POINTER(C.c_ubyte)), ("shape", HpglShape),
+                ("indicator_count", C.c_int)]
+
+
+class HpglIkParams(C.Structure):
+    _fields_ = [("covariance_type", C.c_int), ("ranges", C.c_double * 3), ("angles", C.c_double * 3),
+                ("sill", C.c_double), ("nugget", C.c_double), ("radiuses", C.c_int * 3), ("max_neighbours", C.c_int),
+                ("marginal_prob", C.c_double)]
+
+
+def ik_params_array(params):
+    arr = (HpglIkParams * len(params))()
+    for i, p in enumerate(params):
+        q = arr[i]
+        q.covariance_type = p["cov_type"]
+        q.ranges[:] = p["ranges"]
+        q.angles[:] = p["angles"]
+        q.sill, q.nugget = p["sill"], p["nugget"]
+        q.radiuses[:] = p["radii"]
+        q.max_neighbours = p["max_neighbours"]
+        q.marginal_prob = p.get("marginal_prob", 0.0)
+    return arr
+
+
+def ref_sis(shape, codes, mask, params, seed=1, sim_mask=None, lvm=None, correlogram=False):
+    """The reference's hpgl_sis_simulation / hpgl_sis_simulation_lvm."""
+    ref = reference()
+    sh = _shape(shape)
+    c = np.array(codes, dtype=np.uint8)
+    m = np.array(mask, dtype=np.uint8)
+    K = len(params)
+    arr = HpglIndMaskedArray(_ptr(c, C.c_ubyte), _ptr(m, C.c_ubyte), sh, K)
+    sm_keep = None
+    smp = None
+    if sim_mask is not None:
+        sm_keep = np.ascontiguousarray(sim_mask, dtype=np.uint8)
+        smp = C.byref(HpglUbyteArray(_ptr(sm_keep, C.c_ubyte), sh))
+    ps = ik_params_array(params)
+    if lvm is not None:
+        keep = [np.ascontiguousarray(a, dtype=np.float32) for a in lvm]
+        fa = (HpglFloatArray * K)(*[HpglFloatArray(_ptr(a, C.c_float), sh) for a in keep])
+        ref.hpgl_sis_simulation_lvm(C.byref(arr), ps, fa, K, int(seed), smp, int(correlogram))
+    else:
+        ref.hpgl_sis_simulation(C.byref(arr), ps, K, int(seed), smp)
+    return c, m

@@ -122,11 +122,12 @@ def test_no_gpu_is_an_error_not_a_fallback(native_lib):
     assert e.value.code == N.HPGL_E_CUDA
 
 
-def test_not_provided_entry_points_report(native_lib):
+def test_simulation_entry_points_reject_null_arguments(native_lib):
     L = native_lib
     L.hpgl_sis_simulation(None, None, 0, 0, None)
-    assert L.hpgl_get_last_error() == N.HPGL_E_UNSUPPORTED
-    assert b"not provided" in L.hpgl_get_last_exception_message()
+    assert L.hpgl_get_last_error() == N.HPGL_E_INVALID
+    L.hpgl_sis_simulation_lvm(None, None, None, 2, 0, None, 1)
+    assert L.hpgl_get_last_error() == N.HPGL_E_INVALID
     L.hpgl_sgs_simulation(None, None, None, None, None)
     assert L.hpgl_get_last_error() == N.HPGL_E_INVALID
 
