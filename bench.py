@@ -22,7 +22,10 @@ Metric: kriged nodes/s.
 * ``--impl reference``: that reference CPU path as the timed arm.
 
 ``--workload inc_io``: the INC property file reader and writer instead
-(hpgl_b200/bench_io.py), with the reference's own reader and writer beside.
+(hpgl_b200/bench_io.py), with the reference's own reader and writer beside;
+``--workload variogram``: experimental variograms (hpgl_b200/bench_variogram.py);
+``--workload sgs``: sequential Gaussian and indicator simulation
+(hpgl_b200/bench_sim.py).
 
 Multi-GPU: the path has no exchange step; N ranks (torchrun, one per GPU)
 each krige their own copy of the job ("replicas only", weak scaling).
@@ -173,9 +176,10 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
-    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram"],
+    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs"],
                     help="inc_io: INC property file read/write (hpgl_b200/bench_io.py); variogram: experimental "
-                         "variograms (hpgl_b200/bench_variogram.py); one GPU")
+                         "variograms (hpgl_b200/bench_variogram.py); sgs: sequential Gaussian and indicator "
+                         "simulation (hpgl_b200/bench_sim.py); one GPU")
     args = ap.parse_args()
     if args.workload == "inc_io":
         from hpgl_b200 import bench_io
@@ -183,6 +187,9 @@ def main():
     if args.workload == "variogram":
         from hpgl_b200 import bench_variogram
         return bench_variogram.run(args, ROOT)
+    if args.workload == "sgs":
+        from hpgl_b200 import bench_sim
+        return bench_sim.run(args, ROOT)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)

@@ -680,7 +680,6 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     Group &g = S.groups[0];
     const Plan &P = g.plan;
     SimPath path;
-    std::vector<double> xp;
     try {
         sim_path(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, path);
     } catch (const std::domain_error &e) {
@@ -689,8 +688,15 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
         throw HpglError{HPGL_E_INVALID, e.what()};
     }
     const bool indicator = job.kind == KIND_IK;
-    if (indicator) xp = path.u;  // sample() compares the draw itself
-    else gaussian_quantiles(path.u, xp, host_threads());
+    // per path rank: the draw itself (sample() compares it) or its normal
+    // quantile
+    std::unique_ptr<double[]> quantiles;
+    const double *draws = path.u.data();
+    if (!indicator && !path.u.empty()) {
+        quantiles.reset(new double[path.u.size()]);
+        gaussian_quantiles(path.u.data(), (long long)path.u.size(), quantiles.get(), host_threads());
+        draws = quantiles.get();
+    }
     res.ms_plan = ms_since(t0);
     auto t1 = std::chrono::steady_clock::now();
     cudaStream_t s = C.stream;
@@ -753,7 +759,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
                                    cudaMemcpyHostToDevice, s));
     if (nsim > 0) {
         CUDA_CHECK(cudaMemcpyAsync(scratch + o_nodes, path.nodes.data(), (size_t)nsim * 4, cudaMemcpyHostToDevice, s));
-        CUDA_CHECK(cudaMemcpyAsync(scratch + o_xp, xp.data(), (size_t)nsim * 8, cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(scratch + o_xp, draws, (size_t)nsim * 8, cudaMemcpyHostToDevice, s));
     }
     CUDA_CHECK(cudaMemsetAsync(G.pend, 0, bits_bytes, s));
     CUDA_CHECK(cudaMemsetAsync(G.blocker, 0xff, (size_t)nsim * 4, s));

@@ -24,7 +24,10 @@
 // host threads, because the C library's log and exp define their bits.
 #include "sgs_host.h"
 
+#include "plan.h"
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <stdexcept>
 #include <thread>
@@ -33,29 +36,39 @@ namespace hpgl_b200 {
 
 namespace {
 
+bool is_prime(long long v) {
+    if (v < 2) return false;
+    for (long long d = 2; d * d <= v; ++d)
+        if (v % d == 0) return false;
+    return true;
+}
+
+// The walk x -> (A x + C) mod M and its jumps: an affine map composed with
+// itself (a, c) -> (a a, a c + c) by doubling, all terms below 2^50 for
+// M <= 10^7.
 struct Path {
     long long A = 1, C = 2, M = 1, R = 0;
     Path(long long size, long long seed) {
         M = size;
-        const long long lim = (size > 3 ? size : 3) + 1;
-        std::vector<char> comp((size_t)lim + 1, 0);
-        std::vector<long long> primes;
-        for (long long i = 2; i <= lim; ++i) {
-            if (comp[(size_t)i]) continue;
-            primes.push_back(i);
-            for (long long j = i * i; j <= lim; j += i) comp[(size_t)j] = 1;
+        // A: 1 + the product of the distinct primes dividing size (times 2
+        // when 4 divides it)
+        long long rest = size;
+        for (long long d = 2; d * d <= rest; ++d) {
+            if (rest % d) continue;
+            A *= d;
+            while (rest % d == 0) rest /= d;
         }
-        for (long long p : primes) {
-            if (p > size) break;
-            if (size % p == 0) A *= p;
-        }
+        if (rest > 1) A *= rest;
         if (M % 4 == 0) A *= 2;
         A += 1;
-        size_t idx = 0;
-        while (idx + 1 < primes.size() && primes[idx + 1] <= size / 3) ++idx;
-        for (long long k = (long long)idx; k >= 0; k--) {
-            C = primes[(size_t)k];
-            if (std::floor(double(size) / double(C)) != (double(size) / double(C))) break;
+        // C: the largest prime <= size / 3 that does not divide size; 2 when
+        // there is none (the table's first prime)
+        C = 2;
+        for (long long c = size / 3; c >= 2; --c) {
+            if (size % c != 0 && is_prime(c)) {
+                C = c;
+                break;
+            }
         }
         // path_random_generator_t(int size, int seed) takes the seed as int;
         // a negative one makes the walk leave the grid
@@ -63,10 +76,21 @@ struct Path {
         if (s32 < 0) throw std::invalid_argument("the simulation path is undefined for a negative seed");
         R = s32 % size;
     }
-    long long next() {
-        const long long r = R;
-        R = (A * R + C) % M;
-        return r;
+    long long step(long long x) const { return (A * x + C) % M; }
+    // the position `j` steps after x
+    long long jump(long long x, long long j) const {
+        long long a = A % M, c = C % M;  // the map of 2^i steps
+        long long ja = 1, jc = 0;          // the map of the steps taken so far
+        while (j > 0) {
+            if (j & 1) {
+                ja = ja * a % M;
+                jc = (a * jc + c) % M;
+            }
+            c = (a * c + c) % M;
+            a = a * a % M;
+            j >>= 1;
+        }
+        return (ja * x + jc) % M;
     }
 };
 
@@ -83,11 +107,16 @@ struct Mt11213b {
     }
     uint32_t next() {
         if (i >= N) {
+            // the in-place twist, its index wrap-around split into three runs
             const uint32_t upper = ~((1u << R) - 1u), lower = (1u << R) - 1u;
-            for (int k = 0; k < N; ++k) {
-                const uint32_t y = (x[k] & upper) | (x[(k + 1) % N] & lower);
-                x[k] = x[(k + M) % N] ^ (y >> 1) ^ ((y & 1u) ? 0xccab8ee7u : 0u);
-            }
+            auto twist = [&](int k, int k1, int km) {
+                const uint32_t y = (x[k] & upper) | (x[k1] & lower);
+                x[k] = x[km] ^ (y >> 1) ^ ((y & 1u) ? 0xccab8ee7u : 0u);
+            };
+            int k = 0;
+            for (; k < N - M; ++k) twist(k, k + 1, k + M);
+            for (; k < N - 1; ++k) twist(k, k + 1, k + M - N);
+            twist(N - 1, 0, M - 1);
             i = 0;
         }
         uint32_t y = x[i++];
@@ -177,22 +206,47 @@ void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_ma
     if (size <= 0) return;
     if (size > 10000000LL)
         throw std::domain_error("the simulation path is defined for grids of at most 10^7 nodes");
-    Path path(size, seed);
-    long long node = path.next();
-    for (long long counter = 0; counter < size; ++counter, node = path.next()) {
-        if (mask[node]) continue;
-        if (sim_mask && sim_mask[node] != 1) continue;
-        out.nodes.push_back((int)node);
+    const Path path(size, seed);
+    // the draws do not depend on the walk: one thread runs the generator
+    // while the others walk their stretches of the path (from jumps)
+    std::vector<double> u;
+    std::atomic<long long> needed{size};
+    std::thread draws([&] {
+        Mt11213b gen((uint32_t)seed);
+        u.reserve((size_t)size);
+        for (long long k = 0; k < needed.load(std::memory_order_relaxed); ++k)
+            u.push_back(double(gen.next()) / double(0xffffffffu));
+    });
+    const int t = (int)std::max<long long>(1, std::min<long long>(host_threads(), size / (1 << 16)));
+    std::vector<std::vector<int>> part((size_t)t);
+    const long long per = (size + t - 1) / t;
+    std::vector<std::thread> pool;
+    for (int i = 0; i < t; ++i) {
+        pool.emplace_back([&, i] {
+            const long long a = i * per, b = std::min(size, a + per);
+            long long x = path.jump(path.R, a);
+            std::vector<int> &v = part[(size_t)i];
+            for (long long k = a; k < b; ++k, x = path.step(x)) {
+                if (mask[x]) continue;
+                if (sim_mask && sim_mask[x] != 1) continue;
+                v.push_back((int)x);
+            }
+        });
     }
-    Mt11213b gen((uint32_t)seed);
-    out.u.resize(out.nodes.size());
-    for (size_t k = 0; k < out.nodes.size(); ++k) out.u[k] = double(gen.next()) / double(0xffffffffu);
+    for (auto &th : pool) th.join();
+    size_t count = 0;
+    for (auto &v : part) count += v.size();
+    needed = (long long)count;
+    out.nodes.reserve(count);
+    for (auto &v : part) out.nodes.insert(out.nodes.end(), v.begin(), v.end());
+    draws.join();
+    u.resize(count);
+    out.u.swap(u);
 }
 
-void gaussian_quantiles(const std::vector<double> &u, std::vector<double> &xp, int threads) {
-    xp.resize(u.size());
-    parallel_for((long long)u.size(), threads, [&](long long a, long long b) {
-        for (long long k = a; k < b; ++k) xp[(size_t)k] = quantile(u[(size_t)k]);
+void gaussian_quantiles(const double *u, long long n, double *xp, int threads) {
+    parallel_for(n, threads, [&](long long a, long long b) {
+        for (long long k = a; k < b; ++k) xp[k] = quantile(u[k]);
     });
 }
 

@@ -19,8 +19,9 @@ struct SimPath {
 // negative.
 void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out);
 
-// xp[k] = the standard normal quantile of u[k] (gaussian_cdf_t::inverse).
-void gaussian_quantiles(const std::vector<double> &u, std::vector<double> &xp, int threads);
+// xp[k] = the standard normal quantile of u[k] (gaussian_cdf_t::inverse),
+// k < n.
+void gaussian_quantiles(const double *u, long long n, double *xp, int threads);
 
 // A caller's non-parametric CDF (hpgl_non_parametric_cdf_t): `size` values in
 // increasing order and their cumulative probabilities.

@@ -222,9 +222,14 @@ void hpgl_write_gslib_cont_property(hpgl_cont_masked_array_t *data, const char *
 void hpgl_write_gslib_byte_property(hpgl_ind_masked_array_t *data, const char *filename, const char *name,
                                     double undefined_value, unsigned char *values, int values_count);
 
-/* api.h:253-265, 279-309.  Sequential simulation, outside this build: each
-   records "not provided by this build" in the last-error state and returns
-   without touching its buffers. */
+/* api.h:253-265, 279-309.  Sequential Gaussian simulation (in place on the
+   property; `cdf` optional: the normal-score transform around it; `mean`
+   unused, simple kriging runs with mean 0, as in the reference) and
+   sequential indicator simulation (in place on the codes; one params entry
+   per category; the LVM form takes a mean array per category and, with
+   use_correlograms, the correlogram weights).  `simulation_mask` optional:
+   1 in the cells to simulate.  Results identical to the reference's; grids
+   above 10^7 nodes and seeds negative as an int are refused. */
 void hpgl_sgs_simulation(hpgl_cont_masked_array_t *prop, hpgl_sgs_params_t *params, hpgl_non_parametric_cdf_t *cdf,
                          double *mean, hpgl_ubyte_array_t *simulation_mask);
 void hpgl_sgs_lvm_simulation(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params,

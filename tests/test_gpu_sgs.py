@@ -154,3 +154,45 @@ def test_window_bounds_do_not_change_results(native_lib):
         assert _same(r["out"], runs[0]["out"]) and np.array_equal(r["out_mask"], runs[0]["out_mask"])
     assert runs[0]["rounds"] < 1000
     assert int(runs[0]["out_mask"].sum()) == job["values"].size
+
+
+@pytest.mark.parametrize("path", __import__("sim_golden").paths("sgs"), ids=lambda p: p.split("/")[-1])
+def test_gpu_matches_golden(native_lib, path):
+    # through the reference's C entry points (the CDF transforms included)
+    import sim_golden as SG
+    d = SG.load(path)
+    kw = SG.sgs_kwargs(d)
+    values = np.array(d["values"], np.float32)
+    mask = np.array(d["mask"], np.uint8)
+    sh = O._shape(d["shape"])
+    arr = O.HpglContArray(values.ctypes.data_as(C.POINTER(C.c_float)), mask.ctypes.data_as(C.POINTER(C.c_ubyte)), sh)
+    p = d["params"][0]
+    q = O.HpglSgsParams()
+    q.covariance_type = p["cov_type"]
+    q.ranges[:] = p["ranges"]
+    q.angles[:] = p["angles"]
+    q.sill, q.nugget = p["sill"], p["nugget"]
+    q.radiuses[:] = p["radii"]
+    q.max_neighbours = p["max_neighbours"]
+    q.kriging_kind = 0 if kw["ordinary"] else 1
+    q.seed = kw["seed"]
+    keep = []
+    cdfp = smp = None
+    if "cdf" in kw:
+        cv, cp = (np.ascontiguousarray(a, np.float32) for a in kw["cdf"])
+        keep += [cv, cp]
+        cdfp = C.byref(O.HpglNonParametricCdf(cv.ctypes.data_as(C.POINTER(C.c_float)),
+                                              cp.ctypes.data_as(C.POINTER(C.c_float)), cv.size))
+    if "sim_mask" in kw:
+        sm = np.ascontiguousarray(kw["sim_mask"], np.uint8)
+        keep.append(sm)
+        smp = C.byref(O.HpglUbyteArray(sm.ctypes.data_as(C.POINTER(C.c_ubyte)), sh))
+    if "lvm" in kw:
+        lv = np.ascontiguousarray(kw["lvm"], np.float32)
+        keep.append(lv)
+        fa = O.HpglFloatArray(lv.ctypes.data_as(C.POINTER(C.c_float)), sh)
+        native_lib.hpgl_sgs_lvm_simulation(C.byref(arr), C.byref(q), cdfp, C.byref(fa), smp)
+    else:
+        native_lib.hpgl_sgs_simulation(C.byref(arr), C.byref(q), cdfp, None, smp)
+    assert native_lib.hpgl_get_last_error() == 0
+    assert _same(values, d["out_values"]) and np.array_equal(mask, d["out_mask"])

@@ -87,3 +87,35 @@ def test_sis_window_does_not_change_results(native_lib):
     finally:
         native_lib.hpgl_b200_set_sim_window(0)
     assert np.array_equal(runs[0]["out"], runs[1]["out"]) and runs[0]["out_mask"].all()
+
+
+@pytest.mark.parametrize("lvm", [False, True])
+def test_geo_bsd_sis_simulation(native_lib, lvm):
+    from hpgl_b200.geo_bsd import geo, sis
+    c = case(shape=(20, 16, 8), K=3, seed=17)
+    ps = params(3)
+    nx, ny, nz = c["shape"]
+    f = lambda a: np.asfortranarray(np.reshape(a, c["shape"], order="F"))
+    prop = (f(c["codes"]), f(c["mask"]), 3)
+    data = [{"cov_model": geo.CovarianceModel(type=p["cov_type"], ranges=p["ranges"], angles=p["angles"],
+                                               sill=p["sill"], nugget=p["nugget"]),
+             "radiuses": p["radii"], "max_neighbours": p["max_neighbours"]} for p in ps]
+    if lvm:
+        lv = means(c["shape"], 3, seed=18)
+        out = sis.sis_simulation(prop, geo.SugarboxGrid(nx, ny, nz), data, 555, [f(a) for a in lv])
+        want = O.sis(c["shape"], c["codes"], c["mask"], [dict(p, marginal_prob=0.0) for p in ps], seed=555, lvm=lv,
+                     correlogram=True)
+    else:
+        out = sis.sis_simulation(prop, geo.SugarboxGrid(nx, ny, nz), data, 555, [p["marginal_prob"] for p in ps])
+        want = O.sis(c["shape"], c["codes"], c["mask"], ps, seed=555)
+    assert np.array_equal(out.data.ravel(order="F"), want[0]) and np.array_equal(out.mask.ravel(order="F"), want[1])
+
+
+@pytest.mark.parametrize("path", __import__("sim_golden").paths("sis"), ids=lambda p: p.split("/")[-1])
+def test_gpu_matches_golden(native_lib, path):
+    import sim_golden as SG
+    d = SG.load(path)
+    job = dict(shape=d["shape"], codes=d["codes"], mask=d["mask"], values=None, kind="ik", params=d["params"])
+    r = N.simulate_indicator(job, d["seed"], category_means=list(d["lvm"]) if "lvm" in d else None,
+                             correlogram=bool(d["correlogram"]))
+    assert np.array_equal(r["out"], d["out_codes"]) and np.array_equal(r["out_mask"], d["out_mask"])

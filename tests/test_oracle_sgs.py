@@ -94,3 +94,12 @@ def test_cdf_transform_round_trip_is_close():
     g = O.cdf_transform(x, cdf, 0)
     back = O.cdf_transform(g, cdf, 1)
     assert np.allclose(back, x, atol=2e-3)
+
+
+@pytest.mark.parametrize("path", __import__("sim_golden").paths("sgs"), ids=lambda p: p.split("/")[-1])
+def test_oracle_matches_golden(path):
+    import sim_golden as SG
+    d = SG.load(path)
+    job = dict(shape=d["shape"], values=d["values"], mask=d["mask"], params=d["params"])
+    v, m, _ = O.sgs(job, **SG.sgs_kwargs(d))
+    assert np.array_equal(v.view(np.uint32), d["out_values"].view(np.uint32)) and np.array_equal(m, d["out_mask"])

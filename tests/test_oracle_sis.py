@@ -50,3 +50,12 @@ def test_informed_codes_are_kept_and_every_node_simulated():
     codes, mask = O.sis(c["shape"], c["codes"], c["mask"], params(3), seed=5)
     inf = c["mask"] != 0
     assert mask.all() and np.array_equal(codes[inf], c["codes"][inf]) and codes.max() < 3
+
+
+@pytest.mark.parametrize("path", __import__("sim_golden").paths("sis"), ids=lambda p: p.split("/")[-1])
+def test_oracle_matches_golden(path):
+    import sim_golden as SG
+    d = SG.load(path)
+    codes, mask = O.sis(d["shape"], d["codes"], d["mask"], d["params"], seed=d["seed"],
+                        lvm=list(d["lvm"]) if "lvm" in d else None, correlogram=bool(d["correlogram"]))
+    assert np.array_equal(codes, d["out_codes"]) and np.array_equal(mask, d["out_mask"])
