@@ -387,6 +387,7 @@ __global__ void __launch_bounds__(256) k_sgs_commit(DevJob J, DevPlan P, SgsStat
         ctl->commits += count - kept;
     }
     ctl->blocks_done = 0;
+    ctl->cursor = 0;
 }
 
 // Appends the admitted path ranks to window buffer `buf` and marks them

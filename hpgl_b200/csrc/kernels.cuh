@@ -171,6 +171,7 @@ struct SgsCtl {
     int count[2];           // pending nodes in window buffer 0 / 1
     int window;             // window size (pending nodes per round)
     unsigned blocks_done;   // commit kernel: blocks finished
+    unsigned cursor;        // try kernels: next window slot to hand out
     long long next;         // next path rank to admit
     long long total;        // path length
     long long admit_base;   // window slot of the first admitted node

@@ -29,13 +29,21 @@ constexpr int WARPS32 = 4;
 constexpr float MIXED_PIVOT_MIN = 1e-3f;  // on the unit-diagonal scaled system
 constexpr int MIXED_MAX_CORR = 4;
 
-struct SysSmem {
-    double A[N32 * 34];     // exact: in-place factor (column k at k*34); mixed: full system (LD 33)
+// Per-warp shared memory; NA doubles of system storage (the exact path uses
+// columns of 34: NC * 34 for systems of at most NC neighbours).
+template <int NA>
+struct SysSmemN {
+    double A[NA];           // exact: in-place factor (column k at k*34); mixed: full system (LD 33)
     double vd[N32];         // double vector broadcast
     float vf[2][N32];       // float vector broadcast
     float row[2][N32];      // mixed: pivot row broadcast (double buffered)
     int4 nb[N32];           // neighbour offsets from the node (x, y, z, table offset)
 };
+using SysSmem = SysSmemN<N32 * 34>;
+// systems of at most 16 neighbours (sequential simulation): half the
+// registers and shared memory, twice the warps per SM
+constexpr int N16 = 16;
+using SysSmem16 = SysSmemN<N16 * 34>;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -58,7 +66,8 @@ struct NodeData {
     int ox, oy, oz, lin;  // offset of neighbour `lane` from the node, and its table offset
 };
 
-__device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &f,
+template <typename SM>
+__device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P, SM &S, const NodeFetch &f,
                                               int lane) {
     NodeData d;
     const int node = f.node;
@@ -180,7 +189,8 @@ __device__ __forceinline__ double seq_dsum(double init, double term, int n, doub
 // The estimate sums run on lane 0 in neighbour order (combiner.h:9-24:
 // float terms summed in float; median IK in double), which is also the only
 // lane that stores them.
-__device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane,
+template <typename SM>
+__device__ __forceinline__ void write_outputs(const DevJob &J, const DevPlan &P, SM &S, int node, int lane,
                                               const NodeData &d, int status, double w, double variance) {
     const long long slot = (long long)node * J.status_stride + J.status_offset;
     const bool success = status == ST_SUCCESS;
@@ -266,15 +276,15 @@ __device__ __noinline__ double drcp_rn(double a) { return __drcp_rn(a); }
 // registers.  CORR scales entry (i, k) by sg_k sg_i, sg the lanes' sigma
 // (corellogramed_weights_3, my_kriging_weights.h:308-317; b is scaled by the
 // caller).
-template <bool CORR>
-__device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, SysSmem &S, int lane, const NodeData &d,
+template <bool CORR, int NC = N32, typename SM>
+__device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, SM &S, int lane, const NodeData &d,
                                           double sg, double &w_out) {
     constexpr int LD = 34;
     const int n = d.n;
     const bool ordinary = J.kind == 0;
-    double c[N32];
+    double c[NC];
 #pragma unroll
-    for (int i = 0; i < N32; ++i) {
+    for (int i = 0; i < NC; ++i) {
         // A(i, lane) = C(x_i - x_lane) for i <= lane (my_kriging_weights.h:53)
         const int ix = __shfl_sync(FULL_MASK, d.ox, i), iy = __shfl_sync(FULL_MASK, d.oy, i);
         const int iz = __shfl_sync(FULL_MASK, d.oz, i), il = __shfl_sync(FULL_MASK, d.lin, i);
@@ -291,7 +301,7 @@ __device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, Sys
     int info = 0;
     double my_rcp = 0.0;  // RN(1/U(lane,lane))
 #pragma unroll
-    for (int j = 0; j < N32; ++j) {
+    for (int j = 0; j < NC; ++j) {
         if (j >= n) break;
         double t = 0.0;
         const double2 *cj = reinterpret_cast<const double2 *>(S.A + j * LD);
@@ -321,7 +331,7 @@ __device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, Sys
             break;
         }
         rinv = __shfl_sync(FULL_MASK, rinv, j);
-        if (lane > j) {
+        if (lane > j && lane < NC) {  // the lane's column exists (NC * 34 doubles of S.A)
             double v = c[j];
             if (j > 0) v = __dadd_rn(v, -t);
             v = __dmul_rn(rinv, v);
@@ -338,7 +348,7 @@ __device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, Sys
         // DPOTRS 'U': U^T y = b (dot form, k ascending), then U x = y (column form).
         double xa = d.b, xb = 1.0;
 #pragma unroll
-        for (int i = 0; i < N32; ++i) {
+        for (int i = 0; i < NC; ++i) {
             if (i >= n) break;
             double ya = 0.0, yb = 0.0;
             if (lane == i) {
@@ -388,12 +398,13 @@ __device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, Sys
 }
 
 // Solves and writes the outputs of one system.
-__device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, SysSmem &S, int node, int lane,
+template <int NC = N32, typename SM>
+__device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, SM &S, int node, int lane,
                                              const NodeData &d) {
     const int n = d.n;
     const bool ordinary = J.kind == 0;
     double w;
-    const int status = exact_core<false>(J, P, S, lane, d, 0.0, w);
+    const int status = exact_core<false, NC>(J, P, S, lane, d, 0.0, w);
     double variance = -1.0;
     if (J.variance && status == ST_SUCCESS) {
         // c0 - p_0 - p_1 - ... (my_kriging_weights.h): subtracting p is adding -p
@@ -405,7 +416,8 @@ __device__ __forceinline__ void exact_system(const DevJob &J, const DevPlan &P, 
 }
 
 // One node of the exact path; returns whether a system was solved.
-__device__ __forceinline__ bool exact32_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &cur,
+template <int NC = N32, typename SM>
+__device__ __forceinline__ bool exact32_node(const DevJob &J, const DevPlan &P, SM &S, const NodeFetch &cur,
                                              int lane) {
     if (copy_informed(J, cur, lane)) return false;
     const NodeData d = load_node(J, P, S, cur, lane);
@@ -413,7 +425,7 @@ __device__ __forceinline__ bool exact32_node(const DevJob &J, const DevPlan &P, 
         write_outputs(J, P, S, cur.node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
         return false;
     }
-    exact_system(J, P, S, cur.node, lane, d);
+    exact_system<NC>(J, P, S, cur.node, lane, d);
     return true;
 }
 
@@ -640,13 +652,20 @@ constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
 // One speculative round of sequential simulation (at most 32 neighbours):
 // one warp per pending node of window buffer `cur`: the template search with
 // conflict detection, the exact FP64 system and the simulated value.
+template <int NC>
 __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P, SgsState G, int cur) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    using SM = SysSmemN<NC * 34>;
+    SM &S = reinterpret_cast<SM *>(dyn_smem)[warp];
     const int count = G.ctl->count[cur];
     const int *win = cur ? G.win1 : G.win0;
-    for (int base = (blockIdx.x * WARPS32 + warp) * 32; base < count; base += gridDim.x * WARPS32 * 32) {
+    // window slots are handed out 32 at a time as warps free up
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (base >= count) break;
         int my_rank;
         unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
         if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
@@ -661,7 +680,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P,
             __syncwarp();
             if (blocker < 0) {
                 const NodeFetch f = fetch_node(J, P, node, lane);
-                exact32_node(J, P, S, f, lane);
+                exact32_node<NC>(J, P, S, f, lane);
                 __syncwarp();
                 if (lane == 0) sgs_value(J, node, G.xp[rank]);
             }
@@ -680,7 +699,8 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P,
 // Row `lane` of category k's system: dv = indicator - mean of the neighbour
 // (float, combiner.h:18-22), b = C(x_lane - x0), scaled by sg sgc with the
 // correlogram weights (sg: the neighbour's sigma).
-__device__ __forceinline__ NodeData sis_load32(const DevJob &J, const DevPlan &P, SysSmem &S, int node,
+template <typename SM>
+__device__ __forceinline__ NodeData sis_load32(const DevJob &J, const DevPlan &P, SM &S, int node,
                                                const int *list, int n, int k, double sgc, int lane, double &sg) {
     NodeData d;
     d.n = n;
@@ -723,14 +743,21 @@ __device__ __forceinline__ NodeData sis_load32(const DevJob &J, const DevPlan &P
 // (kriging_interpolation.h:228-265 with a double result), the mean when the
 // kriging fails.  Two categories krige category 0 only and take 1 - p for
 // the other (median SIS).  The code is drawn from the float probabilities.
+template <int NC>
 __global__ void __launch_bounds__(WARPS32 * 32) k_sis_try32(DevJob J, const DevPlan *plans, SgsState G, int cur) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
+    using SM = SysSmemN<NC * 34>;
+    SM &S = reinterpret_cast<SM *>(dyn_smem)[warp];
     const int count = G.ctl->count[cur];
     const int *win = cur ? G.win1 : G.win0;
     const int cats = J.K == 2 ? 1 : J.K;
-    for (int base = (blockIdx.x * WARPS32 + warp) * 32; base < count; base += gridDim.x * WARPS32 * 32) {
+    // window slots are handed out 32 at a time as warps free up
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (base >= count) break;
         int my_rank;
         unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
         if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
@@ -754,8 +781,8 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sis_try32(DevJob J, const DevP
                     const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
                     double sg, w;
                     const NodeData d = sis_load32(J, P, S, node, list, cnt, k, sgc, lane, sg);
-                    const int status = J.sis_corr ? exact_core<true>(J, P, S, lane, d, sg, w)
-                                                  : exact_core<false>(J, P, S, lane, d, 0.0, w);
+                    const int status = J.sis_corr ? exact_core<true, NC>(J, P, S, lane, d, sg, w)
+                                                  : exact_core<false, NC>(J, P, S, lane, d, 0.0, w);
                     if (status == ST_SUCCESS)
                         prob = seq_dsum((double)mc, __dmul_rn(w, (double)d.dv), cnt, S.vd, lane);
                 }
@@ -774,13 +801,25 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sis_try32(DevJob J, const DevP
 }  // namespace
 
 void launch_sgs_try32(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
-    const long long g = persistent_grid((const void *)k_sgs_try32, WARPS32 * 32, SMEM32, 0, 1LL << 30);
-    k_sgs_try32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, P, G, cur);
+    if (P.nmax <= N16) {
+        constexpr size_t smem = sizeof(SysSmem16) * WARPS32;
+        const long long g = persistent_grid((const void *)k_sgs_try32<N16>, WARPS32 * 32, smem, 0, 1LL << 30);
+        k_sgs_try32<N16><<<(unsigned)g, WARPS32 * 32, smem, s>>>(J, P, G, cur);
+        return;
+    }
+    const long long g = persistent_grid((const void *)k_sgs_try32<N32>, WARPS32 * 32, SMEM32, 0, 1LL << 30);
+    k_sgs_try32<N32><<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, P, G, cur);
 }
 
 void launch_sis_try32(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s) {
-    const long long g = persistent_grid((const void *)k_sis_try32, WARPS32 * 32, SMEM32, 0, 1LL << 30);
-    k_sis_try32<<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, plans, G, cur);
+    if (J.nb_stride <= N16) {
+        constexpr size_t smem = sizeof(SysSmem16) * WARPS32;
+        const long long g = persistent_grid((const void *)k_sis_try32<N16>, WARPS32 * 32, smem, 0, 1LL << 30);
+        k_sis_try32<N16><<<(unsigned)g, WARPS32 * 32, smem, s>>>(J, plans, G, cur);
+        return;
+    }
+    const long long g = persistent_grid((const void *)k_sis_try32<N32>, WARPS32 * 32, SMEM32, 0, 1LL << 30);
+    k_sis_try32<N32><<<(unsigned)g, WARPS32 * 32, SMEM32, s>>>(J, plans, G, cur);
 }
 
 void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream_t s, int blocks_per_sm) {

@@ -460,7 +460,12 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs_try64(DevJob J, DevP
     Exact64Smem &S = reinterpret_cast<Exact64Smem *>(dyn_smem)[warp];
     const int count = G.ctl->count[cur];
     const int *win = cur ? G.win1 : G.win0;
-    for (int base = (blockIdx.x * WARPS64_BLOCK + warp) * 32; base < count; base += gridDim.x * WARPS64_BLOCK * 32) {
+    // window slots are handed out 32 at a time as warps free up
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (base >= count) break;
         int my_rank;
         unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
         if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
@@ -867,7 +872,12 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sis_try64(DevJob J, cons
     const int count = G.ctl->count[cur];
     const int *win = cur ? G.win1 : G.win0;
     const int cats = J.K == 2 ? 1 : J.K;
-    for (int base = (blockIdx.x * WARPS64_BLOCK + warp) * 32; base < count; base += gridDim.x * WARPS64_BLOCK * 32) {
+    // window slots are handed out 32 at a time as warps free up
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (base >= count) break;
         int my_rank;
         unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
         if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
