@@ -160,10 +160,49 @@ void parallel_for(long long n, int threads, F f) {
     for (auto &th : pool) th.join();
 }
 
+// std::lower_bound over a sorted float array, narrowed by buckets of its
+// range: thresholds t[0] <= ... <= t[nb] (floats) and lo[b] = lower_bound(t[b]).
+// A query v with t[b] <= v < t[b + 1] has its lower bound in [lo[b], lo[b + 1]]:
+// everything before lo[b] is below t[b] <= v, and the element at lo[b + 1] is
+// >= t[b + 1] > v.  Queries outside [t[0], t[nb]), NaN, and arrays holding a
+// NaN take the whole range.  The result is std::lower_bound's.
+struct SortedIndex {
+    const float *a;
+    long long n;
+    int nb = 0;
+    double base = 0, scale = 0;
+    std::vector<float> t;
+    std::vector<int> lo;
+    SortedIndex(const float *arr, long long count, int buckets) : a(arr), n(count) {
+        if (n < 2 || n > 0x7fffffffLL) return;
+        for (long long i = 0; i < n; ++i)
+            if (!std::isfinite(a[i])) return;
+        const double v0 = a[0], v1 = a[n - 1];
+        if (!(v1 > v0)) return;
+        nb = buckets;
+        base = v0;
+        scale = nb / (v1 - v0);
+        t.resize((size_t)nb + 1);
+        lo.resize((size_t)nb + 1);
+        for (int b = 0; b <= nb; ++b) {
+            t[b] = (float)(v0 + b / scale);
+            if (b > 0 && t[b] < t[b - 1]) t[b] = t[b - 1];
+            lo[b] = (int)(std::lower_bound(a, a + n, t[b]) - a);
+        }
+    }
+    const float *lower_bound(float v) const {
+        if (nb == 0 || !(v >= t[0] && v < t[nb])) return std::lower_bound(a, a + n, v);
+        int b = (int)((v - base) * scale);
+        b = std::min(std::max(b, 0), nb - 1);
+        while (b > 0 && v < t[b]) --b;
+        while (b + 1 < nb && v >= t[b + 1]) ++b;
+        return std::lower_bound(a + lo[b], a + lo[b + 1], v);
+    }
+};
+
 // non_parametric_cdf_2_t::operator() (non_parametric_cdf.h:202-228): float
-// interpolation between the bracketing values.
-float npcdf_prob(const NonParametricCdf &c, float value) {
-    const float *it = std::lower_bound(c.values, c.values + c.size, value);
+// interpolation between the bracketing values; it = lower_bound(values, value).
+float npcdf_prob_at(const NonParametricCdf &c, float value, const float *it) {
     if (it == c.values + c.size) return c.probs[c.size - 1];
     if (it == c.values) return c.probs[0];
     const long long i2 = it - c.values, i1 = i2 - 1;
@@ -171,10 +210,10 @@ float npcdf_prob(const NonParametricCdf &c, float value) {
     return y1 + (y2 - y1) / (x2 - x1) * (value - x1);
 }
 
-// non_parametric_cdf_2_t::inverse (non_parametric_cdf.h:230-257).
-float npcdf_inverse(const NonParametricCdf &c, float prob) {
+// non_parametric_cdf_2_t::inverse (non_parametric_cdf.h:230-257), given
+// it = lower_bound(probs, prob).
+float npcdf_inverse_at(const NonParametricCdf &c, float prob, const float *it) {
     if (c.size <= 0) return 0;
-    const float *it = std::lower_bound(c.probs, c.probs + c.size, prob);
     if (it == c.probs) return c.values[0];
     if (it == c.probs + c.size) return c.values[c.size - 1];
     const long long i2 = it - c.probs, i1 = i2 - 1;
@@ -252,21 +291,23 @@ void gaussian_quantiles(const double *u, long long n, double *xp, int threads) {
 
 void cdf_to_gaussian(const NonParametricCdf &cdf, const float *in, float *out, const uint8_t *mask, long long n,
                      int threads) {
+    const SortedIndex index(cdf.values, cdf.size, 1 << 16);
     parallel_for(n, threads, [&](long long a, long long b) {
         for (long long i = a; i < b; ++i) {
             if (mask && !mask[i]) continue;
-            const double P = npcdf_prob(cdf, in[i]);
+            const double P = npcdf_prob_at(cdf, in[i], index.lower_bound(in[i]));
             out[i] = (float)(quantile(P) * std::sqrt(1.0) + 0.0);
         }
     });
 }
 
 void gaussian_to_cdf(const NonParametricCdf &cdf, float *values, const uint8_t *mask, long long n, int threads) {
+    const SortedIndex index(cdf.probs, cdf.size, 1 << 16);
     parallel_for(n, threads, [&](long long a, long long b) {
         for (long long i = a; i < b; ++i) {
             if (!mask[i]) continue;
-            const double P = gaussian_prob(values[i]);
-            values[i] = npcdf_inverse(cdf, (float)P);
+            const float p = (float)gaussian_prob(values[i]);
+            values[i] = npcdf_inverse_at(cdf, p, index.lower_bound(p));
         }
     });
 }
