@@ -600,6 +600,14 @@ static void sgs_call(hpgl_cont_masked_array_t *data, hpgl_sgs_params_t *params, 
     if (!data || !params) throw HpglError{HPGL_E_INVALID, "data or params are null"};
     if (!data->m_data || !data->m_mask) throw HpglError{HPGL_E_INVALID, "property arrays are null"};
     const long long n = volume(&data->m_shape);
+    // refuse what the path cannot do before the CDF transform touches the data
+    try {
+        check_sim_path(n, params->m_seed);
+    } catch (const std::domain_error &e) {
+        throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
+    } catch (const std::invalid_argument &e) {
+        throw HpglError{HPGL_E_INVALID, e.what()};
+    }
     NonParametricCdf c{nullptr, nullptr, 0};
     std::vector<float> gaussian_mean;
     if (cdf) {

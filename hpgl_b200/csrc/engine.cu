@@ -716,7 +716,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     const size_t o_ctl = take(sizeof(SgsCtl)), o_nodes = take((size_t)nsim * 4), o_xp = take((size_t)nsim * 8),
                  o_rank = take((size_t)S.size * 4), o_pend = take(bits_bytes), o_blocker = take((size_t)nsim * 4),
                  o_done = take((size_t)nsim), o_w0 = take((size_t)window * 4), o_w1 = take((size_t)window * 4),
-                 o_ok = take((size_t)window);
+                 o_ok = take((size_t)window), o_try = take((size_t)window * 4);
     unsigned char *scratch = nullptr;
     CUDA_CHECK(cudaMalloc(&scratch, off));
     struct Free {
@@ -734,6 +734,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     G.win0 = reinterpret_cast<int *>(scratch + o_w0);
     G.win1 = reinterpret_cast<int *>(scratch + o_w1);
     G.ok = scratch + o_ok;
+    G.trylist = reinterpret_cast<int *>(scratch + o_try);
     // indicator simulation: every category's plan (a category shares its
     // group's)
     DevPlan *d_plans = nullptr;

@@ -331,6 +331,31 @@ __device__ __forceinline__ void sgs_bit(const DevJob &J, const DevPlan &P, int n
     bit = 1u << (px & 31);
 }
 
+// The round's try list: the pending nodes of window buffer `cur` without a
+// blocker or whose blocker has committed (one counter update per warp); the
+// others stay pending untried.
+__global__ void __launch_bounds__(256) k_sgs_list(SgsState G, int cur) {
+    SgsCtl *ctl = G.ctl;
+    const int count = ctl->count[cur];
+    const int *win = cur ? G.win1 : G.win0;
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += stride) {
+        const int i = base + lane;
+        bool tr = false;
+        if (i < count) {
+            const int b = G.blocker[win[i]];
+            tr = b < 0 || G.done[b];
+            if (!tr) G.ok[i] = 0;
+        }
+        const unsigned m = __ballot_sync(FULL_MASK, tr);
+        int slot0 = 0;
+        if (lane == 0 && m) slot0 = atomicAdd(&ctl->ntry, __popc(m));
+        slot0 = __shfl_sync(FULL_MASK, slot0, 0);
+        if (tr) G.trylist[slot0 + __popc(m & ((1u << lane) - 1u))] = i;
+    }
+}
+
 // Commits the nodes of window buffer `cur` that the round kept (informed bit
 // set, pending bit cleared, done) and moves the others to the other buffer
 // (one counter update per warp).  The last block to finish (a ticket
@@ -386,6 +411,8 @@ __global__ void __launch_bounds__(256) k_sgs_commit(DevJob J, DevPlan P, SgsStat
         ctl->rounds += 1;
         ctl->commits += count - kept;
     }
+    ctl->tries += ctl->ntry;
+    ctl->ntry = 0;
     ctl->blocks_done = 0;
     ctl->cursor = 0;
 }
@@ -423,14 +450,20 @@ void launch_sgs_admit(const DevJob &J, const DevPlan &P, const SgsState &G, int 
     sgs_commit_admit(J, P, G, cur, s);
 }
 
+static void sgs_list(const SgsState &G, int cur, cudaStream_t s) {
+    k_sgs_list<<<(unsigned)sm_count() * 4, 256, 0, s>>>(G, cur);
+}
+
 void launch_sis_round(const DevJob &J, const DevPlan &P0, const DevPlan *plans, int family, const SgsState &G,
                       int cur, cudaStream_t s) {
+    sgs_list(G, cur, s);
     if (family == 0) launch_sis_try32(J, plans, G, cur, s);
     else launch_sis_try64(J, plans, G, cur, s);
     sgs_commit_admit(J, P0, G, cur, s);
 }
 
 void launch_sgs_round(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
+    sgs_list(G, cur, s);
     if (P.nmax <= 32) launch_sgs_try32(J, P, G, cur, s);
     else launch_sgs_try64(J, P, G, cur, s);
     sgs_commit_admit(J, P, G, cur, s);

@@ -171,7 +171,8 @@ struct SgsCtl {
     int count[2];           // pending nodes in window buffer 0 / 1
     int window;             // window size (pending nodes per round)
     unsigned blocks_done;   // commit kernel: blocks finished
-    unsigned cursor;        // try kernels: next window slot to hand out
+    unsigned cursor;        // try kernels: next entry of the try list to hand out
+    int ntry;               // entries of this round's try list
     long long next;         // next path rank to admit
     long long total;        // path length
     long long admit_base;   // window slot of the first admitted node
@@ -188,10 +189,12 @@ struct SgsState {
     uint8_t *done;          // per path rank: committed
     int *win0, *win1;       // window buffers (path ranks)
     uint8_t *ok;            // per window slot: the node committed this round
+    int *trylist;           // window slots tried this round (blocker committed or none)
 };
 // rank_of from the mask and the path
 void launch_sgs_ranks(const DevJob &J, const SgsState &G, long long nsim, cudaStream_t s);
-// one round: try the pending nodes of window buffer `cur`, commit, admit
+// one round: list the pending nodes of window buffer `cur` to try, try them,
+// commit, admit
 void launch_sgs_round(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
 void launch_sgs_try32(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);
 void launch_sgs_try64(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s);

@@ -104,15 +104,39 @@ __device__ __forceinline__ void template_node(const DevJob &J, const DevPlan &P,
     if (lane == 0) J.nbcount[node] = min(cnt, nmax);
 }
 
+// One lane's template entry of a speculative search: the informed and
+// pending words of its target cell, loaded ahead of their use.
+struct SpecProbe {
+    int delta;
+    uint32_t bit, inf, pen;  // bit == 0: past the template or outside the grid
+};
+
+__device__ __forceinline__ SpecProbe spec_probe(const DevJob &J, const DevPlan &P, const SgsState &G, int x, int y,
+                                                int z, int t) {
+    SpecProbe q{0, 0u, 0u, 0u};
+    if (t < P.tmpl_len) {
+        const int4 e = __ldg(&P.tmpl[t]);
+        q.delta = e.w;
+        const int yy = y + e.y, zz = z + e.z;
+        if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
+            const int px = x + e.x;  // padded x of the target cell
+            const long long w = ((long long)zz * J.ny + yy) * P.wpr + (px >> 5);
+            q.bit = 1u << (px & 31);
+            q.inf = __ldg(J.bits + w);
+            q.pen = __ldg(G.pend + w);
+        }
+    }
+    return q;
+}
+
 // neighbour_lookup_t::find for one node of a speculative simulation round
 // (path rank `rank`): as template_node, over the committed nodes of lower
 // rank (informed bit set and rank_of below `rank`; informed data have rank
 // -1); the list goes to `out`, its length to `count`.  Returns -1 when the
-// search completed, else the rank of the first
-// pending node of lower rank met before the point where the search would
-// stop: in the sequential order that node would have been simulated and
-// seen, so nothing of this search is kept.  The bits and ranks are read-only
-// while a round's nodes are tried.
+// search completed, else the rank of the first pending node of lower rank met
+// before the point where the search would stop: in the sequential order that
+// node would have been simulated and seen, so nothing of this search is kept.
+// The bits and ranks are read-only while a round's nodes are tried.
 __device__ __forceinline__ int template_node_spec(const DevJob &J, const DevPlan &P, const SgsState &G, int node,
                                                   int rank, int lane, int *out, int &count) {
     int x, y, z;
@@ -120,26 +144,18 @@ __device__ __forceinline__ int template_node_spec(const DevJob &J, const DevPlan
     const int nmax = P.nmax;
     int cnt = 0;
     count = 0;
+    // the next chunk's entries and words are loaded while this chunk's ranks
+    // are read and its hits counted
+    SpecProbe q = spec_probe(J, P, G, x, y, z, lane);
     for (int tb = 0; tb < P.tmpl_len && cnt < nmax; tb += 32) {
-        const int t = tb + lane;
+        const SpecProbe nq = spec_probe(J, P, G, x, y, z, tb + 32 + lane);
         bool hit = false, conflict = false;
-        int delta = 0, r = -1;
-        if (t < P.tmpl_len) {
-            const int4 e = __ldg(&P.tmpl[t]);
-            delta = e.w;
-            const int yy = y + e.y, zz = z + e.z;
-            if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
-                const int px = x + e.x;  // padded x of the target cell
-                const long long w = ((long long)zz * J.ny + yy) * P.wpr + (px >> 5);
-                const uint32_t bit = 1u << (px & 31);
-                const bool inf = (__ldg(J.bits + w) & bit) != 0;
-                const bool pen = (__ldg(G.pend + w) & bit) != 0;
-                if (inf || pen) {  // set bits only inside the grid
-                    r = __ldg(G.rank_of + node + delta);
-                    hit = inf && r < rank;
-                    conflict = pen && r < rank;
-                }
-            }
+        int r = -1;
+        const bool inf = (q.inf & q.bit) != 0, pen = (q.pen & q.bit) != 0;
+        if (inf || pen) {  // set bits only inside the grid
+            r = __ldg(G.rank_of + node + q.delta);
+            hit = inf && r < rank;
+            conflict = pen && r < rank;
         }
         const unsigned b = __ballot_sync(FULL_MASK, hit);
         const unsigned c = __ballot_sync(FULL_MASK, conflict);
@@ -149,28 +165,25 @@ __device__ __forceinline__ int template_node_spec(const DevJob &J, const DevPlan
             if (cnt + __popc(b & ((1u << first) - 1u)) < nmax) return blocker;
         }
         const int pos = __popc(b & ((1u << lane) - 1u));
-        if (hit && cnt + pos < nmax) out[cnt + pos] = node + delta;
+        if (hit && cnt + pos < nmax) out[cnt + pos] = node + q.delta;
         cnt += __popc(b);
+        q = nq;
     }
     count = min(cnt, nmax);
     return -1;
 }
 
-// The pending entries of a round, 32 per warp: lane l holds entry base + l;
-// entries whose blocker has not committed are left alone.  Returns the mask
-// of lanes whose node is tried this round; the others' ok flags are cleared.
-__device__ __forceinline__ unsigned sgs_lanes_to_try(const SgsState &G, const int *win, int count, int base,
-                                                     int lane, int &rank) {
-    const int i = base + lane;
-    bool tr = false;
-    rank = -1;
-    if (i < count) {
-        rank = win[i];
-        const int b = G.blocker[rank];
-        tr = b < 0 || G.done[b];
-        if (!tr) G.ok[i] = 0;
-    }
-    return __ballot_sync(FULL_MASK, tr);
+// The next node to try this round, handed out one at a time from the round's
+// try list: its window slot and path rank; false once the list is used up.
+__device__ __forceinline__ bool sgs_next_try(const SgsState &G, const int *win, int ntry, int lane, int &slot,
+                                             int &rank) {
+    int k = 0;
+    if (lane == 0) k = (int)atomicAdd(&G.ctl->cursor, 1u);
+    k = __shfl_sync(FULL_MASK, k, 0);
+    if (k >= ntry) return false;
+    slot = G.trylist[k];
+    rank = win[slot];
+    return true;
 }
 
 // The simulated value of a kriged node (sequential_simulation.h:106-110,

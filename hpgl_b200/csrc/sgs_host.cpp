@@ -238,13 +238,19 @@ double gaussian_prob(double x) {
 
 }  // namespace
 
+void check_sim_path(long long size, long long seed) {
+    if (size > 10000000LL)
+        throw std::domain_error("the simulation path is defined for grids of at most 10^7 nodes");
+    if ((int)(uint32_t)seed < 0)
+        throw std::invalid_argument("the simulation path is undefined for a negative seed");
+}
+
 void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out) {
     const long long size = (long long)nx * ny * nz;
     out.nodes.clear();
     out.u.clear();
     if (size <= 0) return;
-    if (size > 10000000LL)
-        throw std::domain_error("the simulation path is defined for grids of at most 10^7 nodes");
+    check_sim_path(size, seed);
     const Path path(size, seed);
     // the draws do not depend on the walk: one thread runs the generator
     // while the others walk their stretches of the path (from jumps)

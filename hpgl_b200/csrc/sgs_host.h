@@ -19,6 +19,9 @@ struct SimPath {
 // negative.
 void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out);
 
+// The checks sim_path makes before any work (same exceptions).
+void check_sim_path(long long size, long long seed);
+
 // xp[k] = the standard normal quantile of u[k] (gaussian_cdf_t::inverse),
 // k < n.
 void gaussian_quantiles(const double *u, long long n, double *xp, int threads);

@@ -658,38 +658,27 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     using SM = SysSmemN<NC * 34>;
     SM &S = reinterpret_cast<SM *>(dyn_smem)[warp];
-    const int count = G.ctl->count[cur];
+    const int ntry = G.ctl->ntry;
     const int *win = cur ? G.win1 : G.win0;
-    // window slots are handed out 32 at a time as warps free up
-    for (;;) {
-        int base = 0;
-        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
-        base = __shfl_sync(FULL_MASK, base, 0);
-        if (base >= count) break;
-        int my_rank;
-        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
-        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
-        while (todo) {
-            const int l = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
-            const int node = G.nodes[rank];
-            int cnt;
-            const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
-            if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
+    // the round's tries are handed out one at a time as warps free up
+    int slot, rank;
+    while (sgs_next_try(G, win, ntry, lane, slot, rank)) {
+        const int node = G.nodes[rank];
+        int cnt;
+        const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
+        if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
+        __syncwarp();
+        if (blocker < 0) {
+            const NodeFetch f = fetch_node(J, P, node, lane);
+            exact32_node<NC>(J, P, S, f, lane);
             __syncwarp();
-            if (blocker < 0) {
-                const NodeFetch f = fetch_node(J, P, node, lane);
-                exact32_node<NC>(J, P, S, f, lane);
-                __syncwarp();
-                if (lane == 0) sgs_value(J, node, G.xp[rank]);
-            }
-            if (lane == 0) {
-                G.ok[base + l] = blocker < 0;
-                if (blocker >= 0) G.blocker[rank] = blocker;
-            }
-            __syncwarp();
+            if (lane == 0) sgs_value(J, node, G.xp[rank]);
         }
+        if (lane == 0) {
+            G.ok[slot] = blocker < 0;
+            if (blocker >= 0) G.blocker[rank] = blocker;
+        }
+        __syncwarp();
     }
 }
 
@@ -749,52 +738,41 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sis_try32(DevJob J, const DevP
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     using SM = SysSmemN<NC * 34>;
     SM &S = reinterpret_cast<SM *>(dyn_smem)[warp];
-    const int count = G.ctl->count[cur];
+    const int ntry = G.ctl->ntry;
     const int *win = cur ? G.win1 : G.win0;
     const int cats = J.K == 2 ? 1 : J.K;
-    // window slots are handed out 32 at a time as warps free up
-    for (;;) {
-        int base = 0;
-        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
-        base = __shfl_sync(FULL_MASK, base, 0);
-        if (base >= count) break;
-        int my_rank;
-        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
-        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
-        while (todo) {
-            const int l = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
-            const int node = G.nodes[rank];
-            int *list = J.nb + (long long)node * J.nb_stride;
-            float *probs = J.probs + (long long)node * J.K;
-            int blocker = -1;
-            for (int k = 0; k < cats; ++k) {
-                const DevPlan &P = plans[k];
-                int cnt;
-                blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
-                if (blocker >= 0) break;
-                __syncwarp();
-                const float mc = sis_mean(J, k, node);
-                double prob = (double)mc;
-                if (cnt > 0) {
-                    const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
-                    double sg, w;
-                    const NodeData d = sis_load32(J, P, S, node, list, cnt, k, sgc, lane, sg);
-                    const int status = J.sis_corr ? exact_core<true, NC>(J, P, S, lane, d, sg, w)
-                                                  : exact_core<false, NC>(J, P, S, lane, d, 0.0, w);
-                    if (status == ST_SUCCESS)
-                        prob = seq_dsum((double)mc, __dmul_rn(w, (double)d.dv), cnt, S.vd, lane);
-                }
-                if (lane == 0) {
-                    probs[k] = __double2float_rn(prob);
-                    if (J.K == 2) probs[1] = __double2float_rn(__dsub_rn(1.0, prob));
-                }
-                __syncwarp();
+    // the round's tries are handed out one at a time as warps free up
+    int slot, rank;
+    while (sgs_next_try(G, win, ntry, lane, slot, rank)) {
+        const int node = G.nodes[rank];
+        int *list = J.nb + (long long)node * J.nb_stride;
+        float *probs = J.probs + (long long)node * J.K;
+        int blocker = -1;
+        for (int k = 0; k < cats; ++k) {
+            const DevPlan &P = plans[k];
+            int cnt;
+            blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
+            if (blocker >= 0) break;
+            __syncwarp();
+            const float mc = sis_mean(J, k, node);
+            double prob = (double)mc;
+            if (cnt > 0) {
+                const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
+                double sg, w;
+                const NodeData d = sis_load32(J, P, S, node, list, cnt, k, sgc, lane, sg);
+                const int status = J.sis_corr ? exact_core<true, NC>(J, P, S, lane, d, sg, w)
+                                              : exact_core<false, NC>(J, P, S, lane, d, 0.0, w);
+                if (status == ST_SUCCESS)
+                    prob = seq_dsum((double)mc, __dmul_rn(w, (double)d.dv), cnt, S.vd, lane);
             }
-            if (lane == 0) sis_finish(J, G, node, rank, base + l, blocker);
+            if (lane == 0) {
+                probs[k] = __double2float_rn(prob);
+                if (J.K == 2) probs[1] = __double2float_rn(__dsub_rn(1.0, prob));
+            }
             __syncwarp();
         }
+        if (lane == 0) sis_finish(J, G, node, rank, slot, blocker);
+        __syncwarp();
     }
 }
 

@@ -458,38 +458,27 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs_try64(DevJob J, DevP
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Exact64Smem &S = reinterpret_cast<Exact64Smem *>(dyn_smem)[warp];
-    const int count = G.ctl->count[cur];
+    const int ntry = G.ctl->ntry;
     const int *win = cur ? G.win1 : G.win0;
-    // window slots are handed out 32 at a time as warps free up
-    for (;;) {
-        int base = 0;
-        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
-        base = __shfl_sync(FULL_MASK, base, 0);
-        if (base >= count) break;
-        int my_rank;
-        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
-        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
-        while (todo) {
-            const int l = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
-            const int node = G.nodes[rank];
-            int cnt;
-            const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
-            if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
+    // the round's tries are handed out one at a time as warps free up
+    int slot, rank;
+    while (sgs_next_try(G, win, ntry, lane, slot, rank)) {
+        const int node = G.nodes[rank];
+        int cnt;
+        const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
+        if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
+        __syncwarp();
+        if (blocker < 0) {
+            const NodeFetch f = fetch_node(J, P, node, lane);
+            exact64_node(J, P, S, s_cs, f, lane);
             __syncwarp();
-            if (blocker < 0) {
-                const NodeFetch f = fetch_node(J, P, node, lane);
-                exact64_node(J, P, S, s_cs, f, lane);
-                __syncwarp();
-                if (lane == 0) sgs_value(J, node, G.xp[rank]);
-            }
-            if (lane == 0) {
-                G.ok[base + l] = blocker < 0;
-                if (blocker >= 0) G.blocker[rank] = blocker;
-            }
-            __syncwarp();
+            if (lane == 0) sgs_value(J, node, G.xp[rank]);
         }
+        if (lane == 0) {
+            G.ok[slot] = blocker < 0;
+            if (blocker >= 0) G.blocker[rank] = blocker;
+        }
+        __syncwarp();
     }
 }
 
@@ -869,55 +858,44 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sis_try64(DevJob J, cons
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Sis64Smem &S = reinterpret_cast<Sis64Smem *>(dyn_smem)[warp];
-    const int count = G.ctl->count[cur];
+    const int ntry = G.ctl->ntry;
     const int *win = cur ? G.win1 : G.win0;
     const int cats = J.K == 2 ? 1 : J.K;
-    // window slots are handed out 32 at a time as warps free up
-    for (;;) {
-        int base = 0;
-        if (lane == 0) base = (int)atomicAdd(&G.ctl->cursor, 32u);
-        base = __shfl_sync(FULL_MASK, base, 0);
-        if (base >= count) break;
-        int my_rank;
-        unsigned todo = sgs_lanes_to_try(G, win, count, base, lane, my_rank);
-        if (lane == 0 && todo) atomicAdd(reinterpret_cast<unsigned long long *>(&G.ctl->tries), __popc(todo));
-        while (todo) {
-            const int l = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int rank = __shfl_sync(FULL_MASK, my_rank, l);
-            const int node = G.nodes[rank];
-            int *list = J.nb + (long long)node * J.nb_stride;
-            float *probs = J.probs + (long long)node * J.K;
-            int blocker = -1;
-            for (int k = 0; k < cats; ++k) {
-                const DevPlan &P = plans[k];
-                int cnt;
-                blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
-                if (blocker >= 0) break;
-                __syncwarp();
-                const float mc = sis_mean(J, k, node);
-                double prob = (double)mc;
-                if (cnt > 0) {
-                    const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
-                    const Node64 d = sis_load64(J, P, S, node, list, cnt, k, sgc, lane);
-                    double w0, w1;
-                    const int status =
-                        J.sis_corr ? exact64_core<true>(J, P, S.e, s_cs, g_pairs64.v, lane, d, S.sg, w0, w1)
-                                   : exact64_core<false>(J, P, S.e, s_cs, g_pairs64.v, lane, d, nullptr, w0, w1);
-                    if (status == ST_SUCCESS) {
-                        const double t0 = __dmul_rn(w0, (double)d.dv[0]), t1 = __dmul_rn(w1, (double)d.dv[1]);
-                        prob = rows_dsum((double)mc, t0, t1, cnt);
-                    }
+    // the round's tries are handed out one at a time as warps free up
+    int slot, rank;
+    while (sgs_next_try(G, win, ntry, lane, slot, rank)) {
+        const int node = G.nodes[rank];
+        int *list = J.nb + (long long)node * J.nb_stride;
+        float *probs = J.probs + (long long)node * J.K;
+        int blocker = -1;
+        for (int k = 0; k < cats; ++k) {
+            const DevPlan &P = plans[k];
+            int cnt;
+            blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
+            if (blocker >= 0) break;
+            __syncwarp();
+            const float mc = sis_mean(J, k, node);
+            double prob = (double)mc;
+            if (cnt > 0) {
+                const double sgc = J.sis_corr ? sis_sigma(mc) : 0.0;
+                const Node64 d = sis_load64(J, P, S, node, list, cnt, k, sgc, lane);
+                double w0, w1;
+                const int status =
+                    J.sis_corr ? exact64_core<true>(J, P, S.e, s_cs, g_pairs64.v, lane, d, S.sg, w0, w1)
+                               : exact64_core<false>(J, P, S.e, s_cs, g_pairs64.v, lane, d, nullptr, w0, w1);
+                if (status == ST_SUCCESS) {
+                    const double t0 = __dmul_rn(w0, (double)d.dv[0]), t1 = __dmul_rn(w1, (double)d.dv[1]);
+                    prob = rows_dsum((double)mc, t0, t1, cnt);
                 }
-                if (lane == 0) {
-                    probs[k] = __double2float_rn(prob);
-                    if (J.K == 2) probs[1] = __double2float_rn(__dsub_rn(1.0, prob));
-                }
-                __syncwarp();
             }
-            if (lane == 0) sis_finish(J, G, node, rank, base + l, blocker);
+            if (lane == 0) {
+                probs[k] = __double2float_rn(prob);
+                if (J.K == 2) probs[1] = __double2float_rn(__dsub_rn(1.0, prob));
+            }
             __syncwarp();
         }
+        if (lane == 0) sis_finish(J, G, node, rank, slot, blocker);
+        __syncwarp();
     }
 }
 

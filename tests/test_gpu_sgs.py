@@ -196,3 +196,38 @@ def test_gpu_matches_golden(native_lib, path):
         native_lib.hpgl_sgs_simulation(C.byref(arr), C.byref(q), cdfp, None, smp)
     assert native_lib.hpgl_get_last_error() == 0
     assert _same(values, d["out_values"]) and np.array_equal(mask, d["out_mask"])
+
+
+def test_sgs_refuses_negative_seed_without_touching_data(native_lib):
+    # the reference's walk leaves the grid for a seed negative as an int; here
+    # the call is refused before the CDF transform changes the property
+    job = _job((12, 10, 4), seed=20)
+    values = np.array(job["values"], np.float32)
+    mask = np.array(job["mask"], np.uint8)
+    before = values.copy()
+    sh = O._shape(job["shape"])
+    arr = O.HpglContArray(values.ctypes.data_as(C.POINTER(C.c_float)), mask.ctypes.data_as(C.POINTER(C.c_ubyte)), sh)
+    p = job["params"][0]
+    q = O.HpglSgsParams()
+    q.covariance_type = p["cov_type"]
+    q.ranges[:] = p["ranges"]
+    q.angles[:] = p["angles"]
+    q.sill, q.nugget = p["sill"], p["nugget"]
+    q.radiuses[:] = p["radii"]
+    q.max_neighbours = p["max_neighbours"]
+    q.kriging_kind = 1
+    cv = np.sort(values[mask != 0])[:-1].copy()
+    cp = np.linspace(0.1, 0.9, cv.size).astype(np.float32)
+    cdf = O.HpglNonParametricCdf(cv.ctypes.data_as(C.POINTER(C.c_float)), cp.ctypes.data_as(C.POINTER(C.c_float)),
+                                 cv.size)
+    for seed in (-1, 2 ** 31 + 7):
+        q.seed = seed
+        native_lib.hpgl_sgs_simulation(C.byref(arr), C.byref(q), C.byref(cdf), None, None)
+        assert native_lib.hpgl_get_last_error() == N.HPGL_E_INVALID
+        assert np.array_equal(values, before)
+    # a seed above 2^32 is taken modulo 2^32, as the reference's int and uint32 casts do
+    q.seed = 2 ** 32 + 9
+    native_lib.hpgl_sgs_simulation(C.byref(arr), C.byref(q), None, None, None)
+    assert native_lib.hpgl_get_last_error() == 0
+    v, m, _ = O.sgs(job, seed=9)
+    assert _same(values, v) and np.array_equal(mask, m)
