@@ -92,6 +92,8 @@ def run(args, root):
     _, r = _timed(sgs_dev, steps, warmup)
     ms_sgs_dev = float(np.median(dev[-steps:]))
     rounds, tries = r["rounds"], r["systems"]
+    # where the time of one hpgl_b200_krige call goes (no CDF transforms)
+    split = {k: round(float(r[k]), 2) for k in ("ms_plan", "ms_h2d", "ms_device", "ms_d2h", "ms_total")}
 
     # SIS
     ind = geo.IndProperty(f(codes), f(mask), 2)
@@ -127,7 +129,8 @@ def run(args, root):
         "steps": steps, "warmup": warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
         "ms_device": ms_sgs_dev,
         "config": {"workload": "sgs_%dx%dx%d_1pct_r20_n12_exp10+sis_2cat" % GRID, "simulated_nodes": nsim,
-                   "rounds": rounds, "tries": tries, "ms_per_round": ms_sgs_dev / max(rounds, 1)},
+                   "rounds": rounds, "tries": tries, "ms_per_round": ms_sgs_dev / max(rounds, 1),
+                   "call_split": split},
         "e2e": {"value": nsim / (ms_sgs_e2e / 1e3), "unit": "nodes/s", "ms": ms_sgs_e2e,
                 "h2d_bytes_per_step": int(values.nbytes + mask.nbytes + cdf.values.nbytes + cdf.probs.nbytes),
                 "d2h_bytes_per_step": int(values.nbytes + mask.nbytes)},

@@ -681,7 +681,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     const Plan &P = g.plan;
     SimPath path;
     try {
-        sim_path(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, path);
+        sim_path(job.nx, job.ny, job.nz, job.mask, job.simulation_mask, job.seed, job.kind != KIND_IK, path);
     } catch (const std::domain_error &e) {
         throw HpglError{HPGL_E_UNSUPPORTED, e.what()};
     } catch (const std::invalid_argument &e) {
@@ -690,13 +690,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     const bool indicator = job.kind == KIND_IK;
     // per path rank: the draw itself (sample() compares it) or its normal
     // quantile
-    std::unique_ptr<double[]> quantiles;
     const double *draws = path.u.data();
-    if (!indicator && !path.u.empty()) {
-        quantiles.reset(new double[path.u.size()]);
-        gaussian_quantiles(path.u.data(), (long long)path.u.size(), quantiles.get(), host_threads());
-        draws = quantiles.get();
-    }
     res.ms_plan = ms_since(t0);
     auto t1 = std::chrono::steady_clock::now();
     cudaStream_t s = C.stream;

@@ -245,22 +245,30 @@ void check_sim_path(long long size, long long seed) {
         throw std::invalid_argument("the simulation path is undefined for a negative seed");
 }
 
-void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out) {
+void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, bool quantiles,
+              SimPath &out) {
     const long long size = (long long)nx * ny * nz;
     out.nodes.clear();
     out.u.clear();
     if (size <= 0) return;
     check_sim_path(size, seed);
     const Path path(size, seed);
-    // the draws do not depend on the walk: one thread runs the generator
-    // while the others walk their stretches of the path (from jumps)
+    // The draws do not depend on the walk: one thread runs the generator
+    // while the others walk their stretches of the path (from jumps) and then
+    // turn the finished stretches of draws into quantiles, in place, behind
+    // the generator (`produced` publishes its progress).
     std::vector<double> u;
-    std::atomic<long long> needed{size};
+    u.reserve((size_t)size);
+    double *const ud = u.data();
+    std::atomic<long long> needed{size}, produced{0};
     std::thread draws([&] {
         Mt11213b gen((uint32_t)seed);
-        u.reserve((size_t)size);
-        for (long long k = 0; k < needed.load(std::memory_order_relaxed); ++k)
+        long long k = 0;
+        for (; k < needed.load(std::memory_order_relaxed); ++k) {
             u.push_back(double(gen.next()) / double(0xffffffffu));
+            if ((k & 4095) == 4095) produced.store(k + 1, std::memory_order_release);
+        }
+        produced.store(k, std::memory_order_release);
     });
     const int t = (int)std::max<long long>(1, std::min<long long>(host_threads(), size / (1 << 16)));
     std::vector<std::vector<int>> part((size_t)t);
@@ -279,20 +287,31 @@ void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_ma
         });
     }
     for (auto &th : pool) th.join();
+    pool.clear();
     size_t count = 0;
     for (auto &v : part) count += v.size();
     needed = (long long)count;
+    if (quantiles) {
+        constexpr long long CH = 1 << 15;
+        std::atomic<long long> next{0};
+        const long long n = (long long)count;
+        const int w = std::max(1, host_threads() - 1);
+        for (int i = 0; i < w; ++i) {
+            pool.emplace_back([&] {
+                for (long long c = next.fetch_add(1); c * CH < n; c = next.fetch_add(1)) {
+                    const long long a = c * CH, b = std::min(n, a + CH);
+                    while (produced.load(std::memory_order_acquire) < b) std::this_thread::yield();
+                    for (long long k = a; k < b; ++k) ud[k] = quantile(ud[k]);
+                }
+            });
+        }
+    }
     out.nodes.reserve(count);
     for (auto &v : part) out.nodes.insert(out.nodes.end(), v.begin(), v.end());
+    for (auto &th : pool) th.join();
     draws.join();
     u.resize(count);
     out.u.swap(u);
-}
-
-void gaussian_quantiles(const double *u, long long n, double *xp, int threads) {
-    parallel_for(n, threads, [&](long long a, long long b) {
-        for (long long k = a; k < b; ++k) xp[k] = quantile(u[k]);
-    });
 }
 
 void cdf_to_gaussian(const NonParametricCdf &cdf, const float *in, float *out, const uint8_t *mask, long long n,

@@ -9,22 +9,20 @@ namespace hpgl_b200 {
 
 struct SimPath {
     std::vector<int> nodes;  // simulated nodes in path order
-    std::vector<double> u;   // the draw of each simulated node, in [0, 1]
+    std::vector<double> u;   // per simulated node: its draw in [0, 1], or the draw's quantile
 };
 
 // The path's uninformed nodes inside `sim_mask` (all when null: a node is
 // simulated when sim_mask[node] == 1) in path order, with the generator's
-// draws in the same order.  Throws std::domain_error above 10^7 nodes and
+// draws in the same order -- or, with `quantiles`, their standard normal
+// quantiles (gaussian_cdf_t::inverse).  Throws std::domain_error above 10^7 nodes and
 // std::invalid_argument when the seed, as the int the path takes, is
 // negative.
-void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, SimPath &out);
+void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_mask, long long seed, bool quantiles,
+              SimPath &out);
 
 // The checks sim_path makes before any work (same exceptions).
 void check_sim_path(long long size, long long seed);
-
-// xp[k] = the standard normal quantile of u[k] (gaussian_cdf_t::inverse),
-// k < n.
-void gaussian_quantiles(const double *u, long long n, double *xp, int threads);
 
 // A caller's non-parametric CDF (hpgl_non_parametric_cdf_t): `size` values in
 // increasing order and their cumulative probabilities.

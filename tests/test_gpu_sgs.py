@@ -49,6 +49,13 @@ def test_sgs_lvm_mask_64_neighbours(native_lib):
     assert _same(r["out"], v) and np.array_equal(r["out_mask"], m)
 
 
+def test_sgs_ordinary_64_neighbours(native_lib):
+    job = _job((18, 16, 10), seed=21, n=44, cov=W.GAUSSIAN, radii=(9, 9, 5))
+    r = N.simulate(job, 4040, kind="ok")
+    v, m, _ = O.sgs(job, ordinary=True, seed=4040)
+    assert _same(r["out"], v) and np.array_equal(r["out_mask"], m)
+
+
 def test_sgs_larger_grid(native_lib):
     job = _job((64, 60, 16), seed=7, n=24, radii=(10, 10, 4))
     r = N.simulate(job, 2024, kind="sk")
