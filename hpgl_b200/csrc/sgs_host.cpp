@@ -270,7 +270,19 @@ void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_ma
         }
         produced.store(k, std::memory_order_release);
     });
-    const int t = (int)std::max<long long>(1, std::min<long long>(host_threads(), size / (1 << 16)));
+    // A - 1 holds every prime factor of the size (and 4 when 4 divides it),
+    // so the walk visits every node once exactly when gcd(C, size) = 1
+    // (Hull and Dobell).  The fallback C = 2 of sizes 2, 4, 6, 8 and 12
+    // divides the size: that walk repeats nodes, and the reference skips a
+    // repeated node as already simulated -- done here by a single thread.
+    long long g = path.C, h = size;
+    while (h) {
+        const long long r = g % h;
+        g = h;
+        h = r;
+    }
+    const bool full_period = g == 1;
+    const int t = full_period ? (int)std::max<long long>(1, std::min<long long>(host_threads(), size / (1 << 16))) : 1;
     std::vector<std::vector<int>> part((size_t)t);
     const long long per = (size + t - 1) / t;
     std::vector<std::thread> pool;
@@ -279,9 +291,14 @@ void sim_path(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *sim_ma
             const long long a = i * per, b = std::min(size, a + per);
             long long x = path.jump(path.R, a);
             std::vector<int> &v = part[(size_t)i];
+            std::vector<char> seen(full_period ? 0 : (size_t)size, 0);
             for (long long k = a; k < b; ++k, x = path.step(x)) {
                 if (mask[x]) continue;
                 if (sim_mask && sim_mask[x] != 1) continue;
+                if (!full_period) {
+                    if (seen[(size_t)x]) continue;
+                    seen[(size_t)x] = 1;
+                }
                 v.push_back((int)x);
             }
         });

@@ -46,7 +46,8 @@ def _path(shc, shape, mask, seed, quantiles, sim_mask=None):
 
 @pytest.mark.parametrize("shape,seed", [((166, 141, 30), 3439275), ((17, 11, 5), 99), ((64, 64, 64), 2 ** 32 + 5),
                                         ((7, 3, 2), 0), ((250, 1, 1), 12345), ((5, 1, 1), 8), ((4, 1, 1), 3),
-                                        ((1, 1, 1), 1)])
+                                        ((1, 1, 1), 1), ((2, 1, 1), 1), ((3, 2, 1), 4), ((2, 2, 2), 5),
+                                        ((3, 2, 2), 6), ((9, 1, 1), 2)])
 def test_path_and_quantiles_match_restatement(shc, shape, seed):
     rng = np.random.default_rng(1)
     n = int(np.prod(shape))
@@ -61,6 +62,16 @@ def test_path_and_quantiles_match_restatement(shc, shape, seed):
     assert np.array_equal(xp.view(np.uint64), O.sgs_draws(seed, nodes.size).view(np.uint64))
     nodes2, u = _path(shc, shape, mask, seed, False, sm)
     assert np.array_equal(nodes2, nodes) and ((u >= 0) & (u <= 1)).all()
+
+
+def test_repeating_walks_skip_simulated_nodes(shc):
+    # sizes 2, 4, 6, 8, 12 fall back to C = 2, which divides the size: the walk
+    # repeats nodes and the reference simulates each once
+    for n in (2, 4, 6, 8, 12):
+        mask = np.zeros(n, np.uint8)
+        for seed in range(n):
+            nodes, _ = _path(shc, (n, 1, 1), mask, seed, True)
+            assert len(set(nodes.tolist())) == nodes.size
 
 
 def test_path_refusals(shc):
