@@ -26,7 +26,14 @@ def _job(shape, seed, n=12, cov=W.SPHERICAL, radii=None, informed=None):
 
 
 def _same(a, b):
-    return np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+    # bit for bit, except that a NaN matches a NaN: where a negative kriging
+    # variance meets the square root, the reference's x86 arithmetic gives its
+    # default NaN (sign set) and the GPU its canonical NaN, and later nodes
+    # that krige from such a node carry the NaN on
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.array_equal(na, nb) and np.array_equal(a[~na].view(np.uint32), b[~nb].view(np.uint32))
 
 
 @pytest.mark.parametrize("kind", ["sk", "ok"])
