@@ -605,6 +605,8 @@ struct SyncContext {
     cudaStream_t stream = nullptr;
     char *arena = nullptr;
     size_t cap = 0;
+    unsigned char *sim = nullptr;  // sequential simulation's scratch (grows, kept)
+    size_t sim_cap = 0;
     char *flush = nullptr;
     size_t flush_cap = 0;
 };
@@ -631,9 +633,19 @@ static void sync_arena(SyncContext &C, size_t bytes) {
     C.cap = bytes;
 }
 
-// Sequential Gaussian simulation (sequential_simulation.h:49-122): the host
-// schedule, then one launch per batch of nodes that do not see each other;
-// the property in the arena is simulated in place and copied out.
+static void sync_sim(SyncContext &C, size_t bytes) {
+    if (bytes <= C.sim_cap) return;
+    if (C.sim) cudaFree(C.sim);
+    C.sim = nullptr;
+    C.sim_cap = 0;
+    CUDA_CHECK(cudaMalloc(&C.sim, bytes));
+    C.sim_cap = bytes;
+}
+
+// Sequential simulation (sequential_simulation.h:49-122,
+// sequential_indicator_simulation.cpp:23-116): the host path and draws, then
+// speculative rounds on the device; the property in the arena is simulated in
+// place and copied out.
 static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::chrono::steady_clock::time_point t0);
 
 void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
@@ -711,12 +723,13 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
                  o_rank = take((size_t)S.size * 4), o_pend = take(bits_bytes), o_blocker = take((size_t)nsim * 4),
                  o_done = take((size_t)nsim), o_w0 = take((size_t)window * 4), o_w1 = take((size_t)window * 4),
                  o_ok = take((size_t)window), o_try = take((size_t)window * 4);
-    unsigned char *scratch = nullptr;
-    CUDA_CHECK(cudaMalloc(&scratch, off));
-    struct Free {
-        void *p;
-        ~Free() { cudaFree(p); }
-    } free_guard{scratch};
+    std::vector<DevPlan> cat_plans;  // indicator simulation: every category's plan (its group's)
+    if (indicator)
+        for (auto &gr : S.groups)
+            for (int k = gr.k0; k < gr.k1; ++k) cat_plans.push_back(gr.dp);
+    const size_t o_plans = take(cat_plans.size() * sizeof(DevPlan));
+    sync_sim(C, off);
+    unsigned char *scratch = C.sim;
     SgsState G;
     G.ctl = reinterpret_cast<SgsCtl *>(scratch + o_ctl);
     G.nodes = reinterpret_cast<const int *>(scratch + o_nodes);
@@ -729,21 +742,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     G.win1 = reinterpret_cast<int *>(scratch + o_w1);
     G.ok = scratch + o_ok;
     G.trylist = reinterpret_cast<int *>(scratch + o_try);
-    // indicator simulation: every category's plan (a category shares its
-    // group's)
-    DevPlan *d_plans = nullptr;
-    std::vector<DevPlan> cat_plans;
-    if (indicator) {
-        for (auto &gr : S.groups)
-            for (int k = gr.k0; k < gr.k1; ++k) cat_plans.push_back(gr.dp);
-        CUDA_CHECK(cudaMalloc(&d_plans, cat_plans.size() * sizeof(DevPlan)));
-    }
-    struct FreePlans {
-        void *p;
-        ~FreePlans() {
-            if (p) cudaFree(p);
-        }
-    } free_plans{d_plans};
+    DevPlan *d_plans = reinterpret_cast<DevPlan *>(scratch + o_plans);
     SgsCtl hc;
     memset(&hc, 0, sizeof(hc));
     hc.window = window;

@@ -85,12 +85,20 @@ def reference_available():
     return os.path.exists(REF_SO)
 
 
+_REF_OUTPUT = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p)(lambda text, param: 0)
+_REF_PROGRESS = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_int, C.c_void_p)(lambda stage, pct, param: 0)
+
+
 def reference():
     global _ref
     if _ref is None:
         _ref = C.CDLL(REF_SO)
         _ref.hpgl_get_last_exception_message.restype = C.c_char_p
         _ref.ref_template.restype = C.c_int
+        # the reference logs to stdout unless given handlers (output.cpp:9-20);
+        # silence it so that a benchmark's JSON line stays alone on stdout
+        _ref.hpgl_set_output_handler(_REF_OUTPUT, None)
+        _ref.hpgl_set_progress_handler(_REF_PROGRESS, None)
     return _ref
 
 
