@@ -1,8 +1,9 @@
 """Sequential Gaussian simulation on the GPU against the CPU restatement:
-every simulated value bit for bit (the batches of mutually distant nodes
-reproduce the sequential order exactly), for SK (mean 0), OK and LVM, with a
-simulation mask, with more than 32 neighbours, and through the reference's
-C entry points."""
+every simulated value bit for bit (the speculative rounds reproduce the
+sequential order exactly), for SK (mean 0), OK and LVM, with a simulation
+mask, with up to 16, 32 and 64 neighbours, with CDF transforms, through the
+reference's C entry points and the geo_bsd wrapper, and independent of the
+rounds' window."""
 
 import ctypes as C
 

@@ -51,6 +51,18 @@ def test_sis_mask_and_64_neighbours(native_lib, correlogram):
     assert np.array_equal(r["out"], codes) and np.array_equal(r["out_mask"], mask)
 
 
+@pytest.mark.parametrize("nmax", [24, 32])
+def test_sis_17_to_32_neighbours(native_lib, nmax):
+    # the largest category decides the kernel: 17-32 neighbours take the
+    # 32-column systems
+    c = case(shape=(22, 20, 8), K=3, seed=19)
+    ps = params(3)
+    ps[2] = dict(ps[2], max_neighbours=nmax)
+    r = N.simulate_indicator(_job(c, ps), 2468)
+    codes, mask = O.sis(c["shape"], c["codes"], c["mask"], ps, seed=2468)
+    assert np.array_equal(r["out"], codes) and np.array_equal(r["out_mask"], mask)
+
+
 def test_sis_reference_entry_points(native_lib):
     c = case(shape=(20, 18, 6), K=3, seed=14)
     ps = params(3)
