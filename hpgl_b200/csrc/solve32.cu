@@ -649,9 +649,50 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_fused32(DevJob J, DevPlan P) {
 
 constexpr size_t SMEM32 = sizeof(SysSmem) * WARPS32;
 
+// The simulated value of one node of sequential Gaussian simulation from its
+// neighbour list (`list`, `n` entries, in shared memory): the exact system,
+// the estimate and variance by exact_system's and write_outputs' rules,
+// and the value xp sqrt(variance) + estimate (sgs_value's rule), kept in
+// registers instead of going through the status / variance / estimate
+// arrays.  Written to the property and its mask by lane 0.
+template <int NC, typename SM>
+__device__ __forceinline__ void sgs_node32(const DevJob &J, const DevPlan &P, SM &S, int node, const int *list, int n,
+                                           double xp, int lane) {
+    NodeFetch f;
+    f.node = node;
+    f.n = n;
+    f.cell = lane < n ? list[lane] : 0;
+    f.cell2 = 0;
+    f.informed = false;
+    const NodeData d = load_node(J, P, S, f, lane);
+    const bool ordinary = J.kind == 0;
+    int status = ST_NO_NEIGHBOURS;
+    double variance = 0.0;
+    float est = 0.f;
+    if (n > 0) {
+        double w;
+        status = exact_core<false, NC>(J, P, S, lane, d, 0.0, w);
+        if (status == ST_SUCCESS) {
+            double v = seq_dsum(P.c0, -__dmul_rn(w, d.b), n, S.vd, lane);
+            if (ordinary) v = __dsub_rn(v, __shfl_sync(FULL_MASK, w, n - 1));
+            variance = v;
+            const float term = __double2float_rn(__dmul_rn(w, (double)d.dv));
+            const float m0 = J.kind == 1 ? J.sk_mean_f : (J.kind == 2 ? J.mean[node] : 0.f);
+            est = seq_fsum(m0, term, n, S.vf[0], lane);
+        }
+    }
+    if (lane == 0) {
+        const double value = status == ST_SUCCESS ? __dadd_rn(__dmul_rn(xp, __dsqrt_rn(variance)), (double)est)
+                                                  : __dadd_rn(__dmul_rn(xp, 1.0), 0.0);
+        J.sim_values[node] = __double2float_rn(value);
+        J.sim_mask[node] = 1;
+    }
+}
+
 // One speculative round of sequential simulation (at most 32 neighbours):
 // one warp per pending node of window buffer `cur`: the template search with
-// conflict detection, the exact FP64 system and the simulated value.
+// conflict detection (the list in shared memory), the exact FP64 system and
+// the simulated value.
 template <int NC>
 __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P, SgsState G, int cur) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -662,17 +703,15 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sgs_try32(DevJob J, DevPlan P,
     const int *win = cur ? G.win1 : G.win0;
     // the round's tries are handed out one at a time as warps free up
     int slot, rank;
+    int *list = reinterpret_cast<int *>(S.row);  // 64 ints, unused by the exact path
     while (sgs_next_try(G, win, ntry, lane, slot, rank)) {
         const int node = G.nodes[rank];
         int cnt;
-        const int blocker = template_node_spec(J, P, G, node, rank, lane, J.nb + (long long)node * P.nmax, cnt);
-        if (lane == 0 && blocker < 0) J.nbcount[node] = cnt;
+        const int blocker = template_node_spec(J, P, G, node, rank, lane, list, cnt);
         __syncwarp();
         if (blocker < 0) {
-            const NodeFetch f = fetch_node(J, P, node, lane);
-            exact32_node<NC>(J, P, S, f, lane);
+            sgs_node32<NC>(J, P, S, node, list, cnt, G.xp[rank], lane);
             __syncwarp();
-            if (lane == 0) sgs_value(J, node, G.xp[rank]);
         }
         if (lane == 0) {
             G.ok[slot] = blocker < 0;
@@ -745,7 +784,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_sis_try32(DevJob J, const DevP
     int slot, rank;
     while (sgs_next_try(G, win, ntry, lane, slot, rank)) {
         const int node = G.nodes[rank];
-        int *list = J.nb + (long long)node * J.nb_stride;
+        int *list = reinterpret_cast<int *>(S.row);  // 64 ints, unused by the exact path
         float *probs = J.probs + (long long)node * J.K;
         int blocker = -1;
         for (int k = 0; k < cats; ++k) {
