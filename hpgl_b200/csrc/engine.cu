@@ -760,10 +760,16 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     CUDA_CHECK(cudaMemsetAsync(G.done, 0, (size_t)nsim, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     res.ms_h2d = ms_since(t1);
-    cudaEvent_t e0, e1;
-    CUDA_CHECK(cudaEventCreate(&e0));
-    CUDA_CHECK(cudaEventCreate(&e1));
-    CUDA_CHECK(cudaEventRecord(e0, s));
+    struct Events {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
+    CUDA_CHECK(cudaEventCreate(&ev.e0));
+    CUDA_CHECK(cudaEventCreate(&ev.e1));
+    CUDA_CHECK(cudaEventRecord(ev.e0, s));
     DevJob J = make_devjob(S, g);
     Counters *cnt = at<Counters>(S, S.ar.o_counters);
     CUDA_CHECK(cudaMemsetAsync(cnt, 0, sizeof(Counters), s));
@@ -775,6 +781,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
         // every round commits at least the pending node of lowest rank
         launch_sgs_admit(J, g.dp, G, 1, s);
         int chunk = 4;
+        long long committed = 0;
         for (;;) {
             for (int c = 0; c < chunk; ++c, ++round) {
                 if (indicator) launch_sis_round(J, g.dp, d_plans, S.nmax_all <= 32 ? 0 : 1, G, (int)(round & 1), s);
@@ -784,18 +791,20 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
             CUDA_CHECK(cudaMemcpyAsync(&hc, G.ctl, sizeof(hc), cudaMemcpyDeviceToHost, s));
             CUDA_CHECK(cudaStreamSynchronize(s));
             if (hc.next >= hc.total && hc.count[round & 1] == 0) break;
-            if (round > nsim + 64) throw HpglError{HPGL_E_INTERNAL, "sequential simulation made no progress"};
+            // a round with pending nodes commits at least one of them
+            if (hc.commits <= committed)
+                throw HpglError{HPGL_E_INTERNAL, "sequential simulation made no progress in " +
+                                                     std::to_string(chunk) + " rounds"};
+            committed = hc.commits;
             chunk = std::min(chunk * 2, 64);
         }
     }
-    CUDA_CHECK(cudaEventRecord(e1, s));
+    CUDA_CHECK(cudaEventRecord(ev.e1, s));
     Counters hcnt;
     CUDA_CHECK(cudaMemcpyAsync(&hcnt, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    cudaEventElapsedTime(&ms, ev.e0, ev.e1);
     res.ms_device = ms;
     if (hcnt.err)
         throw HpglError{HPGL_E_INTERNAL, "device invariant violated (error bits " + std::to_string(hcnt.err) + ")"};
