@@ -25,7 +25,8 @@ Metric: kriged nodes/s.
 (hpgl_b200/bench_io.py), with the reference's own reader and writer beside;
 ``--workload variogram``: experimental variograms (hpgl_b200/bench_variogram.py);
 ``--workload sgs``: sequential Gaussian and indicator simulation
-(hpgl_b200/bench_sim.py).
+(hpgl_b200/bench_sim.py); ``--workload cokriging``: colocated simple
+cokriging, Markov models I and II (hpgl_b200/bench_cok.py).
 
 Multi-GPU: the path has no exchange step; N ranks (torchrun, one per GPU)
 each krige their own copy of the job ("replicas only", weak scaling).
@@ -176,10 +177,11 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
-    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs"],
+    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs", "cokriging"],
                     help="inc_io: INC property file read/write (hpgl_b200/bench_io.py); variogram: experimental "
                          "variograms (hpgl_b200/bench_variogram.py); sgs: sequential Gaussian and indicator "
-                         "simulation (hpgl_b200/bench_sim.py); one GPU")
+                         "simulation (hpgl_b200/bench_sim.py); cokriging: colocated simple cokriging "
+                         "(hpgl_b200/bench_cok.py); one GPU")
     args = ap.parse_args()
     if args.workload == "inc_io":
         from hpgl_b200 import bench_io
@@ -190,6 +192,9 @@ def main():
     if args.workload == "sgs":
         from hpgl_b200 import bench_sim
         return bench_sim.run(args, ROOT)
+    if args.workload == "cokriging":
+        from hpgl_b200 import bench_cok
+        return bench_cok.run(args, ROOT)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)

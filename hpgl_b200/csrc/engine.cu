@@ -918,7 +918,9 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     bench.ms_search = search_sum / phase_runs;
     bench.ms_resolve = resolve_sum / phase_runs;
     snprintf(bench.top_kernel, sizeof(bench.top_kernel), "%s",
-             top_kernel_name(S.nmax_all, S.precision, tuning_get(tuning_family(S.nmax_all), S.precision).schedule));
+             S.cok ? "k_cokriging"
+                   : top_kernel_name(S.nmax_all, S.precision,
+                                     tuning_get(tuning_family(S.nmax_all), S.precision).schedule));
     bench.launches_per_iter = pt.launches;
     cudaEventDestroy(pt.search0);
     cudaEventDestroy(pt.top0);
