@@ -5,6 +5,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <cstring>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -332,27 +333,56 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
         int cx = (int)(x / P.cl_r[0]), cy = (int)(y / P.cl_r[1]), cz = (int)(z / P.cl_r[2]);
         return ((long long)cz * P.my + cy) * P.mx + cx;
     };
-    for (long long i = 0; i < P.size; ++i) {
-        if (!mask[i]) continue;
-        long long b = bucket_of(i);
-        if (exceeded[b]) continue;
-        if (count[b] >= P.limit) {
+    // The informed nodes in index order (stretches of the mask scanned on all
+    // threads, eight bytes at a time).  A box takes nodes in that order until
+    // it holds `limit`, and the next one makes it overflow: it overflows
+    // exactly when it receives more than `limit` nodes.
+    std::vector<int> informed;
+    {
+        const long long chunk = std::max<long long>(1 << 16, (P.size + threads - 1) / std::max(threads, 1));
+        const long long parts = (P.size + chunk - 1) / chunk;
+        std::vector<std::vector<int>> part((size_t)parts);
+        parallel_for(parts, threads, [&](long long lo, long long hi) {
+            for (long long c = lo; c < hi; ++c) {
+                const long long a = c * chunk, e = std::min(P.size, a + chunk);
+                std::vector<int> &v = part[(size_t)c];
+                long long i = a;
+                for (; i < e && (i & 7); ++i)
+                    if (mask[i]) v.push_back((int)i);
+                for (; i + 8 <= e; i += 8) {
+                    uint64_t w;
+                    memcpy(&w, mask + i, 8);
+                    if (!w) continue;
+                    for (int k = 0; k < 8; ++k)
+                        if (mask[i + k]) v.push_back((int)(i + k));
+                }
+                for (; i < e; ++i)
+                    if (mask[i]) v.push_back((int)i);
+            }
+        });
+        size_t total = 0;
+        for (auto &v : part) total += v.size();
+        informed.reserve(total);
+        for (auto &v : part) informed.insert(informed.end(), v.begin(), v.end());
+    }
+    std::vector<long long> box_of(informed.size());
+    for (size_t k = 0; k < informed.size(); ++k) {
+        box_of[k] = bucket_of(informed[k]);
+        count[box_of[k]]++;
+    }
+    for (long long b = 0; b < nb; ++b)
+        if (count[b] > P.limit) {
             exceeded[b] = 1;
             count[b] = 0;
-            continue;
         }
-        count[b]++;
-    }
     P.bucket_start.assign(nb + 1, 0);
     for (long long b = 0; b < nb; ++b) P.bucket_start[b + 1] = P.bucket_start[b] + count[b];
     P.bucket_nodes.assign(P.bucket_start[nb], 0);
     {
         std::vector<int> fill(P.bucket_start.begin(), P.bucket_start.end() - 1);
-        for (long long i = 0; i < P.size; ++i) {
-            if (!mask[i]) continue;
-            long long b = bucket_of(i);
-            if (exceeded[b]) continue;
-            P.bucket_nodes[fill[b]++] = (int)i;
+        for (size_t k = 0; k < informed.size(); ++k) {
+            const long long b = box_of[k];
+            if (!exceeded[b]) P.bucket_nodes[fill[b]++] = informed[k];
         }
     }
     P.bucket_clean.assign(nb, 0);
@@ -402,8 +432,15 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
         P.B[a] = std::max(0, std::min(need, n3[a] - 1));
         P.trunc[a] = P.truncated ? p.radii[a] : P.B[a];
     }
-    fill_symmetric(P.table, P.B[0], P.B[1], P.B[2], threads,
-                   [&](int x, int y, int z) { return cov((double)x, (double)y, (double)z); });
+    if (P.B[0] == rx && P.B[1] == ry && P.B[2] == rz) {
+        // the template's box already holds C(-v) at v, which is C(v) bit for
+        // bit (the transform of -v is the negated transform of v, and only
+        // its squares enter the distance)
+        P.table.swap(data);
+    } else {
+        fill_symmetric(P.table, P.B[0], P.B[1], P.B[2], threads,
+                       [&](int x, int y, int z) { return cov((double)x, (double)y, (double)z); });
+    }
     P.c0 = c0;
     lap("table");
 
