@@ -26,7 +26,8 @@ Metric: kriged nodes/s.
 ``--workload variogram``: experimental variograms (hpgl_b200/bench_variogram.py);
 ``--workload sgs``: sequential Gaussian and indicator simulation
 (hpgl_b200/bench_sim.py); ``--workload cokriging``: colocated simple
-cokriging, Markov models I and II (hpgl_b200/bench_cok.py).
+cokriging, Markov models I and II (hpgl_b200/bench_cok.py); ``--workload
+configs``: every kriging configuration, mixed and FP64 (hpgl_b200/bench_configs.py).
 
 Multi-GPU: the path has no exchange step; N ranks (torchrun, one per GPU)
 each krige their own copy of the job ("replicas only", weak scaling).
@@ -177,11 +178,12 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
-    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs", "cokriging"],
+    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs", "cokriging", "configs"],
                     help="inc_io: INC property file read/write (hpgl_b200/bench_io.py); variogram: experimental "
                          "variograms (hpgl_b200/bench_variogram.py); sgs: sequential Gaussian and indicator "
                          "simulation (hpgl_b200/bench_sim.py); cokriging: colocated simple cokriging "
-                         "(hpgl_b200/bench_cok.py); one GPU")
+                         "(hpgl_b200/bench_cok.py); configs: every kriging configuration "
+                         "(hpgl_b200/bench_configs.py); one GPU")
     args = ap.parse_args()
     if args.workload == "inc_io":
         from hpgl_b200 import bench_io
@@ -195,6 +197,9 @@ def main():
     if args.workload == "cokriging":
         from hpgl_b200 import bench_cok
         return bench_cok.run(args, ROOT)
+    if args.workload == "configs":
+        from hpgl_b200 import bench_configs
+        return bench_configs.run(args, ROOT)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)
