@@ -11,7 +11,9 @@ neighbours, exponential variogram of ranges (10, 10, 10).
   (what the reference's sgs_simulation passes).
 * SIS: two categories with marginal probabilities 0.8 / 0.2 (20 % of the
   informed codes are 1), the same variogram for both (median SIS), seed
-  3241347.
+  3241347; and (``sis4``, device time) the test's four categories: spherical
+  ranges 4, 6, 2 and 10, sill 0.25, marginal probabilities 0.24, 0.235, 0.34
+  and 0.18.
 
 Unit: simulated nodes per second.  ``--grid NXxNYxNZ`` runs the same
 workload on another grid (profiling runs).  ``value``: the simulation's device time
@@ -112,6 +114,23 @@ def run(args, root):
     _, rs = _timed(sis_dev, steps, warmup)
     ms_sis_dev = float(np.median(sdev[-steps:]))
 
+    # four categories (the reference's multi-indicator case of the same test)
+    rng4 = np.random.default_rng(4)
+    probs4 = (0.24, 0.235, 0.34, 0.18)
+    codes4 = rng4.choice(4, size=codes.size, p=np.array(probs4) / sum(probs4)).astype(np.uint8)
+    sis4_params = [dict(_params(0.25), cov_type=0, ranges=(r, r, r), marginal_prob=q)
+                   for r, q in zip((4.0, 6.0, 2.0, 10.0), probs4)]
+    s4job = dict(shape=GRID, codes=codes4, mask=mask, values=None, kind="ik", params=sis4_params)
+    s4dev = []
+
+    def sis4_dev():
+        rr = N.simulate_indicator(s4job, SIS_SEED)
+        s4dev.append(rr["ms_device"])
+        return rr
+
+    _, rs4 = _timed(sis4_dev, steps, warmup)
+    ms_sis4_dev = float(np.median(s4dev[-steps:]))
+
     cpu = None
     if not args.no_cpu_baseline and O.reference_available():
         t0 = time.perf_counter()
@@ -121,9 +140,12 @@ def run(args, root):
         t0 = time.perf_counter()
         O.ref_sis(GRID, codes, mask, sis_params, seed=SIS_SEED)
         t_sis = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.ref_sis(GRID, codes4, mask, sis4_params, seed=SIS_SEED)
+        t_sis4 = time.perf_counter() - t0
         cpu = {"kind": "reference", "cores": 1, "sample": "the full workload (SGS with the CDF transform; SIS)",
                "value": nsim / t_sgs, "unit": "nodes/s", "sgs_s": t_sgs, "sis_s": t_sis,
-               "sis_nodes_per_s": nsim / t_sis}
+               "sis_nodes_per_s": nsim / t_sis, "sis4_s": t_sis4, "sis4_nodes_per_s": nsim / t_sis4}
     line = {
         "metric": "simulated nodes/s", "value": nsim / (ms_sgs_dev / 1e3), "unit": "nodes/s", "n_gpus": 1,
         "steps": steps, "warmup": warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
@@ -136,6 +158,8 @@ def run(args, root):
                 "d2h_bytes_per_step": int(values.nbytes + mask.nbytes)},
         "sis": {"value": nsim / (ms_sis_dev / 1e3), "ms_device": ms_sis_dev, "e2e": nsim / (ms_sis_e2e / 1e3),
                 "ms": ms_sis_e2e, "rounds": rs["rounds"], "tries": rs["systems"]},
+        "sis4": {"value": nsim / (ms_sis4_dev / 1e3), "ms_device": ms_sis4_dev, "rounds": rs4["rounds"],
+                 "tries": rs4["systems"]},
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
