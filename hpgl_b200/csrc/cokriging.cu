@@ -150,19 +150,29 @@ __device__ void cok_node(const DevJob &J, const DevPlan &P, CokSmem &S, int node
             for (int j = i + lane; j < ms; j += 32) S.A[row * LD + j] = div_by_rcp(S.A[row * LD + j], coef, y);
             if (lane == 0) S.B[row] = div_by_rcp(S.B[row], coef, y);
             __syncwarp();
-            // eliminate column i from every unused row
+            // eliminate column i from every unused row.  The unused rows are
+            // listed (in shared memory; the neighbour offsets are no longer
+            // needed) and dealt out to the lanes in turn, so that no lane
+            // takes two rows while another is idle (a 33-row system would
+            // otherwise leave lane 0 two rows per step).
             const double *pr = S.A + row * LD;
             const double bp = S.B[row];
-#pragma unroll
-            for (int h = 0; h < 3; ++h) {
-                const int r = lane + 32 * h;
-                const bool live = r < ms && !(h == 0 ? used0 : (h == 1 ? used1 : used2));
-                if (live) {
-                    double *ar = S.A + r * LD;
-                    const double c = ar[i];
-                    for (int k = i; k < ms; ++k) ar[k] = __dsub_rn(ar[k], __dmul_rn(c, pr[k]));
-                    S.B[r] = __dsub_rn(S.B[r], __dmul_rn(c, bp));
-                }
+            int *live = reinterpret_cast<int *>(S.nb);
+            const bool l0 = lane < ms && !used0, l1 = lane + 32 < ms && !used1, l2 = lane + 64 < ms && !used2;
+            const unsigned lb0 = __ballot_sync(FULL_MASK, l0), lb1 = __ballot_sync(FULL_MASK, l1),
+                           lb2 = __ballot_sync(FULL_MASK, l2);
+            const unsigned below = (1u << lane) - 1u;
+            if (l0) live[__popc(lb0 & below)] = lane;
+            if (l1) live[__popc(lb0) + __popc(lb1 & below)] = lane + 32;
+            if (l2) live[__popc(lb0) + __popc(lb1) + __popc(lb2 & below)] = lane + 64;
+            const int nlive = __popc(lb0) + __popc(lb1) + __popc(lb2);
+            __syncwarp();
+            for (int t = lane; t < nlive; t += 32) {
+                const int r = live[t];
+                double *ar = S.A + r * LD;
+                const double c = ar[i];
+                for (int k = i; k < ms; ++k) ar[k] = __dsub_rn(ar[k], __dmul_rn(c, pr[k]));
+                S.B[r] = __dsub_rn(S.B[r], __dmul_rn(c, bp));
             }
             __syncwarp();
         }
