@@ -103,3 +103,32 @@ def test_oracle_matches_golden(path):
     job = dict(shape=d["shape"], values=d["values"], mask=d["mask"], params=d["params"])
     v, m, _ = O.sgs(job, **SG.sgs_kwargs(d))
     assert np.array_equal(v.view(np.uint32), d["out_values"].view(np.uint32)) and np.array_equal(m, d["out_mask"])
+
+
+@need_ref
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 1, 1), (4, 1, 1), (3, 2, 1), (2, 2, 2), (3, 2, 2), (5, 1, 1),
+                                   (3, 3, 1)])
+def test_tiny_grids_match_reference(shape):
+    # grids whose path repeats nodes (sizes 2, 4, 6, 8, 12) and other tiny ones
+    rng = np.random.default_rng(sum(shape))
+    n = int(np.prod(shape))
+    job = dict(shape=shape, values=rng.normal(size=n).astype(np.float32),
+               mask=(rng.random(n) < 0.3).astype(np.uint8),
+               params=[dict(cov_type=0, ranges=(3.0, 3.0, 3.0), angles=(0.0, 0.0, 0.0), sill=1.0, nugget=0.0,
+                            radii=(2, 2, 2), max_neighbours=4)])
+    for seed in (0, 1, 5):
+        v1, m1, _ = O.sgs(job, seed=seed)
+        v2, m2 = O.ref_sgs(job, seed=seed)
+        assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32)) and np.array_equal(m1, m2)
+
+
+@need_ref
+def test_simulation_mask_values_other_than_one_are_skipped():
+    # the reference simulates a node only where the simulation mask is exactly 1
+    job = _job(shape=(14, 12, 4), seed=13)
+    rng = np.random.default_rng(6)
+    sm = rng.integers(0, 3, job["values"].size).astype(np.uint8)
+    v1, m1, _ = O.sgs(job, seed=21, sim_mask=sm)
+    v2, m2 = O.ref_sgs(job, seed=21, sim_mask=sm)
+    assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32)) and np.array_equal(m1, m2)
+    assert not m1[(sm == 2) & (job["mask"] == 0)].any()

@@ -59,3 +59,18 @@ def test_oracle_matches_golden(path):
     codes, mask = O.sis(d["shape"], d["codes"], d["mask"], d["params"], seed=d["seed"],
                         lvm=list(d["lvm"]) if "lvm" in d else None, correlogram=bool(d["correlogram"]))
     assert np.array_equal(codes, d["out_codes"]) and np.array_equal(mask, d["out_mask"])
+
+
+@need_ref
+@pytest.mark.parametrize("shape", [(2, 1, 1), (4, 1, 1), (3, 2, 1), (2, 2, 2), (3, 2, 2), (3, 3, 1)])
+def test_tiny_grids_match_reference(shape):
+    # including the sizes whose path repeats nodes (2, 4, 6, 8, 12)
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(n)
+    codes = rng.integers(0, 3, n).astype(np.uint8)
+    mask = (rng.random(n) < 0.3).astype(np.uint8)
+    ps = [dict(p, radii=(2, 2, 2), max_neighbours=4) for p in params(3)]
+    for seed in (0, 3):
+        a = O.sis(shape, codes, mask, ps, seed=seed)
+        b = O.ref_sis(shape, codes, mask, ps, seed=seed)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
