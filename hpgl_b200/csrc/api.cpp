@@ -1,5 +1,5 @@
 // extern "C" entry points of hpgl.so: the reference's kriging ABI
-// (src/geo_bsd/hpgl/api.h, api.cpp) plus this build's additions, all declared
+// (src/geo_bsd/hpgl/api.h, api.cpp) plus this library's additions, all declared
 // in include/hpgl.h.  Every entry point catches every error and records it
 // for hpgl_get_last_exception_message / hpgl_get_last_error.
 #include <algorithm>

@@ -566,9 +566,9 @@ __device__ __forceinline__ void mixed32_node(const DevJob &J, const DevPlan &P, 
             dmax = fmax(dmax, fabs(db));
             xmax = fmax(xmax, fabs(xb));
         }
-        const int verdict = gate.step(warp_max(dmax), warp_max(xmax));
-        if (verdict != 0) {
-            converged = verdict > 0;
+        const int decision = gate.step(warp_max(dmax), warp_max(xmax));
+        if (decision != 0) {
+            converged = decision > 0;
             break;
         }
     }

@@ -725,9 +725,9 @@ __device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, 
             dmax = fmax(dmax, fmax(fabs(db0), fabs(db1)));
             xmax = fmax(xmax, fmax(fabs(xb0), fabs(xb1)));
         }
-        const int verdict = gate.step(warp_max64(dmax), warp_max64(xmax));
-        if (verdict != 0) {
-            converged = verdict > 0;
+        const int decision = gate.step(warp_max64(dmax), warp_max64(xmax));
+        if (decision != 0) {
+            converged = decision > 0;
             break;
         }
     }
