@@ -17,9 +17,11 @@ Metric: kriged nodes/s.
 * ``e2e``: the same metric through the public C ABI (hpgl_b200_krige) from
   host buffers: planning, host->device copies, device work and device->host
   copies of the estimate and mask inside each timed call.
-* ``cpu_baseline``: the reference's own kriging (compiled from its sources by
-  oracle/build_ref.sh) on a node sample of the same job, all host threads.
-* ``--impl reference``: that reference CPU path as the timed arm.
+* ``cpu_baseline``: the reference's own simple kriging (compiled from its
+  sources by oracle/build_ref.sh) through its stock entry point
+  hpgl_simple_kriging on the whole job, all host threads (2 timed calls).
+* ``--impl reference``: that reference CPU path as the timed arm, one whole
+  job per step.
 
 ``--workload inc_io``: the INC property file reader and writer instead
 (hpgl_b200/bench_io.py), with the reference's own reader and writer beside;
@@ -119,29 +121,32 @@ def algorithmic_flops(nb_counts, rhs):
     return float(f.sum())
 
 
-def cpu_reference(job, steps, warmup, sample_nodes, threads):
-    """The reference's own per-node kriging (oracle/_ref) on a node sample;
-    falls back to the oracle restatement when the reference library is not
-    present.  Returns (nodes/s per step list, kind, sample description)."""
+def cpu_reference(job, steps, warmup, threads):
+    """The reference's own simple kriging through its stock C entry point
+    hpgl_simple_kriging (compiled from its sources into oracle/_ref; the
+    per-node progress tick of cont_kriging.h:108-111 included) on the whole
+    job, `threads` OpenMP threads.  Returns (nodes/s per timed call, kind,
+    description, threads used).  Without the reference build, the oracle
+    restatement runs the same job ("port")."""
     from oracle import oracle as O
-    rng = np.random.default_rng(7)
-    un = np.nonzero(job["mask"] == 0)[0]
-    sample = np.sort(rng.choice(un, min(sample_nodes, len(un)), replace=False)).astype(np.int32)
-    use_ref = O.reference_available()
+    kriged = int((job["mask"] == 0).sum())
+    if O.reference_available():
+        r = O.RefSimpleKriging(job, threads)
+        call, used, kind = r.call, r.threads, "reference"
+    else:
+        def call():
+            O.run(job, dumps=False, threads=threads)
+        used, kind = threads, "port"
     rates = []
     for it in range(warmup + steps):
         t = time.perf_counter()
-        if use_ref:
-            O.ref_sample(job, sample, threads=threads)
-        else:
-            O.run(job, node_list=sample, dumps=False, threads=threads)
+        call()
         dt = time.perf_counter() - t
         if it >= warmup:
-            rates.append(len(sample) / dt)
-    kind = "reference" if use_ref else "port"
-    desc = ("%d uniformly sampled uninformed nodes of the same job per step (lookup construction included), "
-            "%d OpenMP threads" % (len(sample), threads))
-    return rates, kind, desc
+            rates.append(kriged / dt)
+    desc = ("the whole job (%d kriged nodes) per call through hpgl_simple_kriging, %d OpenMP threads"
+            % (kriged, used))
+    return rates, kind, desc, used
 
 
 def run_reference_arm(args):
@@ -150,15 +155,21 @@ def run_reference_arm(args):
         return 0
     from hpgl_b200 import workloads as W
     job = W.sk_ok_256x256x64()
+    kriged = int((job["mask"] == 0).sum())
     threads = os.cpu_count() or 1
-    rates, kind, desc = cpu_reference(job, args.steps, args.warmup, 200000, threads)
+    # one whole job per step takes seconds on the host cores: one untimed
+    # call warms the library (page faults, thread pool) and keeps the run
+    # within a few minutes
+    warm = min(args.warmup, 1)
+    rates, kind, desc, used = cpu_reference(job, args.steps, warm, threads)
     v = float(np.median(rates))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "nodes/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * 200000 / v,
+        "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * kriged / v,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": desc},
-        "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": threads, "kind": kind, "sample": desc},
+        "config": {"workload": WORKLOAD, "grid": list(job["shape"]), "kriged_nodes_per_step": kriged,
+                   "entry": "hpgl_simple_kriging", "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": used, "kind": kind, "sample": desc},
         "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -172,7 +183,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=200000)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=40.0)
@@ -222,7 +232,7 @@ def main():
     size = int(np.prod(job["shape"]))
     kriged = int((job["mask"] == 0).sum())
 
-    from hpgl_b200.replicas import barrier, max_over_ranks, whole_job_rate
+    from replicas import barrier, max_over_ranks, whole_job_rate
 
     # Untimed run of each path first (library warm-up, neighbour counts).
     dump = N.krige(job, precision="fp64", dumps=True)
@@ -253,18 +263,39 @@ def main():
     value = whole_job_rate(world, kriged * args.steps, t_mixed)
     fp64_value = whole_job_rate(world, kriged * args.steps, t_fp64)
 
-    # End to end through the public API from host buffers.
-    for _ in range(1):
-        N.krige(job, precision="mixed")
-    barrier()
-    e2e_ms = []
-    for _ in range(args.steps):
-        r = N.krige(job, precision="mixed")
-        e2e_ms.append(r["ms_total"])
-    t_e2e = max_over_ranks(float(np.sum(e2e_ms)))
-    e2e_value = whole_job_rate(world, kriged * args.steps, t_e2e)
+    # End to end through the public API from host buffers, both precisions;
+    # the library reports each call's split (planning, copies, device).
+    e2e = {}
+    for prec in ("mixed", "fp64"):
+        N.krige(job, precision=prec)
+        barrier()
+        parts = {k: [] for k in ("ms_total", "ms_plan", "ms_h2d", "ms_device", "ms_d2h")}
+        for _ in range(args.steps):
+            r = N.krige(job, precision=prec)
+            for k in parts:
+                parts[k].append(r[k])
+        t_e2e = max_over_ranks(float(np.sum(parts["ms_total"])))
+        e2e[prec] = dict(value=whole_job_rate(world, kriged * args.steps, t_e2e), ms_per_step=t_e2e / args.steps,
+                         split_ms={k[3:]: float(np.mean(v)) for k, v in parts.items() if k != "ms_total"})
     h2d = size * 4 + size * 1
     d2h = size * 4 + size * 1
+
+    # Per-result error of the mixed path against the FP64 path (bit-identical
+    # to the reference's arithmetic): every kriged node's estimate and
+    # kriging variance, untimed.
+    ref64 = N.krige(job, precision="fp64", dumps="variance")
+    mix = N.krige(job, precision="mixed", dumps="variance")
+    okv = ref64["status"] == 0
+    scale = float(np.max(np.abs(job["values"][job["mask"] > 0])))
+    sill = job["params"][0]["sill"]
+    err_est = np.abs(mix["out"].astype(np.float64) - ref64["out"]) / np.maximum(np.abs(ref64["out"]), 1e-6 * scale)
+    err_var = np.abs(mix["variance"][okv] - ref64["variance"][okv]) / np.maximum(np.abs(ref64["variance"][okv]),
+                                                                                  1e-6 * sill)
+    mixed_error = {"max_rel_err_estimate": float(err_est.max()), "max_rel_err_variance": float(err_var.max()),
+                   "tolerance": 1e-6, "floors": "1e-6 x max |informed value| (estimates), 1e-6 x sill (variances)",
+                   "nodes": int(okv.sum()), "statuses_equal": bool(np.array_equal(ref64["status"], mix["status"])),
+                   "masks_equal": bool(np.array_equal(ref64["out_mask"], mix["out_mask"]))}
+    del ref64, mix
 
     # Roofline of the dominant kernel (the solve): algorithmic flops per
     # launch / CUDA-event duration; FP32 CUDA-core peak (nominal: 148 SMs x
@@ -301,8 +332,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rates, kind, desc = cpu_reference(job, 2, 1, args.cpu_sample, threads)
-        cpu = {"value": float(np.median(rates)), "unit": "nodes/s", "cores": threads, "kind": kind,
+        rates, kind, desc, used = cpu_reference(job, 2, 1, threads)
+        cpu = {"value": float(np.median(rates)), "unit": "nodes/s", "cores": used, "kind": kind,
                "sample": desc}
 
     if rank == 0:
@@ -318,8 +349,11 @@ def main():
                      "top_kernel_ms": info_f["ms_top_kernel"]},
             "mixed_vs_fp64": value / fp64_value,
             "routed_to_fp64": info_m["systems_fp64"] / max(1, info_m["systems"]),
-            "e2e": {"value": e2e_value, "unit": "nodes/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": t_e2e / args.steps},
+            "e2e": {"value": e2e["mixed"]["value"], "unit": "nodes/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e["mixed"]["ms_per_step"],
+                    "split_ms": e2e["mixed"]["split_ms"],
+                    "fp64": e2e["fp64"]},
+            "mixed_error": mixed_error,
             "roofline": roofline,
             "clocks": clk,
             "gpu_launches": info_m["launches"] * args.steps,

@@ -214,31 +214,30 @@ void sk_weights_alloc(const float *center, const float *xs, const float *ys, con
 // call's contents behind; k_sk_weights writes each word of its layout before
 // reading it (coordinates by the host copy, then A, b, x and the status word
 // by the kernel), so nothing needs clearing between calls.  Calls that
-// overlapped on the GPU would race on the array; this library serialises its
-// own calls with a lock.
+// overlapped on the GPU would race on the array; the static entry point's
+// calls are serialised with each other by g_static_mutex (the allocating
+// entry point has its own scratch and lock).  The copies and the kernel run
+// on the calling thread's per-thread default stream, which does not wait for
+// the caller's other (blocking) streams as the legacy stream 0 would.
 constexpr int STATIC_WEIGHTS_MAX = HPGL_B200_STATIC_WEIGHTS_MAX;
 constexpr size_t STATIC_WEIGHTS_BYTES = (WeightsScratchLayout::bytes(STATIC_WEIGHTS_MAX) + 255) / 256 * 256;
 static __device__ __align__(256) unsigned char g_weights_scratch[STATIC_WEIGHTS_BYTES];
 
 static std::mutex g_static_mutex;
-static void *g_static_addr[256];
 
 // Device address of g_weights_scratch on the current device.  In host code
-// the array's name is only a stand-in, never a device address, so the real
-// address is looked up once per device (first call on that device, with it
-// current) and cached.
+// the array's name is only a stand-in, never a device address.  The address
+// is looked up on every call, with the calling device current: the lookup
+// allocates nothing, and a context that was reset and re-created (which
+// reloads the library's module, possibly elsewhere) is followed.  The first
+// lookup on a device also loads the module there, so that first call should
+// come before any stream capture.
 static double *static_scratch() {
-    int dev = 0;
-    WCHECK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 256) throw HpglError{HPGL_E_UNSUPPORTED, "device ordinal above 255"};
-    if (!g_static_addr[dev]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_weights_scratch);
-        if (e != cudaSuccess || !ptr)
-            throw HpglError{HPGL_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
-        g_static_addr[dev] = ptr;
-    }
-    return (double *)g_static_addr[dev];
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_weights_scratch);
+    if (e != cudaSuccess || !ptr)
+        throw HpglError{HPGL_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
+    return (double *)ptr;
 }
 
 void sk_weights_static(const float *center, const float *xs, const float *ys, const float *zs, int n,
@@ -251,6 +250,7 @@ void sk_weights_static(const float *center, const float *xs, const float *ys, co
     if (n == 0) return;
     std::lock_guard<std::mutex> lock(g_static_mutex);
     double *scratch = static_scratch();
+    const cudaStream_t s = cudaStreamPerThread;
     double coords[3 * STATIC_WEIGHTS_MAX + 3];
     for (int i = 0; i < n; ++i) {
         coords[3 * i] = xs[i];
@@ -258,14 +258,15 @@ void sk_weights_static(const float *center, const float *xs, const float *ys, co
         coords[3 * i + 2] = zs[i];
     }
     for (int i = 0; i < 3; ++i) coords[3 * n + i] = center[i];
-    WCHECK(cudaMemcpy(scratch, coords, (3 * (size_t)n + 3) * sizeof(double), cudaMemcpyHostToDevice));
-    k_sk_weights<<<1, 32>>>(cov, n, scratch);
+    WCHECK(cudaMemcpyAsync(scratch, coords, (3 * (size_t)n + 3) * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_sk_weights<<<1, 32, 0, s>>>(cov, n, scratch);
     WCHECK(cudaGetLastError());
     double x[STATIC_WEIGHTS_MAX + 1];
     const double *dx = scratch + 3 * (size_t)n + 3 + (size_t)n * n + n;
-    WCHECK(cudaMemcpy(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost));
     int status = 0;
-    WCHECK(cudaMemcpy(&status, dx + n, sizeof(int), cudaMemcpyDeviceToHost));
+    WCHECK(cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    WCHECK(cudaMemcpyAsync(&status, dx + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    WCHECK(cudaStreamSynchronize(s));
     if (status != 0) throw HpglError{HPGL_E_INVALID, "kriging system is not positive definite"};
     for (int i = 0; i < n; ++i) weights[i] = (float)x[i];
 }

@@ -193,17 +193,21 @@ class _Prepared:
         r.out_codes = None if self.cont else _ptr(self.out, C.c_ubyte)
         r.out_mask = _ptr(self.out_mask, C.c_ubyte)
         if dumps:
+            # dumps="variance": per-slot variance and status only (whole-grid
+            # checks of large jobs); any other true value adds the neighbour
+            # lists and weights
             a = self.arrays
             a["variance"] = np.full(slots, np.nan)
             a["status"] = np.full(slots, -2, dtype=np.int8)
-            a["nb_count"] = np.full(slots, -1, dtype=np.int32)
-            a["nb_index"] = np.full(slots * cap, -1, dtype=np.int32)
-            a["weights"] = np.zeros(slots * cap)
             r.variance = _ptr(a["variance"], C.c_double)
             r.status = _ptr(a["status"], C.c_byte)
-            r.nb_count = _ptr(a["nb_count"], C.c_int)
-            r.nb_index = _ptr(a["nb_index"], C.c_int)
-            r.weights = _ptr(a["weights"], C.c_double)
+            if dumps != "variance":
+                a["nb_count"] = np.full(slots, -1, dtype=np.int32)
+                a["nb_index"] = np.full(slots * cap, -1, dtype=np.int32)
+                a["weights"] = np.zeros(slots * cap)
+                r.nb_count = _ptr(a["nb_count"], C.c_int)
+                r.nb_index = _ptr(a["nb_index"], C.c_int)
+                r.weights = _ptr(a["weights"], C.c_double)
         if not self.cont:
             self.arrays["probs"] = np.zeros(self.size * (self.K if self.kind == "ik" else 1), dtype=np.float32)
             r.probs = _ptr(self.arrays["probs"], C.c_float)

@@ -425,11 +425,13 @@ int hpgl_b200_set_launch(int family, int precision, int schedule, int blocks_per
    allocating routine.  Its scratch is a fixed device array inside the
    library, present on every GPU that loads it until the process exits, sized
    for at most HPGL_B200_STATIC_WEIGHTS_MAX neighbours: larger counts return
-   -1 with HPGL_E_CAPACITY.  The first call on a device looks up the array's
-   device address (make that first call before any stream capture).  All
-   calls share the array and it keeps the last call's contents; the library
-   serialises its own calls, and calls that overlapped on the GPU would race
-   on it. */
+   -1 with HPGL_E_CAPACITY.  Each call looks up the array's device address
+   on the current device; the first call on a device also loads the library
+   there (make that first call before any stream capture).  The copies and
+   the kernel run on the calling thread's per-thread default stream.  All
+   calls share the array and it keeps the last call's contents; this entry
+   point's calls are serialised with each other by a lock inside the library,
+   and calls that overlapped on the GPU would race on it. */
 #define HPGL_B200_STATIC_WEIGHTS_MAX 256
 int hpgl_b200_simple_kriging_weights_static(float *center_coords, float *neighbours_x, float *neighbours_y,
                                             float *neighbours_z, int neighbours_count, hpgl_cov_params_t *params,

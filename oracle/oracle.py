@@ -85,6 +85,14 @@ def reference_available():
     return os.path.exists(REF_SO)
 
 
+def reference_src():
+    """The reference checkout's src/ directory (read-only sources, test data
+    and headers): $HPGL_REFERENCE_SRC, the same variable oracle/build_ref.sh
+    reads, else the checkout's usual place.  Absent where only the prebuilt
+    files travel."""
+    return os.environ.get("HPGL_REFERENCE_SRC", "/root/reference/src")
+
+
 _REF_OUTPUT = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p)(lambda text, param: 0)
 _REF_PROGRESS = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_int, C.c_void_p)(lambda stage, pct, param: 0)
 
@@ -251,6 +259,33 @@ def ref_run(job, threads=0, kind=None, sk_auto_mean=False, median_marginal1=None
         q.marginal_probs[:] = (1.0 - m1, m1)
         ref.hpgl_median_ik(C.byref(a), C.byref(q), C.byref(b))
     return out, out_mask
+
+
+class RefSimpleKriging:
+    """The reference's stock simple-kriging entry point, hpgl_simple_kriging
+    (api.cpp:261-288 -> simple_kriging.cpp:40-70 -> cont_kriging.h:75-113,
+    per-node progress tick included), on a whole job with `threads` OpenMP
+    threads (hpgl_set_thread_num).  The buffers are prepared once, as geo.py
+    does (the output a clone of the input); ``call()`` is the C call alone.
+    Every uninformed node is rewritten by each call (SK writes the mean where
+    a system fails), so calls can repeat on the same buffers."""
+
+    def __init__(self, job, threads):
+        self.ref = reference()
+        self.ref.hpgl_set_thread_num(int(threads))
+        self.threads = int(self.ref.hpgl_get_thread_num())
+        self.sh = _shape(job["shape"])
+        self.values = np.array(job["values"], dtype=np.float32)
+        self.mask = np.array(job["mask"], dtype=np.uint8)
+        self.out, self.out_mask = self.values.copy(), self.mask.copy()
+        self.sp = _ok_params(job["params"][0], HpglSkParams)
+        self.sp.automatic_mean = 0
+        self.sp.mean = job.get("sk_mean", 0.0)
+
+    def call(self):
+        self.ref.hpgl_simple_kriging(_ptr(self.values, C.c_float), _ptr(self.mask, C.c_ubyte), C.byref(self.sh),
+                                     C.byref(self.sp), _ptr(self.out, C.c_float), _ptr(self.out_mask, C.c_ubyte),
+                                     C.byref(self.sh))
 
 
 def ref_dump(job, kind=None, category=0, marginal=None, threads=0):

@@ -19,10 +19,11 @@ import numpy as np
 import pytest
 
 from hpgl_b200 import native as N
+from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "hpgl.h")
-REF_API = "/root/reference/src/geo_bsd/hpgl/api.h"
+REF_API = os.path.join(O.reference_src(), "geo_bsd", "hpgl", "api.h")
 
 
 def declared_functions():
@@ -135,7 +136,7 @@ def test_simulation_entry_points_reject_null_arguments(native_lib):
 # ---- the experimental-variogram ABI (include/cvariogram.h) -------------------------
 
 CV_HEADER = os.path.join(ROOT, "include", "cvariogram.h")
-REF_CV_API = "/root/reference/src/geo_bsd/_cvariogram/api.h"
+REF_CV_API = os.path.join(O.reference_src(), "geo_bsd", "_cvariogram", "api.h")
 CV_STRUCTS = ["vector_t", "ellipsoid_t", "variogram_search_template_t", "cont_point_set_t", "hard_data_t",
               "float_data_t"]
 

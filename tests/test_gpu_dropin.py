@@ -98,3 +98,94 @@ def test_ik_with_differing_categories(native_lib):
     assert np.array_equal(got["out"], ref["out"])
     assert np.array_equal(got["status"], ref["status"])
     assert np.array_equal(got["probs"].view(np.uint32), ref["probs"].view(np.uint32))
+
+
+def _sk_params(p, automatic, mean):
+    from hpgl_b200.geo_bsd import geo
+    from hpgl_b200.geo_bsd.hpgl_wrap import _HPGL_SK_PARAMS
+    cm = geo.CovarianceModel(type=p["cov_type"], ranges=p["ranges"], angles=p["angles"], sill=p["sill"],
+                             nugget=p["nugget"])
+    return _HPGL_SK_PARAMS(automatic_mean=int(automatic), mean=mean,
+                           **geo._kriging_fields(cm, p["radii"], p["max_neighbours"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("automatic", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_simple_kriging_c_abi(native_lib, automatic, precision):
+    """hpgl_simple_kriging (api.cpp:261-288) called with the reference's
+    struct: a given mean, or m_automatic_mean = 1 -- the mean of the
+    informed values (calc_mean.cpp:6-30, simple_kriging.cpp:50-59), the
+    given mean ignored."""
+    import ctypes as C
+    from hpgl_b200.geo_bsd import geo
+    from hpgl_b200.geo_bsd.hpgl_wrap import check_last_error
+    from tests.helpers import rel_err
+    job = W.sk_ok_256x256x64(shape=(40, 40, 16), seed=41)
+    job["values"] = (job["values"] + np.where(job["mask"] > 0, 0.75, 0.0)).astype(np.float32)
+    job["sk_mean"] = 0.3
+    p = job["params"][0]
+    skp = _sk_params(p, automatic, 0.3)
+    data = np.require(job["values"].copy(), np.float32, "F")
+    mask = np.require(job["mask"].copy(), np.uint8, "F")
+    out, out_mask = data.copy(), mask.copy()
+    sh = geo._create_hpgl_shape(job["shape"])
+    with geo._Precision(precision):
+        geo._hpgl_so.hpgl_simple_kriging(data, mask, C.byref(sh), C.byref(skp), out, out_mask, C.byref(sh))
+        check_last_error()
+    ref = O.run(job, kind="sk", sk_auto_mean=automatic, dumps=False)
+    other = O.run(job, kind="sk", sk_auto_mean=not automatic, dumps=False)
+    assert not np.array_equal(ref["out"], other["out"]), "the two means must give different estimates"
+    assert np.array_equal(out_mask, ref["out_mask"])
+    if precision == "fp64":
+        assert np.array_equal(out.view(np.uint32), ref["out"].view(np.uint32))
+    else:
+        scale = float(np.max(np.abs(job["values"][job["mask"] > 0])))
+        assert rel_err(out, ref["out"], 1e-6 * scale).max() <= 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_simple_kriging_entry_without_mean(native_lib, precision):
+    """geo.simple_kriging(..., mean=None) (geo.py:402-425) krigs with the
+    automatic mean."""
+    from hpgl_b200.geo_bsd import geo
+    from tests.helpers import rel_err
+    job = W.sk_ok_256x256x64(shape=(36, 30, 12), seed=43)
+    job["values"] = (job["values"] - np.where(job["mask"] > 0, 0.4, 0.0)).astype(np.float32)
+    p = job["params"][0]
+    cm = geo.CovarianceModel(type=p["cov_type"], ranges=p["ranges"], angles=p["angles"], sill=p["sill"],
+                             nugget=p["nugget"])
+    out = geo.simple_kriging(_cont_prop(job), geo.SugarboxGrid(36, 30, 12), p["radii"], p["max_neighbours"], cm,
+                             mean=None, precision=precision)
+    ref = O.run(job, kind="sk", sk_auto_mean=True, dumps=False)
+    data = out.data.reshape(-1, order="F")
+    assert np.array_equal(out.mask.reshape(-1, order="F"), ref["out_mask"])
+    if precision == "fp64":
+        assert np.array_equal(data.view(np.uint32), ref["out"].view(np.uint32))
+    else:
+        scale = float(np.max(np.abs(job["values"][job["mask"] > 0])))
+        assert rel_err(data, ref["out"], 1e-6 * scale).max() <= 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lvm_kriging_entry(native_lib, precision):
+    """geo.lvm_kriging -> hpgl_lvm_kriging (api.cpp:344-383) with a mean cube,
+    Gaussian variogram and clustered data (singular systems included)."""
+    from hpgl_b200.geo_bsd import geo
+    from tests.helpers import rel_err
+    job = W.lvm_512x512x32(shape=(64, 64, 12), seed=44, blobs=20)
+    p = job["params"][0]
+    cm = geo.CovarianceModel(type=p["cov_type"], ranges=p["ranges"], angles=p["angles"], sill=p["sill"],
+                             nugget=p["nugget"])
+    out = geo.lvm_kriging(_cont_prop(job), geo.SugarboxGrid(64, 64, 12), job["mean"], p["radii"],
+                          p["max_neighbours"], cm, precision=precision)
+    ref = O.run(job, kind="lvm", dumps=False)
+    data = out.data.reshape(-1, order="F")
+    assert np.array_equal(out.mask.reshape(-1, order="F"), ref["out_mask"])
+    if precision == "fp64":
+        assert np.array_equal(data.view(np.uint32), ref["out"].view(np.uint32))
+    else:
+        scale = float(np.max(np.abs(job["values"][job["mask"] > 0])))
+        assert rel_err(data, ref["out"], 1e-6 * scale).max() <= 1e-6

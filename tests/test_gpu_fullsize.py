@@ -71,6 +71,13 @@ def test_fullsize_sampled_parity(native_lib, name, precision):
         informed = job["mask"] > 0
         scale = float(np.max(np.abs(job["values"][informed])))
         assert rel_err(got["out"][sample], ref["out"][sample], 1e-6 * scale).max() <= 1e-6
+    ok = ref["status"][sr] == 0
+    rv, gv = ref["variance"][sr][ok], got["variance"][sg][ok]
+    if precision == "fp64":
+        assert np.array_equal(rv.view(np.uint64), gv.view(np.uint64)), "variances differ"
+    else:
+        sill = job["params"][0]["sill"]
+        assert rel_err(gv, rv, 1e-6 * sill).max() <= 1e-6, "variances beyond 1e-6"
     # whole-grid properties
     if kind in ("sk", "lvm", "ik"):
         assert got["out_mask"].all(), "every node is written"
@@ -79,3 +86,28 @@ def test_fullsize_sampled_parity(native_lib, name, precision):
         assert np.array_equal(got["out"][informed].view(np.uint32), job["values"][informed].view(np.uint32))
     if precision == "mixed":
         assert got["systems_fp64"] <= got["systems"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_fullsize_mixed_against_fp64_whole_grid(native_lib, name):
+    """Every node of the full-size configuration: the mixed path (FP32
+    factorisation + FP64 refinement, FP64 re-solve of routed systems)
+    against the FP64 path (bit-identical to the oracle on the sampled
+    nodes): statuses and masks identical; estimates within 1e-6 relative
+    (floor 1e-6 of the field's scale), variances within 1e-6 relative
+    (floor 1e-6 of the sill); IK categories identical."""
+    job, kind, _, _ = _job(name)
+    ref = N.krige(job, precision="fp64", kind=kind, dumps="variance")
+    got = N.krige(job, precision="mixed", kind=kind, dumps="variance")
+    assert np.array_equal(ref["status"], got["status"])
+    assert np.array_equal(ref["out_mask"], got["out_mask"])
+    if kind == "ik":
+        assert np.array_equal(ref["out"], got["out"])
+    else:
+        informed = job["mask"] > 0
+        scale = float(np.max(np.abs(job["values"][informed])))
+        assert rel_err(got["out"], ref["out"], 1e-6 * scale).max() <= 1e-6
+    ok = ref["status"] == 0
+    sill = job["params"][0]["sill"]
+    assert rel_err(got["variance"][ok], ref["variance"][ok], 1e-6 * sill).max() <= 1e-6

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _rank_main(rank, world, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    from hpgl_b200.replicas import barrier, max_over_ranks, whole_job_rate
+    from replicas import barrier, max_over_ranks, whole_job_rate
     barrier()
     ms = 10.0 * (rank + 1)  # rank 1 is the slow one
     m = max_over_ranks(ms)
