@@ -184,8 +184,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-jobs", type=int, default=60)
-    ap.add_argument("--serve-rate", type=float, default=40.0)
+    ap.add_argument("--serve-jobs", type=int, default=40)
+    ap.add_argument("--serve-rates", default="5,20,50,100,200", help="arrival rates (jobs/s) of the serving sweep")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
     ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs", "cokriging", "configs"],
@@ -314,20 +314,36 @@ def main():
                 "peak_source": "nominal FP32 CUDA-core peak (MEASURED_PEAKS.json has HBM and bf16 tensor only)",
                 "ms_per_launch": info_m["ms_top_kernel"], "flop_per_launch": flops}
 
-    # Serving: a Poisson stream of mixed OK/SK/IK jobs (grids 32^3 .. 256x256x64,
-    # ranges 5-60, 8-64 neighbours) replayed in real time against the
-    # continuous-batching server; p50/p99 submit-to-completion latency.
+    # Serving: Poisson streams of mixed OK/SK/IK jobs (grids 32^3 ..
+    # 256x256x64, ranges 5-60, 8-64 neighbours) replayed in real time
+    # against the continuous-batching server at each arrival rate; p50/p99
+    # submit-to-completion latency, systems/s and where a job's time went.
+    # The same jobs run back to back through the synchronous call give the
+    # batch rate the stream is compared with.
     serve = None
     if not args.no_serve:
         from hpgl_b200 import serve as SV
-        stream = W.serve_stream(args.serve_jobs, args.serve_rate, seed=5 + rank)
-        serve = {"rate_jobs_per_s": args.serve_rate, "jobs": args.serve_jobs, "hbm_budget_gb": 120,
-                 "max_inflight": 8}
+        rates = [float(r) for r in args.serve_rates.split(",")]
+        serve = {"jobs_per_rate": args.serve_jobs, "hbm_budget_gb": 120, "max_inflight": 8, "rates": []}
+        batch_stream = W.serve_stream(args.serve_jobs, 1.0, seed=5 + rank)
         for prec in ("mixed", "fp64"):
-            st, _ = SV.run_stream(stream, precision=prec, hbm_budget_bytes=120 << 30, max_inflight=8)
-            serve[prec] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "systems_per_s": st["systems_per_s"],
-                           "completed": st["completed"], "failed": st["failed"],
-                           "peak_inflight": st["peak_inflight"]}
+            t = time.perf_counter()
+            systems = 0
+            for _, job in batch_stream:
+                systems += N.krige(job, precision=prec)["systems"]
+            serve["batch_" + prec] = {"systems_per_s": systems / (time.perf_counter() - t),
+                                      "note": "the same jobs back to back through hpgl_b200_krige (whole calls)"}
+        for rate in rates:
+            stream = W.serve_stream(args.serve_jobs, rate, seed=5 + rank)
+            row = {"rate_jobs_per_s": rate}
+            for prec in ("mixed", "fp64"):
+                st, _ = SV.run_stream(stream, precision=prec, hbm_budget_bytes=120 << 30, max_inflight=8)
+                row[prec] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "systems_per_s": st["systems_per_s"],
+                             "completed": st["completed"], "failed": st["failed"],
+                             "peak_inflight": st["peak_inflight"],
+                             "mean_split_ms": {"plan": st["mean_plan_ms"], "admission_wait": st["mean_wait_ms"],
+                                               "device_and_copies": st["mean_run_ms"]}}
+            serve["rates"].append(row)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -391,6 +391,12 @@ static void upload(JobState &S, cudaStream_t s) {
         d.my = P.my;
         d.mz = P.mz;
         d.max_candidates = std::max(1, P.max_candidates);
+        d.hx = P.hot[0];
+        d.hy = P.hot[1];
+        d.hz = P.hot[2];
+        d.hsx = 2 * P.hot[0] + 1;
+        d.hsyx = d.hsx * (2 * P.hot[1] + 1);
+        d.packed_ok = P.reach[0] <= 511 && P.reach[1] <= 511 && P.reach[2] <= 255;
     }
 }
 
@@ -827,12 +833,12 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     res.rounds = hc.rounds;
 }
 
-static const char *top_kernel_name(int nmax, int precision, int schedule) {
+static const char *top_kernel_name(int nmax, int precision, int schedule, const DevPlan &dp) {
     if (schedule == SCHED_FUSED) {
         if (nmax <= 32) return precision ? "k_fused32<1>" : "k_fused32<0>";
         return precision ? "k_fused64<1>" : "k_fused64<0>";
     }
-    if (nmax <= 32) return precision ? "k_solve_mixed32" : "k_solve_exact32";
+    if (nmax <= 32) return precision ? mixed32_kernel_name(dp) : "k_solve_exact32";
     return precision ? "k_solve_mixed64" : "k_solve_exact64";
 }
 
@@ -920,7 +926,7 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     snprintf(bench.top_kernel, sizeof(bench.top_kernel), "%s",
              S.cok ? "k_cokriging"
                    : top_kernel_name(S.nmax_all, S.precision,
-                                     tuning_get(tuning_family(S.nmax_all), S.precision).schedule));
+                                     tuning_get(tuning_family(S.nmax_all), S.precision).schedule, S.groups[0].dp));
     bench.launches_per_iter = pt.launches;
     cudaEventDestroy(pt.search0);
     cudaEventDestroy(pt.top0);
@@ -1044,6 +1050,7 @@ struct ServerJob {
     int code = HPGL_OK;
     std::string message;
     double latency_ms = 0;
+    double plan_ms = 0, wait_ms = 0, run_ms = 0;
 };
 
 struct Server {
@@ -1078,12 +1085,15 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
     long long bytes = 0;
     try {
         CUDA_CHECK(cudaSetDevice(device));
+        const auto t_plan = std::chrono::steady_clock::now();
         prepare(S, sj->job, *sj->result);
+        sj->plan_ms = ms_since(t_plan);
         bytes = (long long)S.ar.total;
         if (bytes > budget)
             throw HpglError{HPGL_E_CAPACITY, "job needs " + std::to_string(bytes) +
                                                  " bytes of device memory, above the server's budget of " +
                                                  std::to_string(budget)};
+        const auto t_wait = std::chrono::steady_clock::now();
         {
             std::unique_lock<std::mutex> l(mu);
             cv_admit.wait(l, [&] { return stopping || (!free_slots.empty() && in_use + bytes <= budget); });
@@ -1095,6 +1105,8 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
             ++inflight;
             peak_inflight = std::max(peak_inflight, inflight);
         }
+        sj->wait_ms = ms_since(t_wait);
+        const auto t_run = std::chrono::steady_clock::now();
         cudaStream_t s = streams[slot];
         void *arena = nullptr;
         CUDA_CHECK(cudaMallocAsync(&arena, S.ar.total, s));
@@ -1111,6 +1123,7 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
         }
         CUDA_CHECK(cudaFreeAsync(arena, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
+        sj->run_ms = ms_since(t_run);
     } catch (const HpglError &e) {
         sj->code = e.code;
         sj->message = e.message;
@@ -1211,11 +1224,18 @@ void server_stats(void *h, hpgl_b200_server_stats_t &st) {
     std::lock_guard<std::mutex> l(sv->mu);
     std::vector<double> lat;
     long long failed = 0, completed = 0;
+    double plan = 0, wait = 0, run = 0;
     for (auto &sj : sv->all) {
         if (!sj->done) continue;
         ++completed;
-        if (sj->code != HPGL_OK) ++failed;
-        else lat.push_back(sj->latency_ms);
+        if (sj->code != HPGL_OK) {
+            ++failed;
+        } else {
+            lat.push_back(sj->latency_ms);
+            plan += sj->plan_ms;
+            wait += sj->wait_ms;
+            run += sj->run_ms;
+        }
     }
     std::sort(lat.begin(), lat.end());
     auto pct = [&](double q) {
@@ -1239,6 +1259,10 @@ void server_stats(void *h, hpgl_b200_server_stats_t &st) {
     st.systems_per_s = st.wall_s > 0 ? sv->systems_done / st.wall_s : 0;
     st.peak_inflight = sv->peak_inflight;
     st.peak_bytes = sv->peak_bytes;
+    const double nok = lat.empty() ? 1.0 : (double)lat.size();
+    st.mean_plan_ms = plan / nok;
+    st.mean_wait_ms = wait / nok;
+    st.mean_run_ms = run / nok;
 }
 
 void server_destroy(void *h) {

@@ -36,6 +36,12 @@ struct DevPlan {
     double crx, cry, crz;
     int mx, my, mz;
     int max_candidates;
+    // shared-memory box of the table for the mixed-precision solve: folded
+    // to vz >= 0, |vx| <= hx, |vy| <= hy, vz <= hz; hsx = 2hx+1, hsyx =
+    // hsx (2hy+1).  packed_ok: every neighbour offset fits the 32-bit packed
+    // form (|x|, |y| <= 511, |z| <= 255).
+    int hx, hy, hz, hsx, hsyx;
+    int packed_ok;
 };
 
 // Division by a runtime-invariant divisor d >= 1 of any n < 2^32 with one
@@ -207,6 +213,8 @@ void launch_sis_round(const DevJob &J, const DevPlan &P0, const DevPlan *plans, 
                       int cur, cudaStream_t s);
 void launch_sis_try32(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s);
 void launch_sis_try64(const DevJob &J, const DevPlan *plans, const SgsState &G, int cur, cudaStream_t s);
+// solve32.cu: the mixed-precision kernel launch_solve32 runs for plan P
+const char *mixed32_kernel_name(const DevPlan &P);
 // solve32.cu: register-resident solves for max_neighbours <= 32
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm);

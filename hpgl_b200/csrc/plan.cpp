@@ -19,10 +19,14 @@
 
 namespace hpgl_b200 {
 
+// Shared-memory table box budget of the mixed-precision solve: 72 KiB of
+// doubles (its blocks hold the box beside their warps' system buffers).
+constexpr long long HOT_TABLE_ENTRIES = 72 * 1024 / 8;
+
 static std::atomic<int> g_threads{0};
 
 template <typename F>
-static void parallel_for(long long n, int threads, F f);
+static void parallel_for(long long n, int threads, F f, long long grain = 4096);
 
 int host_threads() {
     int n = g_threads.load();
@@ -33,9 +37,11 @@ int host_threads() {
 
 void set_host_threads(int n) { g_threads.store(n > 0 ? n : 0); }
 
+// f(lo, hi) over [0, n) split across up to `threads` threads, at least
+// `grain` items per thread.
 template <typename F>
-static void parallel_for(long long n, int threads, F f) {
-    threads = (int)std::max<long long>(1, std::min<long long>(threads, n / 4096 + 1));
+static void parallel_for(long long n, int threads, F f, long long grain) {
+    threads = (int)std::max<long long>(1, std::min<long long>(threads, n / grain + 1));
     if (threads == 1) {
         f(0LL, n);
         return;
@@ -59,18 +65,27 @@ static void fill_symmetric(std::vector<double> &out, int rx, int ry, int rz, int
     const int xd = 2 * rx + 1, yd = 2 * ry + 1;
     out.assign((size_t)xd * yd * (2 * rz + 1), 0.0);
     auto idx = [&](int x, int y, int z) { return ((size_t)(z + rz) * yd + (y + ry)) * xd + (x + rx); };
-    parallel_for(rz + 1, threads, [&](long long lo, long long hi) {
-        for (long long zz = lo; zz < hi; ++zz) {
-            const int z = (int)zz;
-            for (int y = (z == 0 ? 0 : -ry); y <= ry; ++y)
+    // rows (z, y) of the evaluated half, z = 0..rz (y >= 0 at z = 0), a few
+    // thousand covariances per thread at least
+    const long long rows = (long long)(rz + 1) * yd;
+    parallel_for(
+        rows, threads,
+        [&](long long lo, long long hi) {
+            for (long long r = lo; r < hi; ++r) {
+                const int z = (int)(r / yd), y = (int)(r % yd) - ry;
+                if (z == 0 && y < 0) continue;
                 for (int x = (z == 0 && y == 0 ? 0 : -rx); x <= rx; ++x) {
                     const double v = f(x, y, z);
                     out[idx(x, y, z)] = v;
                     out[idx(-x, -y, -z)] = v;
                 }
-        }
-    });
+            }
+        },
+        std::max<long long>(1, 4096 / xd));
 }
+
+// Sub-ranges above this many entries may go to another thread.
+constexpr int SORT_SPAWN_MIN = 4096;
 
 // The reference's std::sort permutation (introsort.h) with the independent
 // right-hand sub-ranges of large partitions sorted on other threads: each
@@ -87,11 +102,11 @@ static void sort_subrange(SortArr a, int lo, int hi, int depth, std::atomic<int>
         const int mid = lo + (hi - lo) / 2;
         sort_median_to_first(a, lo, lo + 1, mid, hi - 1);
         const int cut = sort_partition(a, lo + 1, hi, lo);
-        if (hi - cut > 65536 && spare.fetch_sub(1) > 0) {
+        if (hi - cut > SORT_SPAWN_MIN && spare.fetch_sub(1) > 0) {
             std::lock_guard<std::mutex> l(mu);
             spawned.emplace_back([=, &spare, &spawned, &mu] { sort_subrange(a, cut, hi, depth, spare, spawned, mu); });
         } else {
-            if (hi - cut > 65536) spare.fetch_add(1);
+            if (hi - cut > SORT_SPAWN_MIN) spare.fetch_add(1);
             sort_subrange(a, cut, hi, depth, spare, spawned, mu);
         }
         hi = cut;
@@ -250,7 +265,9 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
         const int zd = 2 * rz + 1;
         std::vector<std::vector<double>> kz(zd);
         std::vector<std::vector<int>> oz(zd);
-        parallel_for(zd, threads, [&](long long lo, long long hi) {
+        parallel_for(
+            zd, threads,
+            [&](long long lo, long long hi) {
             for (long long zi = lo; zi < hi; ++zi) {
                 const int z = (int)zi - rz;
                 for (int y = -ry; y <= ry; ++y)
@@ -262,7 +279,8 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
                         }
                     }
             }
-        });
+            },
+            std::max<long long>(1, 4096 / ((long long)xd * yd)));
         size_t total = 0;
         for (auto &v : kz) total += v.size();
         keys.reserve(total);
@@ -448,6 +466,80 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     P.px = 32 * ((P.ext[0] + 31) / 32);
     P.nseg = (nx + 31) / 32;
     P.wpr = P.nseg + 2 * (P.px / 32) + 2;
+
+    // ---- reach of the searches and the shared-memory table box ----
+    for (int a = 0; a < 3; ++a) P.reach[a] = std::max(P.ext[a], P.any_clean ? 2 * p.radii[a] : 0);
+    choose_hot_box(P, (double)informed.size() / (double)std::max<long long>(1, P.size), HOT_TABLE_ENTRIES);
+}
+
+void choose_hot_box(Plan &P, double density, long long budget) {
+    int cap[3];
+    for (int a = 0; a < 3; ++a) cap[a] = std::max(0, std::min(P.trunc[a], P.B[a]));
+    P.hot[0] = P.hot[1] = P.hot[2] = 0;
+    const long long len = (long long)P.tmpl.size();
+    if (len < 2 || budget < 1) return;
+    const double expect = (double)P.nmax / std::max(density, 1e-9);
+    const long long K = std::max<long long>(2, std::min<long long>(len, (long long)std::ceil(expect)));
+    const int SAMPLE = 384;
+    std::vector<int> pick;
+    const long long m = std::min<long long>(K, SAMPLE);
+    for (long long i = 0; i < m; ++i) pick.push_back((int)(i * K / m));
+    // histogram over |dx| <= cap0, |dy| <= cap1, 0 <= dz <= cap2 (folded)
+    const int mx = cap[0] + 1, my = cap[1] + 1, mz = cap[2] + 1;
+    std::vector<double> h((size_t)mx * my * mz, 0.0);
+    double total = 0;
+    for (size_t i = 0; i < pick.size(); ++i)
+        for (size_t j = i + 1; j < pick.size(); ++j) {
+            const TemplateEntry &a = P.tmpl[pick[i]], &b = P.tmpl[pick[j]];
+            int dx = a.dx - b.dx, dy = a.dy - b.dy, dz = a.dz - b.dz;
+            if (dz < 0) {
+                dx = -dx;
+                dy = -dy;
+                dz = -dz;
+            }
+            total += 1;
+            dx = std::abs(dx);
+            dy = std::abs(dy);
+            if (dx > cap[0] || dy > cap[1] || dz > cap[2]) continue;
+            h[((size_t)dz * my + dy) * mx + dx] += 1;
+        }
+    // prefix sums: cum(x, y, z) = pairs with |dx| <= x, |dy| <= y, dz <= z
+    for (int z = 0; z < mz; ++z)
+        for (int y = 0; y < my; ++y)
+            for (int x = 0; x < mx; ++x) {
+                double v = h[((size_t)z * my + y) * mx + x];
+                if (x) v += h[((size_t)z * my + y) * mx + x - 1];
+                if (y) v += h[((size_t)z * my + y - 1) * mx + x];
+                if (z) v += h[((size_t)(z - 1) * my + y) * mx + x];
+                if (x && y) v -= h[((size_t)z * my + y - 1) * mx + x - 1];
+                if (x && z) v -= h[((size_t)(z - 1) * my + y) * mx + x - 1];
+                if (y && z) v -= h[((size_t)(z - 1) * my + y - 1) * mx + x];
+                if (x && y && z) v -= h[((size_t)(z - 1) * my + y - 1) * mx + x - 1];
+                h[((size_t)z * my + y) * mx + x] = v;
+            }
+    // every (hy, hz) with the widest hx the budget allows; the box serving
+    // the most sampled pairs wins (ties: the smaller box)
+    int b[3] = {0, 0, 0};
+    double best = -1;
+    long long best_size = 0;
+    for (int z = 0; z < mz; ++z)
+        for (int y = 0; y < my; ++y) {
+            const long long rows = (long long)(2 * y + 1) * (z + 1);
+            if (rows > budget) continue;
+            const int x = (int)std::min<long long>(cap[0], (budget / rows - 1) / 2);
+            const double served = h[((size_t)z * my + y) * mx + x];
+            const int c[3] = {x, y, z};
+            const long long size = hot_entries(c);
+            if (served > best || (served == best && size < best_size)) {
+                best = served;
+                best_size = size;
+                b[0] = x;
+                b[1] = y;
+                b[2] = z;
+            }
+        }
+    (void)total;
+    for (int a = 0; a < 3; ++a) P.hot[a] = b[a];
 }
 
 void fill_cov_table(std::vector<double> &table, const int B[3], const KrigingParams &p, int threads) {

@@ -23,7 +23,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
                 ("systems", C.c_longlong), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("wall_s", C.c_double), ("systems_per_s", C.c_double), ("peak_inflight", C.c_int),
-                ("peak_bytes", C.c_longlong)]
+                ("peak_bytes", C.c_longlong), ("mean_plan_ms", C.c_double), ("mean_wait_ms", C.c_double),
+                ("mean_run_ms", C.c_double)]
 
 
 def _bind():

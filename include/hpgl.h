@@ -460,6 +460,10 @@ typedef struct hpgl_b200_server_stats_t {
     double systems_per_s;
     int peak_inflight;
     long long peak_bytes;
+    /* where the completed jobs' time went, means over the jobs: host
+       planning, waiting for admission (a stream slot and HBM budget), and
+       the run on the device with its copies (upload, kernels, download) */
+    double mean_plan_ms, mean_wait_ms, mean_run_ms;
 } hpgl_b200_server_stats_t;
 /* Returns NULL on error (see hpgl_get_last_exception_message). */
 hpgl_b200_server_t *hpgl_b200_server_create(const hpgl_b200_server_config_t *config);
