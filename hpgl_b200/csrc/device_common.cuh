@@ -135,4 +135,32 @@ struct RefineGate {
     }
 };
 
+// Per-warp guess of whether the mixed path will route a system.  A system
+// the FP32 factorisation or the refinement cannot take costs the FP32
+// attempt and then the FP64 re-solve, so where most systems are routed
+// (ill-conditioned models, clustered data) attempting loses to the FP64
+// path alone.  A warp keeps an average of its recent attempts' outcomes
+// (weight 1/4 for the newest); below 1/2 it stops attempting and routes its
+// systems straight to the FP64 re-solve, attempting every 8th again to
+// notice when its nodes become well conditioned.  The warp's node sequence
+// is fixed by the launch, so the choice is the same on every run; routed
+// systems get the FP64 path's results, which the mixed results match
+// within their tolerance either way.
+struct RouteGuess {
+    float ok = 1.f;
+    int skipped = 0;
+    __device__ __forceinline__ bool attempt() {
+        if (ok >= 0.5f || skipped >= 7) {
+            skipped = 0;
+            return true;
+        }
+        ++skipped;
+        return false;
+    }
+    // outcome: -1 no system, 0 solved, 1 routed
+    __device__ __forceinline__ void record(bool attempted, int outcome) {
+        if (attempted && outcome >= 0) ok = 0.75f * ok + (outcome == 0 ? 0.25f : 0.f);
+    }
+};
+
 }  // namespace hpgl_b200

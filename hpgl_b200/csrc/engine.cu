@@ -93,6 +93,7 @@ struct Arena {
     size_t o_values, o_codes, o_mask, o_mean, o_out_values, o_out_codes, o_out_mask, o_probs, o_pk, o_status,
         o_variance, o_weights, o_nb, o_nbcount, o_untouched, o_routed, o_counters, o_skey, o_sidx, o_svalues,
         o_smask, o_cross;
+    size_t in_total;  // the inputs (mask, values or codes, mean cubes) come first: [0, in_total)
     size_t total;
     long long cluster_warps;
 };
@@ -116,8 +117,18 @@ struct JobState {
     double cok_coef = 0, cok_svar = 0;
     std::vector<double> cross_table;  // Markov model II: the secondary model's table
     Arena ar;
-    char *base = nullptr;
+    // Device addresses: offsets below ar.in_total from in_base (the inputs),
+    // the others from rest + (off - in_total).  One arena: in_base = the
+    // arena, rest = arena + in_total (set_arena); inputs uploaded on their
+    // own (the synchronous calls): in_base = that buffer, rest = the arena.
+    char *in_base = nullptr;
+    char *rest = nullptr;
 };
+
+static void set_arena(JobState &S, char *arena) {
+    S.in_base = arena;
+    S.rest = arena + S.ar.in_total;
+}
 
 static KrigingParams to_params(const hpgl_ik_params_t &p) {
     KrigingParams k;
@@ -146,6 +157,28 @@ static void check_result(const JobState &S, const hpgl_b200_result_t &res) {
 }
 
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// The arena's first part, the job's inputs: mask, values or codes, mean
+// cubes (from S.job, S.size, S.K); returns its size.
+static size_t layout_inputs(JobState &S) {
+    const hpgl_b200_job_t &job = S.job;
+    const bool cont = kind_is_cont(job.kind);
+    const size_t n = (size_t)S.size;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += align_up(bytes ? bytes : 1);
+        return o;
+    };
+    Arena &A = S.ar;
+    A.o_mask = take(n);
+    A.o_values = cont ? take(n * 4) : 0;
+    A.o_codes = cont ? 0 : take(n);
+    S.sis_lvm = job.sequential && job.kind == KIND_IK && job.category_means;
+    A.o_mean = job.kind == KIND_LVM ? take(n * 4) : (S.sis_lvm ? take(n * S.K * 4) : 0);
+    A.in_total = off;
+    return off;
+}
 
 // Host planning and arena layout (no device work).
 static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_result_t &res) {
@@ -263,18 +296,13 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
 
     // arena layout
     const size_t n = (size_t)S.size, slots = n * S.status_stride;
-    size_t off = 0;
+    size_t off = layout_inputs(S);
     auto take = [&](size_t bytes) {
         size_t o = off;
         off += align_up(bytes ? bytes : 1);
         return o;
     };
     Arena &A = S.ar;
-    A.o_mask = take(n);
-    A.o_values = cont ? take(n * 4) : 0;
-    A.o_codes = cont ? 0 : take(n);
-    S.sis_lvm = job.sequential && job.kind == KIND_IK && job.category_means;
-    A.o_mean = job.kind == KIND_LVM ? take(n * 4) : (S.sis_lvm ? take(n * S.K * 4) : 0);
     A.o_out_values = cont ? take(n * 4) : 0;
     A.o_out_codes = cont ? 0 : take(n);
     A.o_out_mask = take(n);
@@ -322,24 +350,41 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
 
 template <typename T>
 static T *at(const JobState &S, size_t off) {
-    return reinterpret_cast<T *>(S.base + off);
+    return reinterpret_cast<T *>(off < S.ar.in_total ? S.in_base + off : S.rest + (off - S.ar.in_total));
 }
 
-static void upload(JobState &S, cudaStream_t s) {
+// The job's input arrays, in the arena's input layout: (offset, host
+// address, bytes).
+struct InputPart {
+    size_t off;
+    const void *src;
+    size_t bytes;
+};
+static std::vector<InputPart> input_parts(const JobState &S) {
     const hpgl_b200_job_t &job = S.job;
     const size_t n = (size_t)S.size;
     const Arena &A = S.ar;
-    CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_mask), job.mask, n, cudaMemcpyHostToDevice, s));
-    if (kind_is_cont(job.kind))
-        CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_values), job.values, n * 4, cudaMemcpyHostToDevice, s));
-    else
-        CUDA_CHECK(cudaMemcpyAsync(at<uint8_t>(S, A.o_codes), job.codes, n, cudaMemcpyHostToDevice, s));
-    if (job.kind == KIND_LVM)
-        CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_mean), job.mean, n * 4, cudaMemcpyHostToDevice, s));
+    std::vector<InputPart> v;
+    v.push_back({A.o_mask, job.mask, n});
+    if (kind_is_cont(job.kind)) v.push_back({A.o_values, job.values, n * 4});
+    else v.push_back({A.o_codes, job.codes, n});
+    if (job.kind == KIND_LVM) v.push_back({A.o_mean, job.mean, n * 4});
     if (S.sis_lvm)
-        for (int k = 0; k < S.K; ++k)
-            CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_mean) + (size_t)k * n, job.category_means[k], n * 4,
-                                       cudaMemcpyHostToDevice, s));
+        for (int k = 0; k < S.K; ++k) v.push_back({A.o_mean + (size_t)k * n * 4, job.category_means[k], n * 4});
+    return v;
+}
+
+static void upload_inputs(JobState &S, cudaStream_t s) {
+    for (const InputPart &p : input_parts(S))
+        CUDA_CHECK(cudaMemcpyAsync(at<char>(S, p.off), p.src, p.bytes, cudaMemcpyHostToDevice, s));
+}
+
+// Everything but the inputs: marginal probabilities, cokriging data, the
+// plans (template, table, clusterizer buckets); fills the device plans.
+static void upload_rest(JobState &S, cudaStream_t s) {
+    const hpgl_b200_job_t &job = S.job;
+    const size_t n = (size_t)S.size;
+    const Arena &A = S.ar;
     CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_pk), S.pk.data(), S.K * 4, cudaMemcpyHostToDevice, s));
     if (S.cok) {
         CUDA_CHECK(cudaMemcpyAsync(at<float>(S, A.o_svalues), job.secondary_values, n * 4, cudaMemcpyHostToDevice, s));
@@ -398,6 +443,11 @@ static void upload(JobState &S, cudaStream_t s) {
         d.hsyx = d.hsx * (2 * P.hot[1] + 1);
         d.packed_ok = P.reach[0] <= 511 && P.reach[1] <= 511 && P.reach[2] <= 255;
     }
+}
+
+static void upload(JobState &S, cudaStream_t s) {
+    upload_inputs(S, s);
+    upload_rest(S, s);
 }
 
 static DevJob make_devjob(const JobState &S, const Group &g) {
@@ -559,7 +609,28 @@ static Counters read_counters(const JobState &S, cudaStream_t s) {
     return c;
 }
 
-static void download(const JobState &S, hpgl_b200_result_t &res, const Counters &cnt, cudaStream_t s) {
+// memcpy on up to host_threads() threads, at least 4 MiB each.
+static void parallel_copy(void *dst, const void *src, size_t bytes) {
+    const size_t grain = 4u << 20;
+    const int threads = (int)std::max<size_t>(1, std::min<size_t>((size_t)host_threads(), bytes / grain));
+    if (threads == 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t chunk = (bytes + threads - 1) / threads;
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) {
+        const size_t lo = (size_t)t * chunk, hi = std::min(bytes, lo + chunk);
+        if (lo >= hi) break;
+        pool.emplace_back([=] { memcpy((char *)dst + lo, (const char *)src + lo, hi - lo); });
+    }
+    for (auto &th : pool) th.join();
+}
+
+// staging: pinned host memory of at least the main outputs' size (the
+// estimate or codes and the mask), or null for direct copies.
+static void download(const JobState &S, hpgl_b200_result_t &res, const Counters &cnt, cudaStream_t s,
+                     char *staging = nullptr) {
     const hpgl_b200_job_t &job = S.job;
     const Arena &A = S.ar;
     const size_t n = (size_t)S.size;
@@ -578,11 +649,17 @@ static void download(const JobState &S, hpgl_b200_result_t &res, const Counters 
             saved_m[i] = res.out_mask[untouched[i]];
         }
     }
-    if (kind_is_cont(job.kind))
-        CUDA_CHECK(cudaMemcpyAsync(res.out_values, at<float>(S, A.o_out_values), n * 4, cudaMemcpyDeviceToHost, s));
-    else
-        CUDA_CHECK(cudaMemcpyAsync(res.out_codes, at<uint8_t>(S, A.o_out_codes), n, cudaMemcpyDeviceToHost, s));
-    CUDA_CHECK(cudaMemcpyAsync(res.out_mask, at<uint8_t>(S, A.o_out_mask), n, cudaMemcpyDeviceToHost, s));
+    const bool cont = kind_is_cont(job.kind);
+    void *out_main = cont ? (void *)res.out_values : (void *)res.out_codes;
+    const size_t main_bytes = cont ? n * 4 : n;
+    const void *dev_main = cont ? (const void *)at<float>(S, A.o_out_values) : (const void *)at<uint8_t>(S, A.o_out_codes);
+    if (staging) {
+        CUDA_CHECK(cudaMemcpyAsync(staging, dev_main, main_bytes, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(staging + main_bytes, at<uint8_t>(S, A.o_out_mask), n, cudaMemcpyDeviceToHost, s));
+    } else {
+        CUDA_CHECK(cudaMemcpyAsync(out_main, dev_main, main_bytes, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(res.out_mask, at<uint8_t>(S, A.o_out_mask), n, cudaMemcpyDeviceToHost, s));
+    }
     const size_t slots = n * S.status_stride;
     if (res.status) CUDA_CHECK(cudaMemcpyAsync(res.status, at<int8_t>(S, A.o_status), slots, cudaMemcpyDeviceToHost, s));
     if (res.variance)
@@ -596,6 +673,10 @@ static void download(const JobState &S, hpgl_b200_result_t &res, const Counters 
                                      wn * 8, slots, cudaMemcpyDeviceToHost, s));
     }
     CUDA_CHECK(cudaStreamSynchronize(s));
+    if (staging) {
+        parallel_copy(out_main, staging, main_bytes);
+        parallel_copy(res.out_mask, staging + main_bytes, n);
+    }
     for (int i = 0; i < cnt.n_untouched; ++i) {
         res.out_values[untouched[i]] = saved_v[i];
         res.out_mask[untouched[i]] = saved_m[i];
@@ -611,6 +692,10 @@ struct SyncContext {
     cudaStream_t stream = nullptr;
     char *arena = nullptr;
     size_t cap = 0;
+    char *inputs = nullptr;   // the job's inputs, uploaded while it is planned
+    size_t in_cap = 0;
+    char *pinned = nullptr;   // host staging of the inputs and the main outputs
+    size_t pinned_cap = 0;
     unsigned char *sim = nullptr;  // sequential simulation's scratch (grows, kept)
     size_t sim_cap = 0;
     char *flush = nullptr;
@@ -639,6 +724,24 @@ static void sync_arena(SyncContext &C, size_t bytes) {
     C.cap = bytes;
 }
 
+static void sync_inputs(SyncContext &C, size_t bytes) {
+    if (bytes <= C.in_cap) return;
+    if (C.inputs) cudaFree(C.inputs);
+    C.inputs = nullptr;
+    C.in_cap = 0;
+    CUDA_CHECK(cudaMalloc(&C.inputs, bytes));
+    C.in_cap = bytes;
+}
+
+static void sync_pinned(SyncContext &C, size_t bytes) {
+    if (bytes <= C.pinned_cap) return;
+    if (C.pinned) cudaFreeHost(C.pinned);
+    C.pinned = nullptr;
+    C.pinned_cap = 0;
+    CUDA_CHECK(cudaMallocHost(&C.pinned, bytes));
+    C.pinned_cap = bytes;
+}
+
 static void sync_sim(SyncContext &C, size_t bytes) {
     if (bytes <= C.sim_cap) return;
     if (C.sim) cudaFree(C.sim);
@@ -654,24 +757,85 @@ static void sync_sim(SyncContext &C, size_t bytes) {
 // place and copied out.
 static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::chrono::steady_clock::time_point t0);
 
+// The inputs of a kriging job can be uploaded before it is planned: its
+// arrays are present and its grid is valid (prepare() reports anything else).
+static bool early_inputs(const hpgl_b200_job_t &job) {
+    if (job.sequential || job.kind < 0 || job.kind > 6 || kind_is_cokriging(job.kind)) return false;
+    if (job.nx <= 0 || job.ny <= 0 || job.nz <= 0) return false;
+    if ((long long)job.nx * job.ny * job.nz > 2147483647LL) return false;
+    if (!job.mask || !job.params || job.n_params < 1) return false;
+    if (kind_is_cont(job.kind) ? !job.values : !job.codes) return false;
+    if (job.kind == KIND_LVM && !job.mean) return false;
+    return true;
+}
+
 void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     auto t0 = std::chrono::steady_clock::now();
     JobState S;
-    prepare(S, job, res);
-    res.ms_plan = ms_since(t0);
-    if (job.sequential) {
-        std::lock_guard<std::mutex> lock(g_sync_mutex);
-        sgs_run(S, res, sync_ctx(), t0);
-        return;
+    if (job.sequential || !early_inputs(job)) {
+        prepare(S, job, res);
+        res.ms_plan = ms_since(t0);
+        if (job.sequential) {
+            std::lock_guard<std::mutex> lock(g_sync_mutex);
+            sgs_run(S, res, sync_ctx(), t0);
+            return;
+        }
     }
     std::lock_guard<std::mutex> lock(g_sync_mutex);
     SyncContext &C = sync_ctx();
-    auto t1 = std::chrono::steady_clock::now();
-    sync_arena(C, S.ar.total);
-    S.base = C.arena;
-    upload(S, C.stream);
-    CUDA_CHECK(cudaStreamSynchronize(C.stream));
-    res.ms_h2d = ms_since(t1);
+    char *staging = nullptr;
+    if (early_inputs(job)) {
+        // The inputs go to pinned staging and on to the device on a helper
+        // thread while this one plans the job; the same layout function
+        // places them in both.
+        S.job = job;
+        S.size = (long long)job.nx * job.ny * job.nz;
+        S.K = job.kind == KIND_IK ? job.n_params : 1;
+        const size_t in_total = layout_inputs(S);
+        const size_t n = (size_t)S.size;
+        const size_t out_bytes = (kind_is_cont(job.kind) ? n * 4 : n) + n;
+        sync_inputs(C, in_total);
+        sync_pinned(C, std::max(in_total, out_bytes));
+        staging = C.pinned;
+        const std::vector<InputPart> parts = input_parts(S);
+        std::exception_ptr copy_error;
+        std::thread copier([&] {
+            try {
+                for (const InputPart &p : parts) parallel_copy(C.pinned + p.off, p.src, p.bytes);
+                CUDA_CHECK(cudaMemcpyAsync(C.inputs, C.pinned, in_total, cudaMemcpyHostToDevice, C.stream));
+            } catch (...) {
+                copy_error = std::current_exception();
+            }
+        });
+        try {
+            prepare(S, job, res);
+        } catch (...) {
+            copier.join();
+            cudaStreamSynchronize(C.stream);
+            throw;
+        }
+        res.ms_plan = ms_since(t0);
+        copier.join();
+        if (copy_error) {
+            cudaStreamSynchronize(C.stream);
+            std::rethrow_exception(copy_error);
+        }
+        if (S.ar.in_total != in_total) throw HpglError{HPGL_E_INTERNAL, "input layout changed while planning"};
+        auto t1 = std::chrono::steady_clock::now();
+        sync_arena(C, S.ar.total - in_total);
+        S.in_base = C.inputs;
+        S.rest = C.arena;
+        upload_rest(S, C.stream);
+        CUDA_CHECK(cudaStreamSynchronize(C.stream));
+        res.ms_h2d = ms_since(t1);
+    } else {
+        auto t1 = std::chrono::steady_clock::now();
+        sync_arena(C, S.ar.total);
+        set_arena(S, C.arena);
+        upload(S, C.stream);
+        CUDA_CHECK(cudaStreamSynchronize(C.stream));
+        res.ms_h2d = ms_since(t1);
+    }
     cudaEvent_t e0, e1;
     CUDA_CHECK(cudaEventCreate(&e0));
     CUDA_CHECK(cudaEventCreate(&e1));
@@ -688,7 +852,7 @@ void run_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res) {
     cudaEventDestroy(e1);
     res.ms_device = ms;
     auto t2 = std::chrono::steady_clock::now();
-    download(S, res, cnt, C.stream);
+    download(S, res, cnt, C.stream, staging);
     res.ms_d2h = ms_since(t2);
     res.ms_total = ms_since(t0);
 }
@@ -713,7 +877,7 @@ static void sgs_run(JobState &S, hpgl_b200_result_t &res, SyncContext &C, std::c
     auto t1 = std::chrono::steady_clock::now();
     cudaStream_t s = C.stream;
     sync_arena(C, S.ar.total);
-    S.base = C.arena;
+    set_arena(S, C.arena);
     upload(S, s);
     const long long nsim = (long long)path.nodes.size();
     const int window = g_sim_window.load();
@@ -868,7 +1032,7 @@ void bench_job(const hpgl_b200_job_t &job, hpgl_b200_result_t &res, hpgl_b200_be
     std::lock_guard<std::mutex> lock(g_sync_mutex);
     SyncContext &C = sync_ctx();
     sync_arena(C, S.ar.total);
-    S.base = C.arena;
+    set_arena(S, C.arena);
     upload(S, C.stream);
     if (bench.flush_bytes > (long long)C.flush_cap) {
         if (C.flush) cudaFree(C.flush);
@@ -964,7 +1128,7 @@ void autotune_job(const hpgl_b200_job_t &job, hpgl_b200_tune_t &rep) {
     std::lock_guard<std::mutex> lock(g_sync_mutex);
     SyncContext &C = sync_ctx();
     sync_arena(C, S.ar.total);
-    S.base = C.arena;
+    set_arena(S, C.arena);
     upload(S, C.stream);
     const size_t flush = 256u << 20;
     if (C.flush_cap < flush) {
@@ -1110,7 +1274,7 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
         cudaStream_t s = streams[slot];
         void *arena = nullptr;
         CUDA_CHECK(cudaMallocAsync(&arena, S.ar.total, s));
-        S.base = (char *)arena;
+        set_arena(S, (char *)arena);
         try {
             upload(S, s);
             device_pass(S, s, nullptr, nullptr);

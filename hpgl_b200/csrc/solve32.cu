@@ -495,20 +495,27 @@ __device__ __forceinline__ float get2(const float2 (&m2)[N32 / 2]) {
 
 // One node of the mixed path (FP32 inverse + FP64 refinement); systems that
 // do not qualify are appended to J.routed.  HOT: the system is built from
-// the block's shared-memory box of the table (SysSmemH).
+// the block's shared-memory box of the table (SysSmemH).  skip: a system
+// is appended to J.routed at once, without the FP32 attempt.  Returns -1
+// when the node needs no system, 0 when it was solved here, 1 when routed.
 template <bool HOT, typename SM>
-__device__ __forceinline__ void mixed32_node(const DevJob &J, const DevPlan &P, SM &S, const double *hot,
-                                             const NodeFetch &cur, int lane) {
+__device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, SM &S, const double *hot,
+                                            const NodeFetch &cur, int lane, bool skip = false) {
     const bool ordinary = J.kind == 0;
     const double inv_c0 = 1.0 / P.c0;
     const int node = cur.node;
-    if (copy_informed(J, cur, lane)) return;
+    if (copy_informed(J, cur, lane)) return -1;
+    if (skip && cur.n > 0) {
+        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        __syncwarp();
+        return 1;
+    }
     NodeData d;
     if constexpr (HOT) d = load_node_h(J, P, S, hot, cur, lane);
     else d = load_node(J, P, S, cur, lane);
     if (d.n <= 0) {
         write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
-        return;
+        return -1;
     }
     const int n = d.n;
     if constexpr (HOT) build_full32h(J, P, hot, S, n, lane);
@@ -552,7 +559,7 @@ __device__ __forceinline__ void mixed32_node(const DevJob &J, const DevPlan &P, 
             J.routed[pos] = node;
         }
         __syncwarp();
-        return;
+        return 1;
     }
     // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
     // refined with FP64 residuals.
@@ -586,7 +593,7 @@ __device__ __forceinline__ void mixed32_node(const DevJob &J, const DevPlan &P, 
             J.routed[pos] = node;
         }
         __syncwarp();
-        return;
+        return 1;
     }
     if (lane >= n) {
         xa = 0.0;
@@ -606,6 +613,7 @@ __device__ __forceinline__ void mixed32_node(const DevJob &J, const DevPlan &P, 
     }
     write_outputs(J, P, S, node, lane, d, ST_SUCCESS, w, variance);
     __syncwarp();
+    return 0;
 }
 
 __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPlan P) {
@@ -615,10 +623,12 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
     const long long stride = (long long)gridDim.x * WARPS32;
     long long it = (long long)blockIdx.x * WARPS32 + warp;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+    RouteGuess guess;
     for (; it < J.size; it += stride) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
-        mixed32_node<false>(J, P, S, nullptr, cur, lane);
+        const bool attempt = guess.attempt();
+        guess.record(attempt, mixed32_node<false>(J, P, S, nullptr, cur, lane, !attempt));
         __syncwarp();
     }
 }
@@ -761,10 +771,12 @@ __global__ void __launch_bounds__(HOT_WARPS * 32, 1) k_solve_mixed32h(DevJob J, 
     const long long stride = (long long)gridDim.x * HOT_WARPS;
     long long it = (long long)blockIdx.x * HOT_WARPS + warp;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+    RouteGuess guess;
     for (; it < J.size; it += stride) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
-        mixed32_node<true>(J, P, S, hot, cur, lane);
+        const bool attempt = guess.attempt();
+        guess.record(attempt, mixed32_node<true>(J, P, S, hot, cur, lane, !attempt));
         __syncwarp();
     }
 }

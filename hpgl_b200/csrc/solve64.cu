@@ -595,20 +595,27 @@ __device__ __forceinline__ void residual64(const Mixed64Smem &S, const int *cs, 
 }
 
 // One node of the mixed path; systems that do not qualify are appended to
-// J.routed.
-__device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, Mixed64Smem &S, const int *cs,
-                                             const NodeFetch &cur, int lane) {
+// J.routed.  skip: a system is appended at once, without the FP32 attempt.
+// Returns -1 when the node needs no system, 0 when solved here, 1 when
+// routed.
+__device__ __forceinline__ int mixed64_node(const DevJob &J, const DevPlan &P, Mixed64Smem &S, const int *cs,
+                                            const NodeFetch &cur, int lane, bool skip = false) {
     const bool ordinary = J.kind == 0;
     const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0)
     const double inv_c0 = 1.0 / P.c0;
     const int r0 = lane, r1 = lane + 32;
     const int cs0 = cs[r0], cs1 = cs[r1];
     const int node = cur.node;
-    if (copy_informed64(J, cur, lane)) return;
+    if (copy_informed64(J, cur, lane)) return -1;
+    if (skip && cur.n > 0) {
+        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        __syncwarp();
+        return 1;
+    }
     const Node64 d = load_node64(J, P, S.nb, cur, lane);
     if (d.n <= 0) {
         write_outputs64(J, P, node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
-        return;
+        return -1;
     }
     const int n = d.n;
     build_packed<false>(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane, nullptr);
@@ -688,7 +695,7 @@ __device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, 
     if (low) {
         if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
         __syncwarp();
-        return;
+        return 1;
     }
     // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
     // refined with FP64 residuals.
@@ -734,7 +741,7 @@ __device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, 
     if (!converged) {
         if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
         __syncwarp();
-        return;
+        return 1;
     }
     if (r0 >= n) xa0 = xb0 = 0.0;
     if (r1 >= n) xa1 = xb1 = 0.0;
@@ -754,6 +761,7 @@ __device__ __forceinline__ void mixed64_node(const DevJob &J, const DevPlan &P, 
     }
     write_outputs64(J, P, node, lane, d, ST_SUCCESS, w0, w1, variance);
     __syncwarp();
+    return 0;
 }
 
 __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
@@ -765,10 +773,12 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     Mixed64Smem &S = *reinterpret_cast<Mixed64Smem *>(dyn_smem);
     long long it = blockIdx.x;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+    RouteGuess guess;
     for (; it < J.size; it += gridDim.x) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + gridDim.x < J.size ? (int)(it + gridDim.x) : -1, lane);
-        mixed64_node(J, P, S, s_cs, cur, lane);
+        const bool attempt = guess.attempt();
+        guess.record(attempt, mixed64_node(J, P, S, s_cs, cur, lane, !attempt));
         __syncwarp();
     }
 }
