@@ -766,6 +766,13 @@ static bool early_inputs(const hpgl_b200_job_t &job) {
     if (!job.mask || !job.params || job.n_params < 1) return false;
     if (kind_is_cont(job.kind) ? !job.values : !job.codes) return false;
     if (job.kind == KIND_LVM && !job.mean) return false;
+    if (job.kind != KIND_IK && job.n_params != 1) return false;
+    if (job.kind == KIND_IK && job.n_params > 255) return false;
+    try {
+        for (int k = 0; k < job.n_params; ++k) validate_params(to_params(job.params[k]), job.kind);
+    } catch (const std::exception &) {
+        return false;
+    }
     return true;
 }
 
