@@ -298,10 +298,13 @@ def main():
     del ref64, mix
 
     # Roofline of the dominant kernel (the solve): algorithmic flops per
-    # launch / CUDA-event duration; FP32 CUDA-core peak (nominal: 148 SMs x
-    # 128 FP32 lanes x 2 flop x 1.965 GHz).
-    peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
+    # launch / CUDA-event duration, against the FP32 CUDA-core rate measured
+    # here by an FMA-loop kernel timed alone (hpgl_b200_fma_peak; the
+    # measured-peaks file holds HBM and bf16-tensor figures only).
+    peak_fp32 = N.fma_peak("mixed")
+    peak_fp64 = N.fma_peak("fp64")
     achieved = flops / (info_m["ms_top_kernel"] / 1000.0) / 1e12
+    achieved64 = flops / (info_f["ms_top_kernel"] / 1000.0) / 1e12
     traffic = None
     try:
         tj = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[info_m["top_kernel"]]
@@ -311,8 +314,10 @@ def main():
         pass
     roofline = {"kernel": info_m["top_kernel"], "bound": "fp32", "achieved": achieved, "peak": peak_fp32,
                 "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic, "traffic_unit": "bytes/launch",
-                "peak_source": "nominal FP32 CUDA-core peak (MEASURED_PEAKS.json has HBM and bf16 tensor only)",
-                "ms_per_launch": info_m["ms_top_kernel"], "flop_per_launch": flops}
+                "peak_source": "measured FP32 CUDA-core rate, FMA-loop kernel timed alone (hpgl_b200_fma_peak)",
+                "ms_per_launch": info_m["ms_top_kernel"], "flop_per_launch": flops,
+                "fp64_solve": {"kernel": info_f["top_kernel"], "achieved": achieved64, "peak": peak_fp64,
+                               "frac": achieved64 / peak_fp64, "ms_per_launch": info_f["ms_top_kernel"]}}
 
     # Serving: Poisson streams of mixed OK/SK/IK jobs (grids 32^3 ..
     # 256x256x64, ranges 5-60, 8-64 neighbours) replayed in real time

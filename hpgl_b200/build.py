@@ -27,7 +27,7 @@ CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-f
 CXX_FLAGS = ["-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wno-unused-function",
              "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include"]
 
-SOURCES_CU = ["kernels.cu", "solve32.cu", "solve64.cu", "cokriging.cu", "engine.cu", "sk_weights.cu", "textio.cu", "variogram.cu"]
+SOURCES_CU = ["kernels.cu", "solve32.cu", "solve64.cu", "cokriging.cu", "engine.cu", "sk_weights.cu", "textio.cu", "variogram.cu", "peak.cu"]
 SOURCES_CXX = ["plan.cpp", "api.cpp", "sgs_host.cpp"]
 
 

@@ -348,6 +348,13 @@ int hpgl_b200_set_launch(int family, int precision, int schedule, int blocks_per
     });
 }
 
+int hpgl_b200_fma_peak(int precision, double *tflops) {
+    return guarded("hpgl_b200_fma_peak", [&] {
+        if (precision < 0 || precision > 1 || !tflops) throw HpglError{HPGL_E_INVALID, "invalid arguments"};
+        *tflops = fma_peak_tflops(precision, 5);
+    });
+}
+
 int hpgl_b200_autotune(const hpgl_b200_job_t *job, hpgl_b200_tune_t *report) {
     return guarded("hpgl_b200_autotune", [&] {
         if (!job || !report) throw HpglError{HPGL_E_INVALID, "null argument"};

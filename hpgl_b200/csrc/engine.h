@@ -37,6 +37,10 @@ int server_wait(void *h, long long ticket, int timeout_ms, std::string &message)
 void server_stats(void *h, hpgl_b200_server_stats_t &st);
 void server_destroy(void *h);
 
+// Measured FMA-loop rate of the FP32 (precision 1) or FP64 (0) CUDA-core
+// pipe, TFLOP/s (peak.cu).
+double fma_peak_tflops(int precision, int repeats);
+
 int default_precision();
 void set_default_precision(int p);
 // Window of the speculative simulation rounds (pending nodes per round).

@@ -294,6 +294,18 @@ def autotune(job, precision="mixed", kind=None):
     return dict(candidates=cands, chosen=cands[t.chosen], family=t.family, precision=t.precision)
 
 
+def fma_peak(precision="mixed"):
+    """Measured rate (TFLOP/s) of the CUDA-core pipe a precision solves on:
+    "mixed" the FP32 pipe (packed multiply-adds), "fp64" the FP64 pipe
+    (hpgl_b200_fma_peak)."""
+    L = lib()
+    v = C.c_double(0.0)
+    rc = L.hpgl_b200_fma_peak({"fp64": 0, "mixed": 1}[precision], C.byref(v))
+    if rc != 0:
+        raise HpglError(rc, L.hpgl_get_last_exception_message().decode())
+    return v.value
+
+
 def set_launch(family, precision, schedule, blocks_per_sm=0):
     """Pins the launch setting of a family (0: <= 32 neighbours, 1: above)
     and precision ("fp64"/"mixed"): schedule "split" or "fused"."""

@@ -416,6 +416,14 @@ int hpgl_b200_autotune(const hpgl_b200_job_t *job, hpgl_b200_tune_t *report);
    on invalid arguments. */
 int hpgl_b200_set_launch(int family, int precision, int schedule, int blocks_per_sm);
 
+/* No counterpart in the reference.  The measured rate of the CUDA-core pipe
+   the solves run on: FP32 (precision 1, packed two-wide multiply-adds) or
+   FP64 (precision 0), from a kernel of independent multiply-add chains
+   timed alone (best of 5 launches after a warm-up), in TFLOP/s (2 flop per
+   multiply-add).  The roofline denominator of the solve kernels.  Returns 0,
+   or -1 (see hpgl_get_last_exception_message). */
+int hpgl_b200_fma_peak(int precision, double *tflops);
+
 /* No counterpart in the reference.  hpgl_simple_kriging_weights for callers
    that cannot allocate device memory: cudaMalloc and cudaFree synchronise
    the whole device, stalling the caller's other GPU work, and a host
