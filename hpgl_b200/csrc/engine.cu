@@ -181,7 +181,8 @@ static size_t layout_inputs(JobState &S) {
 }
 
 // Host planning and arena layout (no device work).
-static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_result_t &res) {
+// plan_threads: host threads for the planning (0: host_threads()).
+static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_result_t &res, int plan_threads = 0) {
     S.job = job;
     if (job.kind < 0 || job.kind > 6) invalid("unknown kriging kind");
     if (job.nx <= 0 || job.ny <= 0 || job.nz <= 0) invalid("grid dimensions must be positive");
@@ -217,7 +218,7 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
         if (!same_system(kp[0], kp[k])) S.per_category = true;
     S.status_stride = S.per_category ? S.K : 1;
     S.nmax_all = 0;
-    const int threads = host_threads();
+    const int threads = plan_threads > 0 ? plan_threads : host_threads();
     if (S.per_category) {
         S.groups.resize(S.K);
         for (int k = 0; k < S.K; ++k) {
@@ -1257,7 +1258,8 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
     try {
         CUDA_CHECK(cudaSetDevice(device));
         const auto t_plan = std::chrono::steady_clock::now();
-        prepare(S, sj->job, *sj->result);
+        // several jobs plan at once: each gets its share of the host threads
+        prepare(S, sj->job, *sj->result, std::max(1, host_threads() / std::max(1, (int)workers.size())));
         sj->plan_ms = ms_since(t_plan);
         bytes = (long long)S.ar.total;
         if (bytes > budget)

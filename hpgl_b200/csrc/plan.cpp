@@ -218,131 +218,18 @@ double informed_mean(const float *values, const uint8_t *mask, long long size) {
     return count == 0 ? 0 : sum / count;
 }
 
-void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
-                int threads, bool sequential) {
-    static const bool timing = getenv("HPGL_B200_PLAN_TIMING") != nullptr;
-    auto t_last = std::chrono::steady_clock::now();
-    auto lap = [&](const char *what) {
-        if (!timing) return;
-        auto now = std::chrono::steady_clock::now();
-        fprintf(stderr, "plan %-10s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - t_last).count());
-        t_last = now;
-    };
-    validate_params(p, kind);
-    CovModel cov(p);
-    P.kind = kind;
-    P.nx = nx;
-    P.ny = ny;
-    P.nz = nz;
-    P.size = (long long)nx * ny * nz;
-    P.nmax = p.max_neighbours;
-    // Ordinary kriging and cokriging use the model itself; cokriging searches
-    // with neighbour_lookup_t alone (simple_cokriging_markI.cpp:201, no
-    // clusterizer).
-    P.truncated = (kind != KIND_OK && !kind_is_cokriging(kind)) || sequential;
-    P.clusterizer = !kind_is_cokriging(kind) && !sequential;
-    for (int i = 0; i < 3; ++i) P.radii[i] = p.radii[i];
-    const int rx = p.radii[0], ry = p.radii[1], rz = p.radii[2];
-
-    // ---- search template: calc_cov_field (covariance_field.h:62-106) ----
-    // C(0 - v) over the +-radius box in z-y-x order, offsets above C(0)/100
-    // kept as the vector -v, sorted descending by std::sort (the same
-    // unstable algorithm on the same input order as the reference, hence the
-    // same order of equal keys).  Every covariance object the reference can
-    // pass here (the model, the precalculated table, covariance_field_t)
-    // yields these same values inside the box.
-    const int xd = 2 * rx + 1, yd = 2 * ry + 1;
-    std::vector<double> data;
-    fill_symmetric(data, rx, ry, rz, threads, [&](int x, int y, int z) { return cov(0.0 - x, 0.0 - y, 0.0 - z); });
-    lap("box");
-    const double c0 = cov(0.0, 0.0, 0.0);
-    const double threshold = c0 / 100;
-    // Offsets -v in z-y-x order of v, keyed by C(v) (= C(-v)); collected per
-    // z-slab in parallel and concatenated in slab order.
-    std::vector<double> keys;
-    std::vector<int> order;
-    {
-        const int zd = 2 * rz + 1;
-        std::vector<std::vector<double>> kz(zd);
-        std::vector<std::vector<int>> oz(zd);
-        parallel_for(
-            zd, threads,
-            [&](long long lo, long long hi) {
-            for (long long zi = lo; zi < hi; ++zi) {
-                const int z = (int)zi - rz;
-                for (int y = -ry; y <= ry; ++y)
-                    for (int x = -rx; x <= rx; ++x) {
-                        const double k = data[((size_t)(z + rz) * yd + (y + ry)) * xd + (x + rx)];
-                        if (k > threshold) {
-                            kz[zi].push_back(k);
-                            oz[zi].push_back((int)((((size_t)(-z + rz) * yd) + (-y + ry)) * xd + (-x + rx)));
-                        }
-                    }
-            }
-            },
-            std::max<long long>(1, 4096 / ((long long)xd * yd)));
-        size_t total = 0;
-        for (auto &v : kz) total += v.size();
-        keys.reserve(total);
-        order.reserve(total);
-        for (int zi = 0; zi < zd; ++zi) {
-            keys.insert(keys.end(), kz[zi].begin(), kz[zi].end());
-            order.insert(order.end(), oz[zi].begin(), oz[zi].end());
-        }
-    }
-    parallel_reference_sort(keys, order, threads);
-    lap("sort");
-    size_t kept = keys.size();
-    for (size_t i = 0; i < keys.size(); ++i)
-        if (keys[i] < threshold) {
-            kept = i;
-            break;
-        }
-    P.tmpl.resize(kept);
-    parallel_for((long long)kept, threads, [&](long long lo, long long hi) {
-        for (long long i = lo; i < hi; ++i) {
-            const int o = order[i];
-            TemplateEntry &e = P.tmpl[i];
-            e.dx = o % xd - rx;
-            e.dy = o / xd % yd - ry;
-            e.dz = o / xd / yd - rz;
-            e.delta = e.dx + nx * (e.dy + ny * e.dz);
-        }
-    });
-    // the template's extent is that of the offsets above the threshold, which
-    // the box scan already knows
-    P.ext[0] = P.ext[1] = P.ext[2] = 0;
-    for (int z = -rz; z <= rz; ++z)
-        for (int y = -ry; y <= ry; ++y) {
-            const double *row = &data[((size_t)(z + rz) * yd + (y + ry)) * xd];
-            for (int x = -rx; x <= rx; ++x)
-                if (row[x + rx] > threshold) {
-                    P.ext[0] = std::max(P.ext[0], std::abs(x));
-                    P.ext[1] = std::max(P.ext[1], std::abs(y));
-                    P.ext[2] = std::max(P.ext[2], std::abs(z));
-                }
-        }
-    if (kept < keys.size()) {
-        // entries cut after the sort (not reachable with the > threshold
-        // filter, kept for the reference's second cut-off) do not widen ext
-        P.ext[0] = P.ext[1] = P.ext[2] = 0;
-        for (const TemplateEntry &e : P.tmpl) {
-            P.ext[0] = std::max(P.ext[0], std::abs(e.dx));
-            P.ext[1] = std::max(P.ext[1], std::abs(e.dy));
-            P.ext[2] = std::max(P.ext[2], std::abs(e.dz));
-        }
-    }
-
-    lap("template");
-    // ---- clusterizer (clusterizer.cpp:52-184) ----
-    // Boxes of the radii (doubles in the reference: sugarbox_search_ellipsoid_t),
-    // mx = (int)(nx / rx + 2); a box overflows past limit = |template| / 250
-    // (sugarbox_indexed_neighbour_lookup.h:58) and then holds no nodes.
+// ---- clusterizer (clusterizer.cpp:52-184) ----
+// Boxes of the radii (doubles in the reference: sugarbox_search_ellipsoid_t),
+// mx = (int)(nx / rx + 2); a box overflows past limit = |template| / 250
+// (sugarbox_indexed_neighbour_lookup.h:58) and then holds no nodes.  Fills
+// P's clusterizer fields (P.size and P.clusterizer set).
+static void build_buckets(Plan &P, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
+                          long long limit, int threads) {
     for (int i = 0; i < 3; ++i) P.cl_r[i] = (double)p.radii[i];
     P.mx = (int)(nx / P.cl_r[0] + 2);
     P.my = (int)(ny / P.cl_r[1] + 2);
     P.mz = (int)(nz / P.cl_r[2] + 2);
-    P.limit = (long long)(P.tmpl.size() / 250);
+    P.limit = limit;
     const long long nb = (long long)P.mx * P.my * P.mz;
     std::vector<int> count(nb, 0);
     std::vector<uint8_t> exceeded(nb, 0);
@@ -383,6 +270,7 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
         informed.reserve(total);
         for (auto &v : part) informed.insert(informed.end(), v.begin(), v.end());
     }
+    P.informed = (long long)informed.size();
     std::vector<long long> box_of(informed.size());
     for (size_t k = 0; k < informed.size(); ++k) {
         box_of[k] = bucket_of(informed[k]);
@@ -432,6 +320,143 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
                 }
             }
 
+}
+
+void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &p, const uint8_t *mask,
+                int threads, bool sequential) {
+    static const bool timing = getenv("HPGL_B200_PLAN_TIMING") != nullptr;
+    auto t_last = std::chrono::steady_clock::now();
+    auto lap = [&](const char *what) {
+        if (!timing) return;
+        auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "plan %-10s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - t_last).count());
+        t_last = now;
+    };
+    validate_params(p, kind);
+    CovModel cov(p);
+    P.kind = kind;
+    P.nx = nx;
+    P.ny = ny;
+    P.nz = nz;
+    P.size = (long long)nx * ny * nz;
+    P.nmax = p.max_neighbours;
+    // Ordinary kriging and cokriging use the model itself; cokriging searches
+    // with neighbour_lookup_t alone (simple_cokriging_markI.cpp:201, no
+    // clusterizer).
+    P.truncated = (kind != KIND_OK && !kind_is_cokriging(kind)) || sequential;
+    P.clusterizer = !kind_is_cokriging(kind) && !sequential;
+    for (int i = 0; i < 3; ++i) P.radii[i] = p.radii[i];
+    const int rx = p.radii[0], ry = p.radii[1], rz = p.radii[2];
+
+    // ---- search template: calc_cov_field (covariance_field.h:62-106) ----
+    // C(0 - v) over the +-radius box in z-y-x order, offsets above C(0)/100
+    // kept as the vector -v, sorted descending by std::sort (the same
+    // unstable algorithm on the same input order as the reference, hence the
+    // same order of equal keys).  Every covariance object the reference can
+    // pass here (the model, the precalculated table, covariance_field_t)
+    // yields these same values inside the box.
+    const int xd = 2 * rx + 1, yd = 2 * ry + 1;
+    std::vector<double> data;
+    fill_symmetric(data, rx, ry, rz, threads, [&](int x, int y, int z) { return cov(0.0 - x, 0.0 - y, 0.0 - z); });
+    lap("box");
+    const double c0 = cov(0.0, 0.0, 0.0);
+    const double threshold = c0 / 100;
+    // Offsets -v in z-y-x order of v, keyed by C(v) (= C(-v)); collected per
+    // z-slab in parallel and concatenated in slab order.
+    std::vector<double> keys;
+    std::vector<int> order;
+    // the template's extent: that of the offsets above the threshold,
+    // per slab while they are collected
+    P.ext[0] = P.ext[1] = P.ext[2] = 0;
+    {
+        const int zd = 2 * rz + 1;
+        std::vector<std::vector<double>> kz(zd);
+        std::vector<std::vector<int>> oz(zd);
+        std::vector<int> ez((size_t)zd * 3, 0);
+        parallel_for(
+            zd, threads,
+            [&](long long lo, long long hi) {
+            for (long long zi = lo; zi < hi; ++zi) {
+                const int z = (int)zi - rz;
+                int ex = 0, ey = 0;
+                for (int y = -ry; y <= ry; ++y)
+                    for (int x = -rx; x <= rx; ++x) {
+                        const double k = data[((size_t)(z + rz) * yd + (y + ry)) * xd + (x + rx)];
+                        if (k > threshold) {
+                            kz[zi].push_back(k);
+                            oz[zi].push_back((int)((((size_t)(-z + rz) * yd) + (-y + ry)) * xd + (-x + rx)));
+                            ex = std::max(ex, std::abs(x));
+                            ey = std::max(ey, std::abs(y));
+                        }
+                    }
+                ez[3 * zi] = ex;
+                ez[3 * zi + 1] = ey;
+                ez[3 * zi + 2] = kz[zi].empty() ? 0 : std::abs(z);
+            }
+            },
+            std::max<long long>(1, 4096 / ((long long)xd * yd)));
+        size_t total = 0;
+        for (auto &v : kz) total += v.size();
+        keys.reserve(total);
+        order.reserve(total);
+        for (int zi = 0; zi < zd; ++zi) {
+            keys.insert(keys.end(), kz[zi].begin(), kz[zi].end());
+            order.insert(order.end(), oz[zi].begin(), oz[zi].end());
+            for (int a = 0; a < 3; ++a) P.ext[a] = std::max(P.ext[a], ez[3 * zi + a]);
+        }
+    }
+    // Every collected key is above the threshold, so the template keeps all
+    // of them and the clusterizer's limit (|template| / 250) is known before
+    // the sort: the buckets are built on their own thread meanwhile.
+    const int bucket_threads = std::max(1, threads / 4);
+    std::exception_ptr bucket_error;
+    std::thread bucket_thread([&] {
+        try {
+            build_buckets(P, nx, ny, nz, p, mask, (long long)(keys.size() / 250), bucket_threads);
+        } catch (...) {
+            bucket_error = std::current_exception();
+        }
+    });
+    try {
+        parallel_reference_sort(keys, order, threads);
+    } catch (...) {
+        bucket_thread.join();
+        throw;
+    }
+    lap("sort");
+    size_t kept = keys.size();
+    for (size_t i = 0; i < keys.size(); ++i)
+        if (keys[i] < threshold) {
+            kept = i;
+            break;
+        }
+    P.tmpl.resize(kept);
+    parallel_for((long long)kept, threads, [&](long long lo, long long hi) {
+        for (long long i = lo; i < hi; ++i) {
+            const int o = order[i];
+            TemplateEntry &e = P.tmpl[i];
+            e.dx = o % xd - rx;
+            e.dy = o / xd % yd - ry;
+            e.dz = o / xd / yd - rz;
+            e.delta = e.dx + nx * (e.dy + ny * e.dz);
+        }
+    });
+    if (kept < keys.size()) {
+        // entries cut after the sort (not reachable with the > threshold
+        // filter, kept for the reference's second cut-off) do not widen ext
+        P.ext[0] = P.ext[1] = P.ext[2] = 0;
+        for (const TemplateEntry &e : P.tmpl) {
+            P.ext[0] = std::max(P.ext[0], std::abs(e.dx));
+            P.ext[1] = std::max(P.ext[1], std::abs(e.dy));
+            P.ext[2] = std::max(P.ext[2], std::abs(e.dz));
+        }
+    }
+
+    lap("template");
+    bucket_thread.join();
+    if (bucket_error) std::rethrow_exception(bucket_error);
+    if ((long long)(P.tmpl.size() / 250) != P.limit)
+        build_buckets(P, nx, ny, nz, p, mask, (long long)(P.tmpl.size() / 250), threads);
     lap("buckets");
     // ---- covariance table ----
     // Truncated kinds read C(v) only for |v| <= radii.  Ordinary kriging uses
@@ -469,7 +494,7 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
 
     // ---- reach of the searches and the shared-memory table box ----
     for (int a = 0; a < 3; ++a) P.reach[a] = std::max(P.ext[a], P.any_clean ? 2 * p.radii[a] : 0);
-    choose_hot_box(P, (double)informed.size() / (double)std::max<long long>(1, P.size), HOT_TABLE_ENTRIES);
+    choose_hot_box(P, (double)P.informed / (double)std::max<long long>(1, P.size), HOT_TABLE_ENTRIES);
 }
 
 void choose_hot_box(Plan &P, double density, long long budget) {

@@ -74,6 +74,7 @@ struct Plan {
     std::vector<uint8_t> bucket_clean;    // no exceeded bucket in the 3x3x3 neighbourhood
     bool any_clean = false;
     int max_candidates = 0;               // largest candidate count of a clean neighbourhood
+    long long informed = 0;               // informed nodes of the mask
 
     // padded informed-bit rows for the template search
     int px = 0;      // x padding in cells, a multiple of 32

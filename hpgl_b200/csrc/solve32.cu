@@ -476,16 +476,20 @@ template <typename SM>
 __device__ __forceinline__ double residual(const SM &S, double *vd, double x, double b, int lane) {
     vd[lane] = x;
     __syncwarp();
-    double acc = 0.0;
+    // four independent accumulation chains (the dot product's order is free
+    // on the refinement path)
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
     const double2 *x2 = reinterpret_cast<const double2 *>(vd);
 #pragma unroll
-    for (int q = 0; q < N32 / 2; ++q) {
-        const double2 u = x2[q];
-        acc = fma(S.A[(2 * q) * 33 + lane], u.x, acc);
-        acc = fma(S.A[(2 * q + 1) * 33 + lane], u.y, acc);
+    for (int q = 0; q < N32 / 4; ++q) {
+        const double2 u = x2[2 * q], w = x2[2 * q + 1];
+        acc0 = fma(S.A[(4 * q) * 33 + lane], u.x, acc0);
+        acc1 = fma(S.A[(4 * q + 1) * 33 + lane], u.y, acc1);
+        acc2 = fma(S.A[(4 * q + 2) * 33 + lane], w.x, acc2);
+        acc3 = fma(S.A[(4 * q + 3) * 33 + lane], w.y, acc3);
     }
     __syncwarp();
-    return b - acc;
+    return b - ((acc0 + acc1) + (acc2 + acc3));
 }
 
 template <int P_>
