@@ -437,11 +437,6 @@ static void upload_rest(JobState &S, cudaStream_t s) {
         d.my = P.my;
         d.mz = P.mz;
         d.max_candidates = std::max(1, P.max_candidates);
-        d.hx = P.hot[0];
-        d.hy = P.hot[1];
-        d.hz = P.hot[2];
-        d.hsx = 2 * P.hot[0] + 1;
-        d.hsyx = d.hsx * (2 * P.hot[1] + 1);
         d.packed_ok = P.reach[0] <= 511 && P.reach[1] <= 511 && P.reach[2] <= 255;
     }
 }

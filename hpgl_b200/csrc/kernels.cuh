@@ -36,11 +36,8 @@ struct DevPlan {
     double crx, cry, crz;
     int mx, my, mz;
     int max_candidates;
-    // shared-memory box of the table for the mixed-precision solve: folded
-    // to vz >= 0, |vx| <= hx, |vy| <= hy, vz <= hz; hsx = 2hx+1, hsyx =
-    // hsx (2hy+1).  packed_ok: every neighbour offset fits the 32-bit packed
-    // form (|x|, |y| <= 511, |z| <= 255).
-    int hx, hy, hz, hsx, hsyx;
+    // every neighbour offset fits the 32-bit packed form of the mixed
+    // solve's pair build (|x|, |y| <= 511, |z| <= 255)
     int packed_ok;
 };
 

@@ -19,9 +19,7 @@
 
 namespace hpgl_b200 {
 
-// Shared-memory table box budget of the mixed-precision solve: 72 KiB of
-// doubles (its blocks hold the box beside their warps' system buffers).
-constexpr long long HOT_TABLE_ENTRIES = 72 * 1024 / 8;
+
 
 static std::atomic<int> g_threads{0};
 
@@ -492,80 +490,11 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     P.nseg = (nx + 31) / 32;
     P.wpr = P.nseg + 2 * (P.px / 32) + 2;
 
-    // ---- reach of the searches and the shared-memory table box ----
+    // ---- reach of the searches (template offsets; clusterizer candidates
+    // lie in the 3x3x3 boxes of the radii around the node's box) ----
     for (int a = 0; a < 3; ++a) P.reach[a] = std::max(P.ext[a], P.any_clean ? 2 * p.radii[a] : 0);
-    choose_hot_box(P, (double)P.informed / (double)std::max<long long>(1, P.size), HOT_TABLE_ENTRIES);
 }
 
-void choose_hot_box(Plan &P, double density, long long budget) {
-    int cap[3];
-    for (int a = 0; a < 3; ++a) cap[a] = std::max(0, std::min(P.trunc[a], P.B[a]));
-    P.hot[0] = P.hot[1] = P.hot[2] = 0;
-    const long long len = (long long)P.tmpl.size();
-    if (len < 2 || budget < 1) return;
-    const double expect = (double)P.nmax / std::max(density, 1e-9);
-    const long long K = std::max<long long>(2, std::min<long long>(len, (long long)std::ceil(expect)));
-    const int SAMPLE = 384;
-    std::vector<int> pick;
-    const long long m = std::min<long long>(K, SAMPLE);
-    for (long long i = 0; i < m; ++i) pick.push_back((int)(i * K / m));
-    // histogram over |dx| <= cap0, |dy| <= cap1, 0 <= dz <= cap2 (folded)
-    const int mx = cap[0] + 1, my = cap[1] + 1, mz = cap[2] + 1;
-    std::vector<double> h((size_t)mx * my * mz, 0.0);
-    double total = 0;
-    for (size_t i = 0; i < pick.size(); ++i)
-        for (size_t j = i + 1; j < pick.size(); ++j) {
-            const TemplateEntry &a = P.tmpl[pick[i]], &b = P.tmpl[pick[j]];
-            int dx = a.dx - b.dx, dy = a.dy - b.dy, dz = a.dz - b.dz;
-            if (dz < 0) {
-                dx = -dx;
-                dy = -dy;
-                dz = -dz;
-            }
-            total += 1;
-            dx = std::abs(dx);
-            dy = std::abs(dy);
-            if (dx > cap[0] || dy > cap[1] || dz > cap[2]) continue;
-            h[((size_t)dz * my + dy) * mx + dx] += 1;
-        }
-    // prefix sums: cum(x, y, z) = pairs with |dx| <= x, |dy| <= y, dz <= z
-    for (int z = 0; z < mz; ++z)
-        for (int y = 0; y < my; ++y)
-            for (int x = 0; x < mx; ++x) {
-                double v = h[((size_t)z * my + y) * mx + x];
-                if (x) v += h[((size_t)z * my + y) * mx + x - 1];
-                if (y) v += h[((size_t)z * my + y - 1) * mx + x];
-                if (z) v += h[((size_t)(z - 1) * my + y) * mx + x];
-                if (x && y) v -= h[((size_t)z * my + y - 1) * mx + x - 1];
-                if (x && z) v -= h[((size_t)(z - 1) * my + y) * mx + x - 1];
-                if (y && z) v -= h[((size_t)(z - 1) * my + y - 1) * mx + x];
-                if (x && y && z) v -= h[((size_t)(z - 1) * my + y - 1) * mx + x - 1];
-                h[((size_t)z * my + y) * mx + x] = v;
-            }
-    // every (hy, hz) with the widest hx the budget allows; the box serving
-    // the most sampled pairs wins (ties: the smaller box)
-    int b[3] = {0, 0, 0};
-    double best = -1;
-    long long best_size = 0;
-    for (int z = 0; z < mz; ++z)
-        for (int y = 0; y < my; ++y) {
-            const long long rows = (long long)(2 * y + 1) * (z + 1);
-            if (rows > budget) continue;
-            const int x = (int)std::min<long long>(cap[0], (budget / rows - 1) / 2);
-            const double served = h[((size_t)z * my + y) * mx + x];
-            const int c[3] = {x, y, z};
-            const long long size = hot_entries(c);
-            if (served > best || (served == best && size < best_size)) {
-                best = served;
-                best_size = size;
-                b[0] = x;
-                b[1] = y;
-                b[2] = z;
-            }
-        }
-    (void)total;
-    for (int a = 0; a < 3; ++a) P.hot[a] = b[a];
-}
 
 void fill_cov_table(std::vector<double> &table, const int B[3], const KrigingParams &p, int threads) {
     CovModel cov(p);

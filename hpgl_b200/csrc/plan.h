@@ -81,28 +81,12 @@ struct Plan {
     int nseg = 0;    // 32-cell segments per row
     int wpr = 0;     // 32-bit words per padded row
 
-    // Box of the covariance table the mixed-precision solve keeps in shared
-    // memory, folded by C(v) = C(-v) to vz >= 0: |vx| <= hot[0],
-    // |vy| <= hot[1], 0 <= vz <= hot[2] (choose_hot_box).
-    int hot[3] = {0, 0, 0};
     // largest |offset| of a neighbour from its node per axis (template or
     // clusterizer path)
     int reach[3] = {0, 0, 0};
 };
 
-// Entries of the shared-memory table box (doubles), (2hx+1)(2hy+1)(hz+1).
-inline long long hot_entries(const int h[3]) {
-    return (long long)(2 * h[0] + 1) * (2 * h[1] + 1) * (h[2] + 1);
-}
 
-// Chooses Plan::hot for a budget of `budget` table entries: the pair offsets
-// of a node's system are differences of its neighbours' offsets, and the
-// neighbours are mostly among the first max_neighbours / density template
-// entries.  A histogram of the folded differences of a strided sample of
-// those entries gives the share of pairs every box serves; of the boxes that
-// fit the budget and the table's truncation box, the one serving the most
-// sampled pairs is kept.
-void choose_hot_box(Plan &P, double density, long long budget);
 
 // Validates parameters (throws std::invalid_argument / std::domain_error).
 void validate_params(const KrigingParams &p, int kind);

@@ -17,8 +17,6 @@
 // Both start from the same system: neighbour offsets from the search lists
 // and covariances gathered from the plan's table (my_kriging_weights.h:49-58,
 // 156-165), padded to 32x32 with the identity.
-#include <cstdlib>
-
 #include "device_common.cuh"
 #include "search_common.cuh"
 
@@ -39,8 +37,36 @@ struct SysSmemN {
     double vd[N32];         // double vector broadcast
     float vf[2][N32];       // float vector broadcast
     float row[2][N32];      // mixed: pivot row broadcast (double buffered)
-    int4 nb[N32];           // neighbour offsets from the node (x, y, z, table offset)
+    unsigned nbp[N32];      // neighbour offsets from the node, packed (pack_off)
+    int nbl[N32];           // and their table offsets
 };
+
+// A neighbour's offset (x, y, z) from its node in one 32-bit word: x and y in
+// 11 bits biased by 512, z in 10 bits biased by 256.  With |x|, |y| <= 511
+// and |z| <= 255 (DevPlan::packed_ok) every field stays below half its
+// range, so pa + PACK_BIAS - pb never borrows across fields and holds the
+// difference's fields (xa - xb + 1024, ya - yb + 1024, za - zb + 512).  The
+// pair build reads two such words per pair: 4-byte reads of a 128-byte array
+// never conflict on the shared-memory banks, where 16-byte reads of random
+// entries do.
+__device__ __forceinline__ unsigned pack_off(int ox, int oy, int oz) {
+    return (unsigned)(ox + 512) | ((unsigned)(oy + 512) << 11) | ((unsigned)(oz + 256) << 22);
+}
+constexpr unsigned PACK_BIAS = 1024u | (1024u << 11) | (512u << 22);
+
+// C(x_a - x_b) from the packed offsets and table offsets of a and b: the
+// range test of cov_lin on the difference's biased fields.
+__device__ __forceinline__ double cov_packed(const DevPlan &P, unsigned pa, unsigned pb, int lin, int *err) {
+    const unsigned d = pa + PACK_BIAS - pb;
+    const bool in = (d & 0x7ffu) + (unsigned)(P.Tx - 1024) <= (unsigned)(2 * P.Tx) &&
+                    ((d >> 11) & 0x7ffu) + (unsigned)(P.Ty - 1024) <= (unsigned)(2 * P.Ty) &&
+                    (d >> 22) + (unsigned)(P.Tz - 512) <= (unsigned)(2 * P.Tz);
+    if (!in) {
+        if (!P.truncated) atomicOr(err, DERR_TABLE_RANGE);
+        return 0.0;
+    }
+    return __ldg(P.table + (P.center + lin));
+}
 using SysSmem = SysSmemN<N32 * 34>;
 // systems of at most 16 neighbours (sequential simulation): half the
 // registers and shared memory, twice the warps per SM
@@ -99,7 +125,8 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
     d.oy = oy;
     d.oz = oz;
     d.lin = oz * P.syx + oy * P.sx + ox;
-    S.nb[lane] = make_int4(ox, oy, oz, d.lin);
+    S.nbp[lane] = pack_off(ox, oy, oz);
+    S.nbl[lane] = d.lin;
     __syncwarp();
     return d;
 }
@@ -108,6 +135,7 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
 // entries A(i,k) = C(x_i - x_k), i < k (my_kriging_weights.h:49-58,
 // 156-165), gathered 32 pairs at a time with 8 gathers in flight per lane,
 // each stored at (i,k) and (k,i); diagonal C(0); the identity beyond n.
+// Needs DevPlan::packed_ok.
 __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, SysSmem &S, int n, int lane) {
     constexpr int LD = 33;
     const int npairs = n * (n - 1) / 2;
@@ -121,8 +149,8 @@ __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, 
             v[e] = 0.0;
             if (p < npairs) {
                 ik[e] = __ldg(g_pairs64.v + p);
-                const int4 a = S.nb[ik[e] & 0xff], b = S.nb[ik[e] >> 8];
-                v[e] = cov_lin(P, a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, J.err);
+                const int i = ik[e] & 0xff, k = ik[e] >> 8;
+                v[e] = cov_packed(P, S.nbp[i], S.nbp[k], S.nbl[i] - S.nbl[k], J.err);
             }
         }
 #pragma unroll
@@ -497,14 +525,39 @@ __device__ __forceinline__ float get2(const float2 (&m2)[N32 / 2]) {
     return (P_ & 1) ? m2[P_ / 2].y : m2[P_ / 2].x;
 }
 
+// The kriging variance of a refined solution, c0 - b.w (ordinary kriging:
+// c0 - b.w - w_{n-1}, my_kriging_weights.h:246), accurate to second order in
+// the solution's error.  With x the accepted solution and r = b - A x its
+// FP64 residual (A symmetric, A x* = b): b.x* = b.x + x*.r, taken as
+// b.x + x.r, whose error (x - x*).r is the product of two tiny quantities;
+// the same holds for the ordinary-kriging sums b.xb*, 1.xa*, 1.xb*
+// (A xb* = 1, its residual rb), from which mu and w_{n-1} are formed.
+// Where the variance is a small difference of c0 and b.w (nodes next to or
+// on informed cells), the plain sum would carry the refinement's relative
+// error of w (up to about 1e-13) straight into it.  One more residual per
+// right-hand side, only when variances are asked for.
+template <typename SM>
+__device__ __forceinline__ double residual_corrected_variance(const SM &S, double c0, double b, double ba,
+                                                              double bb, bool ordinary, int n, double xa,
+                                                              double xb, int lane) {
+    const double ra = residual(S, const_cast<double *>(S.vd), xa, ba, lane);
+    const double bxa = warp_sum(b * xa + xa * ra);
+    if (!ordinary) return c0 - bxa;
+    const double rb = residual(S, const_cast<double *>(S.vd), xb, bb, lane);
+    const double bxb = warp_sum(b * xb + xa * rb);
+    const double oxa = warp_sum(xa + xb * ra);
+    const double oxb = warp_sum(xb + xb * rb);
+    const double mu = (oxa - 1.0) / oxb;
+    const double wl = __shfl_sync(FULL_MASK, xa - mu * xb, n - 1);
+    return c0 - (bxa - mu * bxb) - wl;
+}
+
 // One node of the mixed path (FP32 inverse + FP64 refinement); systems that
-// do not qualify are appended to J.routed.  HOT: the system is built from
-// the block's shared-memory box of the table (SysSmemH).  skip: a system
-// is appended to J.routed at once, without the FP32 attempt.  Returns -1
-// when the node needs no system, 0 when it was solved here, 1 when routed.
-template <bool HOT, typename SM>
-__device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, SM &S, const double *hot,
-                                            const NodeFetch &cur, int lane, bool skip = false) {
+// do not qualify are appended to J.routed.  skip: a system is appended to
+// J.routed at once, without the FP32 attempt.  Returns -1 when the node
+// needs no system, 0 when it was solved here, 1 when routed.
+__device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &cur,
+                                            int lane, bool skip = false) {
     const bool ordinary = J.kind == 0;
     const double inv_c0 = 1.0 / P.c0;
     const int node = cur.node;
@@ -514,16 +567,13 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
         __syncwarp();
         return 1;
     }
-    NodeData d;
-    if constexpr (HOT) d = load_node_h(J, P, S, hot, cur, lane);
-    else d = load_node(J, P, S, cur, lane);
+    const NodeData d = load_node(J, P, S, cur, lane);
     if (d.n <= 0) {
         write_outputs(J, P, S, node, lane, d, ST_NO_NEIGHBOURS, 0.0, -1.0);
         return -1;
     }
     const int n = d.n;
-    if constexpr (HOT) build_full32h(J, P, hot, S, n, lane);
-    else build_full32(J, P, S, n, lane);
+    build_full32(J, P, S, n, lane);
     // Row `lane` of the unit-diagonal system A / C(0) (identity padding).
     float2 m2[N32 / 2];
 #pragma unroll
@@ -611,10 +661,7 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
         w = xa;
     }
     double variance = -1.0;
-    if (J.variance) {
-        variance = P.c0 - warp_sum(w * d.b);
-        if (ordinary) variance -= __shfl_sync(FULL_MASK, w, n - 1);
-    }
+    if (J.variance) variance = residual_corrected_variance(S, P.c0, d.b, ba, bb, ordinary, n, xa, xb, lane);
     write_outputs(J, P, S, node, lane, d, ST_SUCCESS, w, variance);
     __syncwarp();
     return 0;
@@ -632,155 +679,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
         const bool attempt = guess.attempt();
-        guess.record(attempt, mixed32_node<false>(J, P, S, nullptr, cur, lane, !attempt));
-        __syncwarp();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Mixed path with the hot part of the covariance table in shared memory.
-//
-// Every block keeps the box of the plan's table that most pair offsets fall
-// in (DevPlan::hx/hy/hz, chosen on the host, folded by C(v) = C(-v) to
-// vz >= 0) in shared memory beside its warps' system buffers; the system
-// build reads a covariance from it at shared-memory latency and falls back
-// to the global table (L2) for offsets outside the box.  The values are the
-// table's own, so the systems are those of k_solve_mixed32.  Neighbour
-// offsets are packed into one 32-bit word (x, y: 11 bits biased by 512; z:
-// 10 bits biased by 256), so a pair's two endpoints are two conflict-free
-// 4-byte shared loads and their difference one integer subtraction.
-
-struct SysSmemH {
-    double A[N32 * 33];  // full symmetric system (LD 33)
-    double vd[N32];      // double vector broadcast
-    float vf[2][N32];    // float vector broadcast
-    float row[2][N32];   // pivot row broadcast (double buffered)
-    unsigned nbp[N32];   // packed neighbour offsets from the node
-};
-constexpr int HOT_WARPS = 16;
-constexpr size_t HOT_TABLE_BYTES = 72 * 1024;
-constexpr size_t SMEM_HOT = HOT_TABLE_BYTES + sizeof(SysSmemH) * HOT_WARPS;
-
-// |ox|, |oy| <= 511 and |oz| <= 255 (DevPlan::packed_ok): every field of a
-// packed word is below half its range, so pa + PACK_BIAS - pb never borrows
-// across fields and holds (xa - xb + 1024, ya - yb + 1024, za - zb + 512).
-__device__ __forceinline__ unsigned pack_off(int ox, int oy, int oz) {
-    return (unsigned)(ox + 512) | ((unsigned)(oy + 512) << 11) | ((unsigned)(oz + 256) << 22);
-}
-constexpr unsigned PACK_BIAS = 1024u | (1024u << 11) | (512u << 22);
-
-// C(x_a - x_b) from the packed offsets of a and b.
-__device__ __forceinline__ double cov_packed(const DevPlan &P, const double *hot, unsigned pa, unsigned pb,
-                                             int *err) {
-    const unsigned d = pa + PACK_BIAS - pb;
-    int dx = (int)(d & 0x7ffu) - 1024, dy = (int)((d >> 11) & 0x7ffu) - 1024, dz = (int)(d >> 22) - 512;
-    if (dz < 0) {
-        dx = -dx;
-        dy = -dy;
-        dz = -dz;
-    }
-    if ((unsigned)(dx + P.hx) <= (unsigned)(2 * P.hx) && (unsigned)(dy + P.hy) <= (unsigned)(2 * P.hy) && dz <= P.hz)
-        return hot[dz * P.hsyx + (dy + P.hy) * P.hsx + dx + P.hx];
-    return cov_lin(P, dx, dy, dz, dz * P.syx + dy * P.sx + dx, err);
-}
-
-// The node prologue of load_node with packed offsets and b from the box.
-__device__ __forceinline__ NodeData load_node_h(const DevJob &J, const DevPlan &P, SysSmemH &S, const double *hot,
-                                                const NodeFetch &f, int lane) {
-    NodeData d;
-    const int node = f.node;
-    d.n = f.n;
-    int x0, y0, z0;
-    node_xyz(J, node, x0, y0, z0);
-    d.dv = 0.f;
-    d.code = -1;
-    d.b = 0.0;
-    int ox = 0, oy = 0, oz = 0;
-    if (lane < d.n) {
-        const int cell = f.cell;
-        int qx, qy, qz;
-        node_xyz(J, cell, qx, qy, qz);
-        ox = qx - x0;
-        oy = qy - y0;
-        oz = qz - z0;
-        if (is_cont(J.kind)) {
-            const float m = J.kind == 1 ? J.sk_mean_f : (J.kind == 2 ? J.mean[cell] : 0.f);
-            d.dv = __fsub_rn(J.values[cell], m);
-        } else {
-            d.code = J.codes[cell];
-        }
-    }
-    const unsigned pk = pack_off(ox, oy, oz);
-    if (lane < d.n) d.b = cov_packed(P, hot, pk, pack_off(0, 0, 0), J.err);
-    d.ox = ox;
-    d.oy = oy;
-    d.oz = oz;
-    d.lin = 0;
-    S.nbp[lane] = pk;
-    __syncwarp();
-    return d;
-}
-
-// build_full32 with the pair covariances from the box.
-__device__ __forceinline__ void build_full32h(const DevJob &J, const DevPlan &P, const double *hot, SysSmemH &S,
-                                              int n, int lane) {
-    constexpr int LD = 33;
-    const int npairs = n * (n - 1) / 2;
-    for (int p0 = 0; p0 < npairs; p0 += 256) {
-        double v[8];
-        int ik[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int p = p0 + 32 * e + lane;
-            ik[e] = -1;
-            v[e] = 0.0;
-            if (p < npairs) {
-                ik[e] = __ldg(g_pairs64.v + p);
-                v[e] = cov_packed(P, hot, S.nbp[ik[e] & 0xff], S.nbp[ik[e] >> 8], J.err);
-            }
-        }
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            if (ik[e] >= 0) {
-                const int i = ik[e] & 0xff, k = ik[e] >> 8;
-                S.A[k * LD + i] = v[e];
-                S.A[i * LD + k] = v[e];
-            }
-        }
-    }
-    S.A[lane * LD + lane] = lane < n ? P.c0 : 1.0;
-    if (lane >= n) {
-        for (int c = 0; c < N32; ++c) {
-            if (c != lane) {
-                S.A[c * LD + lane] = 0.0;
-                S.A[lane * LD + c] = 0.0;
-            }
-        }
-    }
-    __syncwarp();
-}
-
-__global__ void __launch_bounds__(HOT_WARPS * 32, 1) k_solve_mixed32h(DevJob J, DevPlan P) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    double *hot = reinterpret_cast<double *>(dyn_smem);
-    const int hot_n = (P.hz + 1) * P.hsyx;
-    for (int i = threadIdx.x; i < hot_n; i += blockDim.x) {
-        const int dz = i / P.hsyx, r = i - dz * P.hsyx;
-        const int dy = r / P.hsx - P.hy, dx = r - (r / P.hsx) * P.hsx - P.hx;
-        hot[i] = __ldg(P.table + (P.center + dz * P.syx + dy * P.sx + dx));
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    SysSmemH &S = reinterpret_cast<SysSmemH *>(dyn_smem + HOT_TABLE_BYTES)[warp];
-    const long long stride = (long long)gridDim.x * HOT_WARPS;
-    long long it = (long long)blockIdx.x * HOT_WARPS + warp;
-    NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
-    RouteGuess guess;
-    for (; it < J.size; it += stride) {
-        const NodeFetch cur = next;
-        next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
-        const bool attempt = guess.attempt();
-        guess.record(attempt, mixed32_node<true>(J, P, S, hot, cur, lane, !attempt));
+        guess.record(attempt, mixed32_node(J, P, S, cur, lane, !attempt));
         __syncwarp();
     }
 }
@@ -810,7 +709,7 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_fused32(DevJob J, DevPlan P) {
             const NodeFetch cur = next;
             next = fetch_node(J, P, b + 1 < cnt ? base + b + 1 : -1, lane);
             if (MODE == 0) solved += exact32_node(J, P, S, cur, lane);
-            else mixed32_node<false>(J, P, S, nullptr, cur, lane);
+            else mixed32_node(J, P, S, cur, lane);
             __syncwarp();
         }
     }
@@ -928,7 +827,8 @@ __device__ __forceinline__ NodeData sis_load32(const DevJob &J, const DevPlan &P
     d.oy = oy;
     d.oz = oz;
     d.lin = oz * P.syx + oy * P.sx + ox;
-    S.nb[lane] = make_int4(ox, oy, oz, d.lin);
+    S.nbp[lane] = pack_off(ox, oy, oz);
+    S.nbl[lane] = d.lin;
     __syncwarp();
     return d;
 }
@@ -1013,7 +913,7 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
     const long long segs = (long long)P.nseg * J.ny * J.nz;
     if (segs <= 0) return;
     const int threads = WARPS32 * 32;
-    if (precision == 0) {
+    if (precision == 0 || !P.packed_ok) {
         const long long g = persistent_grid((const void *)k_fused32<0>, threads, SMEM32, blocks_per_sm,
                                             (segs + WARPS32 - 1) / WARPS32);
         k_fused32<0><<<(unsigned)g, threads, SMEM32, s>>>(J, P);
@@ -1024,32 +924,16 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
     }
 }
 
-// Experimental selection between mixed kernels (HPGL_B200_MIXED32 = 0 the
-// global table, 1 the shared-memory box of the table), read once.
-static int mixed32_variant() {
-    static const int v = [] {
-        const char *e = getenv("HPGL_B200_MIXED32");
-        return e ? atoi(e) : 1;
-    }();
-    return v;
-}
-
-const char *mixed32_kernel_name(const DevPlan &P) {
-    return mixed32_variant() == 1 && P.packed_ok ? "k_solve_mixed32h" : "k_solve_mixed32";
-}
-
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm) {
     if (n_max <= 0) return;
     const int threads = WARPS32 * 32;
     const long long units = (n_max + WARPS32 - 1) / WARPS32;
-    if (precision == 0 || node_list) {
+    // the mixed kernel's pair build needs packed offsets; a search reaching
+    // beyond them (radii above 511 cells, 255 in z) is solved in FP64
+    if (precision == 0 || node_list || !P.packed_ok) {
         const long long g = persistent_grid((const void *)k_solve_exact32, threads, SMEM32, blocks_per_sm, units);
         k_solve_exact32<<<(unsigned)g, threads, SMEM32, s>>>(J, P, node_list, n_list);
-    } else if (mixed32_variant() == 1 && P.packed_ok) {
-        const long long g = persistent_grid((const void *)k_solve_mixed32h, HOT_WARPS * 32, SMEM_HOT, 1,
-                                            (n_max + HOT_WARPS - 1) / HOT_WARPS);
-        k_solve_mixed32h<<<(unsigned)g, HOT_WARPS * 32, SMEM_HOT, s>>>(J, P);
     } else {
         const long long g = persistent_grid((const void *)k_solve_mixed32, threads, SMEM32, blocks_per_sm, units);
         k_solve_mixed32<<<(unsigned)g, threads, SMEM32, s>>>(J, P);

@@ -756,8 +756,26 @@ __device__ __forceinline__ int mixed64_node(const DevJob &J, const DevPlan &P, M
     }
     double variance = -1.0;
     if (J.variance) {
-        variance = P.c0 - warp_sum64(w0 * d.b[0] + w1 * d.b[1]);
-        if (ordinary) variance -= row_val(w0, w1, n - 1);
+        // b.x* = b.x + x*.r to second order in the solution's error, with r
+        // = b - A x one more FP64 residual of the accepted solution (likewise
+        // for the ordinary-kriging sums), as residual_corrected_variance in
+        // solve32.cu
+        double qa0, qa1, qb0, qb1;
+        residual64(S, cs, a_diag, n, lane, ordinary, xa0, xa1, xb0, xb1, qa0, qa1, qb0, qb1);
+        qa0 += ba0;
+        qa1 += ba1;
+        const double bxa = warp_sum64(d.b[0] * xa0 + xa0 * qa0 + d.b[1] * xa1 + xa1 * qa1);
+        if (!ordinary) {
+            variance = P.c0 - bxa;
+        } else {
+            qb0 += bb0;
+            qb1 += bb1;
+            const double bxb = warp_sum64(d.b[0] * xb0 + xa0 * qb0 + d.b[1] * xb1 + xa1 * qb1);
+            const double oxa = warp_sum64(xa0 + xb0 * qa0 + xa1 + xb1 * qa1);
+            const double oxb = warp_sum64(xb0 + xb0 * qb0 + xb1 + xb1 * qb1);
+            const double mu = (oxa - 1.0) / oxb;
+            variance = P.c0 - (bxa - mu * bxb) - row_val(xa0 - mu * xb0, xa1 - mu * xb1, n - 1);
+        }
     }
     write_outputs64(J, P, node, lane, d, ST_SUCCESS, w0, w1, variance);
     __syncwarp();
