@@ -924,6 +924,8 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
     }
 }
 
+const char *mixed32_kernel_name(const DevPlan &P) { return P.packed_ok ? "k_solve_mixed32" : "k_solve_exact32"; }
+
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm) {
     if (n_max <= 0) return;
