@@ -107,6 +107,11 @@ struct DevJob {
     // mixed precision routing
     int *routed;
     int *n_routed;
+    // template search: nodes left to k_search_tail (node, template position
+    // to resume at) and their count
+    int *tail_node;
+    int *tail_pos;
+    int *n_tail;
     // counters
     unsigned long long *n_fp64;
     int *err;

@@ -131,13 +131,19 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
     return d;
 }
 
-// The full symmetric system into S.A (column k at k*33): the n(n-1)/2
+// Position of A(i, j) in the mixed kernel's FP64 system: column j at j*33,
+// row i XOR-swizzled by j/4 within it.  A lane reading its row (the FP64
+// residuals, lane = row) and the lanes reading 8x4 tiles (the FP32 copy,
+// rows 8 (lane/8) .. +7, columns 4 (lane%8) .. +3) both hit every
+// shared-memory bank at most twice per 32 doubles, the minimum.
+__device__ __forceinline__ int msw(int i, int j) { return j * 33 + (i ^ (j >> 2)); }
+
+// The full symmetric system into S.A (column k at k*33, msw): the n(n-1)/2
 // entries A(i,k) = C(x_i - x_k), i < k (my_kriging_weights.h:49-58,
 // 156-165), gathered 32 pairs at a time with 8 gathers in flight per lane,
 // each stored at (i,k) and (k,i); diagonal C(0); the identity beyond n.
 // Needs DevPlan::packed_ok.
 __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, SysSmem &S, int n, int lane) {
-    constexpr int LD = 33;
     const int npairs = n * (n - 1) / 2;
     for (int p0 = 0; p0 < npairs; p0 += 256) {
         double v[8];
@@ -157,17 +163,17 @@ __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, 
         for (int e = 0; e < 8; ++e) {
             if (ik[e] >= 0) {
                 const int i = ik[e] & 0xff, k = ik[e] >> 8;
-                S.A[k * LD + i] = v[e];
-                S.A[i * LD + k] = v[e];
+                S.A[msw(i, k)] = v[e];
+                S.A[msw(k, i)] = v[e];
             }
         }
     }
-    S.A[lane * LD + lane] = lane < n ? __ldg(P.table + P.center) : 1.0;
+    S.A[msw(lane, lane)] = lane < n ? __ldg(P.table + P.center) : 1.0;
     if (lane >= n) {
         for (int c = 0; c < N32; ++c) {
             if (c != lane) {
-                S.A[c * LD + lane] = 0.0;
-                S.A[lane * LD + c] = 0.0;
+                S.A[msw(lane, c)] = 0.0;
+                S.A[msw(c, lane)] = 0.0;
             }
         }
     }
@@ -483,23 +489,46 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPla
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-// y = M v (row `lane` of M packed in m2), v broadcast through shared memory.
-__device__ __forceinline__ float apply_inverse(const float2 (&m2)[N32 / 2], float v, float *buf, int lane) {
+// The FP32 inverse is held in 8x4 tiles: lane l owns rows 8 (l/8) .. +7 and
+// columns 4 (l%8) .. +3, t[r][h] = (M(row r, col 2h), M(row r, col 2h+1)).
+// Per sweep step a lane needs the pivot row's 4 values at its columns and 8
+// at its rows (the pivot column, by symmetry): three 16-byte broadcast reads
+// and one store by the 8 lanes of the pivot row, half the shared-memory
+// traffic of a lane holding a whole row.
+struct Tile {
+    float2 t[8][2];
+};
+
+// y = M v for v given row by row (v of row `lane`); returns y of row `lane`.
+// Each lane forms its columns' partial sums over its rows (M is symmetric),
+// the four lanes of a column group add them up while scattering the four
+// columns among themselves (lane (g, c) ends with column 4c + g), and one
+// shuffle brings each row its value.
+__device__ __forceinline__ float apply_inverse(const Tile &T, float v, float *buf, int lane) {
     buf[lane] = v;
     __syncwarp();
-    float2 acc = f2(0.f, 0.f);
-    const float4 *b4 = reinterpret_cast<const float4 *>(buf);
+    const int rg = lane >> 3;
+    const float4 v0 = *reinterpret_cast<const float4 *>(buf + 8 * rg);
+    const float4 v1 = *reinterpret_cast<const float4 *>(buf + 8 * rg + 4);
+    const float vr[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+    float2 a01 = f2(0.f, 0.f), a23 = f2(0.f, 0.f);
 #pragma unroll
-    for (int q = 0; q < N32 / 4; ++q) {
-        const float4 u = b4[q];
-        acc = __ffma2_rn(m2[2 * q], f2(u.x, u.y), acc);
-        acc = __ffma2_rn(m2[2 * q + 1], f2(u.z, u.w), acc);
+    for (int r = 0; r < 8; ++r) {
+        a01 = __ffma2_rn(T.t[r][0], f2(vr[r], vr[r]), a01);
+        a23 = __ffma2_rn(T.t[r][1], f2(vr[r], vr[r]), a23);
     }
     __syncwarp();
-    return acc.x + acc.y;
+    const bool hi2 = (rg & 2) != 0, hi1 = (rg & 1) != 0;
+    float2 keep = hi2 ? a23 : a01;
+    const float2 send = hi2 ? a01 : a23;
+    keep.x += __shfl_xor_sync(FULL_MASK, send.x, 16);
+    keep.y += __shfl_xor_sync(FULL_MASK, send.y, 16);
+    float k = hi1 ? keep.y : keep.x;
+    k += __shfl_xor_sync(FULL_MASK, hi1 ? keep.x : keep.y, 8);
+    return __shfl_sync(FULL_MASK, k, 8 * (lane & 3) + (lane >> 2));
 }
 
-// r = b - A x in FP64 (row `lane`; S.A holds the full symmetric system, LD 33).
+// r = b - A x in FP64 (row `lane`; S.A holds the full symmetric system, msw).
 template <typename SM>
 __device__ __forceinline__ double residual(const SM &S, double *vd, double x, double b, int lane) {
     vd[lane] = x;
@@ -511,18 +540,13 @@ __device__ __forceinline__ double residual(const SM &S, double *vd, double x, do
 #pragma unroll
     for (int q = 0; q < N32 / 4; ++q) {
         const double2 u = x2[2 * q], w = x2[2 * q + 1];
-        acc0 = fma(S.A[(4 * q) * 33 + lane], u.x, acc0);
-        acc1 = fma(S.A[(4 * q + 1) * 33 + lane], u.y, acc1);
-        acc2 = fma(S.A[(4 * q + 2) * 33 + lane], w.x, acc2);
-        acc3 = fma(S.A[(4 * q + 3) * 33 + lane], w.y, acc3);
+        acc0 = fma(S.A[msw(lane, 4 * q)], u.x, acc0);
+        acc1 = fma(S.A[msw(lane, 4 * q + 1)], u.y, acc1);
+        acc2 = fma(S.A[msw(lane, 4 * q + 2)], w.x, acc2);
+        acc3 = fma(S.A[msw(lane, 4 * q + 3)], w.y, acc3);
     }
     __syncwarp();
     return b - ((acc0 + acc1) + (acc2 + acc3));
-}
-
-template <int P_>
-__device__ __forceinline__ float get2(const float2 (&m2)[N32 / 2]) {
-    return (P_ & 1) ? m2[P_ / 2].y : m2[P_ / 2].x;
 }
 
 // The kriging variance of a refined solution, c0 - b.w (ordinary kriging:
@@ -574,38 +598,56 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
     }
     const int n = d.n;
     build_full32(J, P, S, n, lane);
-    // Row `lane` of the unit-diagonal system A / C(0) (identity padding).
-    float2 m2[N32 / 2];
+    // The lane's tile of the unit-diagonal system A / C(0) (identity padding).
+    const int rg = lane >> 3, cg = lane & 7;
+    Tile T;
 #pragma unroll
-    for (int q = 0; q < N32 / 2; ++q)
-        m2[q] = f2((float)(S.A[(2 * q) * 33 + lane] * inv_c0), (float)(S.A[(2 * q + 1) * 33 + lane] * inv_c0));
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            T.t[r][h] = f2((float)(S.A[msw(8 * rg + r, 4 * cg + 2 * h)] * inv_c0),
+                           (float)(S.A[msw(8 * rg + r, 4 * cg + 2 * h + 1)] * inv_c0));
     // Symmetric Gauss-Jordan sweeps (the sweep operator): the matrix stays
-    // symmetric, so row p is column p and every lane publishes its own
-    // element of it; after all sweeps m holds -(A/C(0))^-1.  The pivot
-    // lane's own row update (scaling by 1/pivot) is folded into the same
-    // fused multiply-add as every other lane's elimination.
+    // symmetric, so row p is column p; the lanes holding row p publish it,
+    // every lane reads it at its columns (the update's right factor) and at
+    // its rows (its rows' multipliers).  After all sweeps T holds
+    // -(A/C(0))^-1.  The pivot row's own update (scaling by 1/pivot) is
+    // folded into the same fused multiply-add as every other row's.
     bool low = false;
 #pragma unroll
     for (int p = 0; p < N32; ++p) {
         float *rb = S.row[p & 1];
-        const float mp = (p & 1) ? m2[p / 2].y : m2[p / 2].x;
-        rb[lane] = mp;
+        const int rgp = p >> 3, rp = p & 7, cgp = p >> 2, cp = p & 3;
+        const bool prow = rg == rgp;
+        if (prow)
+            *reinterpret_cast<float4 *>(rb + 4 * cg) =
+                make_float4(T.t[rp][0].x, T.t[rp][0].y, T.t[rp][1].x, T.t[rp][1].y);
         __syncwarp();
+        const float4 cv = *reinterpret_cast<const float4 *>(rb + 4 * cg);
+        const float4 r0 = *reinterpret_cast<const float4 *>(rb + 8 * rg);
+        const float4 r1 = *reinterpret_cast<const float4 *>(rb + 8 * rg + 4);
         const float piv = rb[p];
         low |= !(piv > MIXED_PIVOT_MIN);
         const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
-        const float isp = lane == p ? 1.f : 0.f;
-        const float g = (mp - isp) * dinv;
-        const float2 ng = f2(-g, -g);
-        const float4 *r4 = reinterpret_cast<const float4 *>(rb);
+        const float rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+        float g[8];
 #pragma unroll
-        for (int q = 0; q < N32 / 4; ++q) {
-            const float4 u = r4[q];
-            m2[2 * q] = __ffma2_rn(ng, f2(u.x, u.y), m2[2 * q]);
-            m2[2 * q + 1] = __ffma2_rn(ng, f2(u.z, u.w), m2[2 * q + 1]);
+        for (int r = 0; r < 8; ++r) g[r] = (rv[r] - (r == rp && prow ? 1.f : 0.f)) * dinv;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const float2 ng = f2(-g[r], -g[r]);
+            T.t[r][0] = __ffma2_rn(ng, f2(cv.x, cv.y), T.t[r][0]);
+            T.t[r][1] = __ffma2_rn(ng, f2(cv.z, cv.w), T.t[r][1]);
         }
-        if (p & 1) m2[p / 2].y = g - isp;
-        else m2[p / 2].x = g - isp;
+        if (cg == cgp) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float val = g[r] - (r == rp && prow ? 1.f : 0.f);
+                if (cp & 1) T.t[r][cp >> 1].y = val;
+                else T.t[r][cp >> 1].x = val;
+            }
+        }
+        __syncwarp();
     }
     if (__any_sync(FULL_MASK, low)) {
         if (lane == 0) {
@@ -618,19 +660,19 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
     // A^-1 v = -(M v) / C(0); solutions for b (and the ones vector for OK)
     // refined with FP64 residuals.
     const double sc = -inv_c0;
-    double xa = (double)apply_inverse(m2, (float)d.b, S.vf[0], lane) * sc;
-    double xb = ordinary ? (double)apply_inverse(m2, lane < n ? 1.f : 0.f, S.vf[1], lane) * sc : 0.0;
+    double xa = (double)apply_inverse(T, (float)d.b, S.vf[0], lane) * sc;
+    double xb = ordinary ? (double)apply_inverse(T, lane < n ? 1.f : 0.f, S.vf[1], lane) * sc : 0.0;
     const double ba = d.b, bb = lane < n ? 1.0 : 0.0;
     RefineGate gate;
     bool converged = false;
     for (int corr = 0; corr < MIXED_MAX_CORR; ++corr) {
         const double ra = residual(S, S.vd, xa, ba, lane);
-        const double da = (double)apply_inverse(m2, (float)ra, S.vf[0], lane) * sc;
+        const double da = (double)apply_inverse(T, (float)ra, S.vf[0], lane) * sc;
         xa += da;
         double dmax = fabs(da), xmax = fabs(xa);
         if (ordinary) {
             const double rbv = residual(S, S.vd, xb, bb, lane);
-            const double db = (double)apply_inverse(m2, (float)rbv, S.vf[1], lane) * sc;
+            const double db = (double)apply_inverse(T, (float)rbv, S.vf[1], lane) * sc;
             xb += db;
             dmax = fmax(dmax, fabs(db));
             xmax = fmax(xmax, fabs(xb));
