@@ -74,7 +74,7 @@ struct Counters {
     int n_untouched;
     int n_routed;
     int err;
-    int n_tail;  // template search: nodes left to the tail kernel
+    int pad;
     unsigned long long n_fp64;
 };
 
@@ -437,7 +437,6 @@ static void upload_rest(JobState &S, cudaStream_t s) {
         d.my = P.my;
         d.mz = P.mz;
         d.max_candidates = std::max(1, P.max_candidates);
-        d.packed_ok = P.reach[0] <= 511 && P.reach[1] <= 511 && P.reach[2] <= 255;
     }
 }
 
@@ -493,11 +492,6 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.n_untouched = &cnt->n_untouched;
     J.routed = at<int>(S, A.o_routed);
     J.n_routed = &cnt->n_routed;
-    // the search's tail list borrows the routed and untouched lists, which
-    // only the solves after it fill
-    J.tail_node = at<int>(S, A.o_routed);
-    J.tail_pos = at<int>(S, A.o_untouched);
-    J.n_tail = &cnt->n_tail;
     J.n_fp64 = &cnt->n_fp64;
     J.err = &cnt->err;
     if (S.cok) {
@@ -536,7 +530,6 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
         const LaunchTuning tune64 = tuning_get(tuning_family(g.plan.nmax), HPGL_PRECISION_FP64);
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->search0, s));
         CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
-        CUDA_CHECK(cudaMemsetAsync(J.n_tail, 0, sizeof(int), s));
         launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
         ++launches;
         if (S.cok) {
@@ -548,14 +541,14 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
                 CUDA_CHECK(cudaEventRecord(pt->top1, s));
                 CUDA_CHECK(cudaEventRecord(pt->resolve1, s));
             }
-            launches += 3;
+            launches += 2;
             CUDA_CHECK(cudaGetLastError());
             if (after_group) after_group(g);
             continue;
         }
         if (tune.schedule == SCHED_SPLIT) {
-            launch_search_template(J, g.dp, s);  // the segment walk and its tail
-            launches += 2;
+            launch_search_template(J, g.dp, s);
+            ++launches;
         }
         if (g.plan.any_clean) {
             launch_search_cluster(J, g.dp, at<double>(S, A.o_skey), at<int>(S, A.o_sidx), (int)A.cluster_warps, s);

@@ -39,30 +39,14 @@ __global__ void k_build_bits(DevJob J, DevPlan P, uint32_t *bits) {
 
 // ---------------------------------------------------------------------------
 // Template search: one warp per 32-node x-segment (template_segment in
-// search_common.cuh), persistent over the segments; once at most
-// SEARCH_HANDOFF of a segment's nodes are still searching they are left to
-// k_search_tail (a lone node costs a segment step of about 30 instructions
-// per 32 template entries, its own walk about 12).
-constexpr int SEARCH_HANDOFF = 2;
+// search_common.cuh), persistent over the segments.
 __global__ void __launch_bounds__(256) k_search_template(DevJob J, DevPlan P) {
     __shared__ int delta_sm[8][32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long total = (long long)P.nseg * J.ny * J.nz;
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long segi = (long long)blockIdx.x * (blockDim.x >> 5) + wib; segi < total; segi += nwarps)
-        template_segment(J, P, segi, lane, delta_sm[wib], SEARCH_HANDOFF);
-}
-
-// The template walks k_search_template left to the tail list, one warp per
-// node (grid-stride over the list).
-__global__ void __launch_bounds__(256) k_search_tail(DevJob J, DevPlan P) {
-    const int lane = threadIdx.x & 31;
-    const int count = *J.n_tail;
-    const int nwarps = gridDim.x * (blockDim.x >> 5);
-    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < count; i += nwarps) {
-        const int node = J.tail_node[i];
-        template_node_from(J, P, node, J.tail_pos[i], J.nbcount[node], lane);
-    }
+        template_segment(J, P, segi, lane, delta_sm[wib]);
 }
 
 // ---------------------------------------------------------------------------
@@ -306,7 +290,6 @@ void launch_search_template(const DevJob &J, const DevPlan &P, cudaStream_t s) {
     const long long cap = (long long)sm_count() * 8;  // 8 blocks of 8 warps per SM
     if (blocks > cap) blocks = cap;
     k_search_template<<<(unsigned)std::max<long long>(1, blocks), 256, 0, s>>>(J, P);
-    k_search_tail<<<(unsigned)sm_count() * 8, 256, 0, s>>>(J, P);
 }
 
 void launch_search_cluster(const DevJob &J, const DevPlan &P, double *sk, int *si, int n_warps, cudaStream_t s) {

@@ -36,9 +36,6 @@ struct DevPlan {
     double crx, cry, crz;
     int mx, my, mz;
     int max_candidates;
-    // every neighbour offset fits the 32-bit packed form of the mixed
-    // solve's pair build (|x|, |y| <= 511, |z| <= 255)
-    int packed_ok;
 };
 
 // Division by a runtime-invariant divisor d >= 1 of any n < 2^32 with one
@@ -107,11 +104,6 @@ struct DevJob {
     // mixed precision routing
     int *routed;
     int *n_routed;
-    // template search: nodes left to k_search_tail (node, template position
-    // to resume at) and their count
-    int *tail_node;
-    int *tail_pos;
-    int *n_tail;
     // counters
     unsigned long long *n_fp64;
     int *err;

@@ -490,9 +490,6 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     P.nseg = (nx + 31) / 32;
     P.wpr = P.nseg + 2 * (P.px / 32) + 2;
 
-    // ---- reach of the searches (template offsets; clusterizer candidates
-    // lie in the 3x3x3 boxes of the radii around the node's box) ----
-    for (int a = 0; a < 3; ++a) P.reach[a] = std::max(P.ext[a], P.any_clean ? 2 * p.radii[a] : 0);
 }
 
 

@@ -81,9 +81,6 @@ struct Plan {
     int nseg = 0;    // 32-cell segments per row
     int wpr = 0;     // 32-bit words per padded row
 
-    // largest |offset| of a neighbour from its node per axis (template or
-    // clusterizer path)
-    int reach[3] = {0, 0, 0};
 };
 
 

@@ -29,16 +29,8 @@ __device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
 }
 
 // Returns the segment's first node; dsm is a 32-int per-warp scratch.
-// handoff > 0: once at most `handoff` of the segment's nodes are still
-// searching, their counts so far and the template position they stopped at
-// go to the tail list (J.tail_node, J.tail_pos, J.n_tail) and the warp moves
-// on; k_search_tail finishes them one warp per node in the same template
-// order, so the lists are the ones the segment walk would have produced.  A
-// segment otherwise walks as long as its slowest node -- nodes near the
-// grid's faces, whose template runs partly outside the grid, need several
-// times the probes of the others.
 __device__ __forceinline__ int template_segment(const DevJob &J, const DevPlan &P, long long segi, int lane,
-                                                int *dsm, int handoff = 0) {
+                                                int *dsm) {
     const int seg = (int)(segi % P.nseg);
     const long long row = segi / P.nseg;
     const int y = (int)(row % J.ny), z = (int)(row / J.ny);
@@ -76,49 +68,9 @@ __device__ __forceinline__ int template_segment(const DevJob &J, const DevPlan &
         }
         __syncwarp();
         active = __ballot_sync(FULL_MASK, act && cnt < nmax);
-        if (handoff > 0 && active && __popc(active) <= handoff && tb + 32 < P.tmpl_len) {
-            if (act && cnt < nmax) {
-                const int pos = atomicAdd(J.n_tail, 1);
-                J.tail_node[pos] = node;
-                J.tail_pos[pos] = tb + 32;
-            }
-            break;
-        }
     }
     if (act) J.nbcount[node] = cnt;
     return base;
-}
-
-// The rest of one node's template walk from template position t0 with cnt0
-// neighbours found (neighbour_lookup_t::find, sugarbox_neighbour_lookup.h:
-// 35-61): 32 entries per step, lane t testing entry base + t, hits appended
-// in template order.
-__device__ __forceinline__ void template_node_from(const DevJob &J, const DevPlan &P, int node, int t0, int cnt0,
-                                                   int lane) {
-    int x, y, z;
-    node_xyz(J, node, x, y, z);
-    const int nmax = P.nmax;
-    int *out = J.nb + (long long)node * nmax;
-    int cnt = cnt0;
-    for (int tb = t0; tb < P.tmpl_len && cnt < nmax; tb += 32) {
-        const int t = tb + lane;
-        bool hit = false;
-        int delta = 0;
-        if (t < P.tmpl_len) {
-            const int4 e = __ldg(&P.tmpl[t]);
-            delta = e.w;
-            const int yy = y + e.y, zz = z + e.z;
-            if ((unsigned)yy < (unsigned)J.ny && (unsigned)zz < (unsigned)J.nz) {
-                const int px = x + e.x;  // padded x of the target cell
-                hit = (J.bits[((long long)zz * J.ny + yy) * P.wpr + (px >> 5)] >> (px & 31)) & 1u;
-            }
-        }
-        const unsigned b = __ballot_sync(FULL_MASK, hit);
-        const int rank = __popc(b & ((1u << lane) - 1u));
-        if (hit && cnt + rank < nmax) out[cnt + rank] = node + delta;
-        cnt += __popc(b);
-    }
-    if (lane == 0) J.nbcount[node] = min(cnt, nmax);
 }
 
 // neighbour_lookup_t::find (sugarbox_neighbour_lookup.h:35-61) for one node:

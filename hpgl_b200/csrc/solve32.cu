@@ -37,36 +37,8 @@ struct SysSmemN {
     double vd[N32];         // double vector broadcast
     float vf[2][N32];       // float vector broadcast
     float row[2][N32];      // mixed: pivot row broadcast (double buffered)
-    unsigned nbp[N32];      // neighbour offsets from the node, packed (pack_off)
-    int nbl[N32];           // and their table offsets
+    int4 nb[N32];           // neighbour offsets from the node (x, y, z, table offset)
 };
-
-// A neighbour's offset (x, y, z) from its node in one 32-bit word: x and y in
-// 11 bits biased by 512, z in 10 bits biased by 256.  With |x|, |y| <= 511
-// and |z| <= 255 (DevPlan::packed_ok) every field stays below half its
-// range, so pa + PACK_BIAS - pb never borrows across fields and holds the
-// difference's fields (xa - xb + 1024, ya - yb + 1024, za - zb + 512).  The
-// pair build reads two such words per pair: 4-byte reads of a 128-byte array
-// never conflict on the shared-memory banks, where 16-byte reads of random
-// entries do.
-__device__ __forceinline__ unsigned pack_off(int ox, int oy, int oz) {
-    return (unsigned)(ox + 512) | ((unsigned)(oy + 512) << 11) | ((unsigned)(oz + 256) << 22);
-}
-constexpr unsigned PACK_BIAS = 1024u | (1024u << 11) | (512u << 22);
-
-// C(x_a - x_b) from the packed offsets and table offsets of a and b: the
-// range test of cov_lin on the difference's biased fields.
-__device__ __forceinline__ double cov_packed(const DevPlan &P, unsigned pa, unsigned pb, int lin, int *err) {
-    const unsigned d = pa + PACK_BIAS - pb;
-    const bool in = (d & 0x7ffu) + (unsigned)(P.Tx - 1024) <= (unsigned)(2 * P.Tx) &&
-                    ((d >> 11) & 0x7ffu) + (unsigned)(P.Ty - 1024) <= (unsigned)(2 * P.Ty) &&
-                    (d >> 22) + (unsigned)(P.Tz - 512) <= (unsigned)(2 * P.Tz);
-    if (!in) {
-        if (!P.truncated) atomicOr(err, DERR_TABLE_RANGE);
-        return 0.0;
-    }
-    return __ldg(P.table + (P.center + lin));
-}
 using SysSmem = SysSmemN<N32 * 34>;
 // systems of at most 16 neighbours (sequential simulation): half the
 // registers and shared memory, twice the warps per SM
@@ -125,8 +97,7 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
     d.oy = oy;
     d.oz = oz;
     d.lin = oz * P.syx + oy * P.sx + ox;
-    S.nbp[lane] = pack_off(ox, oy, oz);
-    S.nbl[lane] = d.lin;
+    S.nb[lane] = make_int4(ox, oy, oz, d.lin);
     __syncwarp();
     return d;
 }
@@ -142,7 +113,6 @@ __device__ __forceinline__ int msw(int i, int j) { return j * 33 + (i ^ (j >> 2)
 // entries A(i,k) = C(x_i - x_k), i < k (my_kriging_weights.h:49-58,
 // 156-165), gathered 32 pairs at a time with 8 gathers in flight per lane,
 // each stored at (i,k) and (k,i); diagonal C(0); the identity beyond n.
-// Needs DevPlan::packed_ok.
 __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, SysSmem &S, int n, int lane) {
     const int npairs = n * (n - 1) / 2;
     for (int p0 = 0; p0 < npairs; p0 += 256) {
@@ -155,8 +125,8 @@ __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, 
             v[e] = 0.0;
             if (p < npairs) {
                 ik[e] = __ldg(g_pairs64.v + p);
-                const int i = ik[e] & 0xff, k = ik[e] >> 8;
-                v[e] = cov_packed(P, S.nbp[i], S.nbp[k], S.nbl[i] - S.nbl[k], J.err);
+                const int4 a = S.nb[ik[e] & 0xff], b = S.nb[ik[e] >> 8];
+                v[e] = cov_lin(P, a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, J.err);
             }
         }
 #pragma unroll
@@ -499,7 +469,8 @@ struct Tile {
     float2 t[8][2];
 };
 
-// y = M v for v given row by row (v of row `lane`); returns y of row `lane`.
+// y = (T - 2 I) v for v given row by row (v of row `lane`); returns y of row
+// `lane`.
 // Each lane forms its columns' partial sums over its rows (M is symmetric),
 // the four lanes of a column group add them up while scattering the four
 // columns among themselves (lane (g, c) ends with column 4c + g), and one
@@ -525,7 +496,8 @@ __device__ __forceinline__ float apply_inverse(const Tile &T, float v, float *bu
     keep.y += __shfl_xor_sync(FULL_MASK, send.y, 16);
     float k = hi1 ? keep.y : keep.x;
     k += __shfl_xor_sync(FULL_MASK, hi1 ? keep.x : keep.y, 8);
-    return __shfl_sync(FULL_MASK, k, 8 * (lane & 3) + (lane >> 2));
+    // the sweep leaves +2 on the diagonal
+    return __shfl_sync(FULL_MASK, k, 8 * (lane & 3) + (lane >> 2)) - 2.f * v;
 }
 
 // r = b - A x in FP64 (row `lane`; S.A holds the full symmetric system, msw).
@@ -610,9 +582,12 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
     // Symmetric Gauss-Jordan sweeps (the sweep operator): the matrix stays
     // symmetric, so row p is column p; the lanes holding row p publish it,
     // every lane reads it at its columns (the update's right factor) and at
-    // its rows (its rows' multipliers).  After all sweeps T holds
-    // -(A/C(0))^-1.  The pivot row's own update (scaling by 1/pivot) is
-    // folded into the same fused multiply-add as every other row's.
+    // its rows (its rows' multipliers).  The pivot's own entry of the right
+    // factor is taken as piv - 1, which turns the same fused update into the
+    // swept column p (m_rp / piv) on every other row and leaves 2 - 1/piv
+    // in place of -1/piv on the pivot itself; a swept diagonal entry is never
+    // read again, so after all sweeps T holds -(A/C(0))^-1 + 2 I and the
+    // products subtract the 2 v (apply_inverse).
     bool low = false;
 #pragma unroll
     for (int p = 0; p < N32; ++p) {
@@ -623,29 +598,27 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
             *reinterpret_cast<float4 *>(rb + 4 * cg) =
                 make_float4(T.t[rp][0].x, T.t[rp][0].y, T.t[rp][1].x, T.t[rp][1].y);
         __syncwarp();
-        const float4 cv = *reinterpret_cast<const float4 *>(rb + 4 * cg);
+        float4 cv = *reinterpret_cast<const float4 *>(rb + 4 * cg);
         const float4 r0 = *reinterpret_cast<const float4 *>(rb + 8 * rg);
         const float4 r1 = *reinterpret_cast<const float4 *>(rb + 8 * rg + 4);
         const float piv = rb[p];
         low |= !(piv > MIXED_PIVOT_MIN);
         const float dinv = __fdividef(1.f, piv);  // approximate: the refinement absorbs it
+        if (cg == cgp) {
+            if (cp == 0) cv.x = piv - 1.f;
+            else if (cp == 1) cv.y = piv - 1.f;
+            else if (cp == 2) cv.z = piv - 1.f;
+            else cv.w = piv - 1.f;
+        }
         const float rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-        float g[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) g[r] = (rv[r] - (r == rp && prow ? 1.f : 0.f)) * dinv;
+        const float2 nd = f2(-dinv, -dinv);
+        // the pivot row's multiplier is (m_pp - 1) / piv
+        const float dp = prow ? dinv : 0.f;
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
-            const float2 ng = f2(-g[r], -g[r]);
+            const float2 ng = __ffma2_rn(f2(rv[r], rv[r]), nd, r == rp ? f2(dp, dp) : f2(0.f, 0.f));
             T.t[r][0] = __ffma2_rn(ng, f2(cv.x, cv.y), T.t[r][0]);
             T.t[r][1] = __ffma2_rn(ng, f2(cv.z, cv.w), T.t[r][1]);
-        }
-        if (cg == cgp) {
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const float val = g[r] - (r == rp && prow ? 1.f : 0.f);
-                if (cp & 1) T.t[r][cp >> 1].y = val;
-                else T.t[r][cp >> 1].x = val;
-            }
         }
         __syncwarp();
     }
@@ -869,8 +842,7 @@ __device__ __forceinline__ NodeData sis_load32(const DevJob &J, const DevPlan &P
     d.oy = oy;
     d.oz = oz;
     d.lin = oz * P.syx + oy * P.sx + ox;
-    S.nbp[lane] = pack_off(ox, oy, oz);
-    S.nbl[lane] = d.lin;
+    S.nb[lane] = make_int4(ox, oy, oz, d.lin);
     __syncwarp();
     return d;
 }
@@ -955,7 +927,7 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
     const long long segs = (long long)P.nseg * J.ny * J.nz;
     if (segs <= 0) return;
     const int threads = WARPS32 * 32;
-    if (precision == 0 || !P.packed_ok) {
+    if (precision == 0) {
         const long long g = persistent_grid((const void *)k_fused32<0>, threads, SMEM32, blocks_per_sm,
                                             (segs + WARPS32 - 1) / WARPS32);
         k_fused32<0><<<(unsigned)g, threads, SMEM32, s>>>(J, P);
@@ -966,16 +938,14 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
     }
 }
 
-const char *mixed32_kernel_name(const DevPlan &P) { return P.packed_ok ? "k_solve_mixed32" : "k_solve_exact32"; }
+const char *mixed32_kernel_name(const DevPlan &) { return "k_solve_mixed32"; }
 
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
                     long long n_max, cudaStream_t s, int blocks_per_sm) {
     if (n_max <= 0) return;
     const int threads = WARPS32 * 32;
     const long long units = (n_max + WARPS32 - 1) / WARPS32;
-    // the mixed kernel's pair build needs packed offsets; a search reaching
-    // beyond them (radii above 511 cells, 255 in z) is solved in FP64
-    if (precision == 0 || node_list || !P.packed_ok) {
+    if (precision == 0 || node_list) {
         const long long g = persistent_grid((const void *)k_solve_exact32, threads, SMEM32, blocks_per_sm, units);
         k_solve_exact32<<<(unsigned)g, threads, SMEM32, s>>>(J, P, node_list, n_list);
     } else {
