@@ -334,8 +334,8 @@ def main():
         for prec in ("mixed", "fp64"):
             t = time.perf_counter()
             systems = 0
-            for _, job in batch_stream:
-                systems += N.krige(job, precision=prec)["systems"]
+            for _, sjob in batch_stream:
+                systems += N.krige(sjob, precision=prec)["systems"]
             serve["batch_" + prec] = {"systems_per_s": systems / (time.perf_counter() - t),
                                       "note": "the same jobs back to back through hpgl_b200_krige (whole calls)"}
         for rate in rates:
