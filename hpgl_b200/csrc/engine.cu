@@ -1240,6 +1240,7 @@ struct Server {
     std::chrono::steady_clock::time_point first_submit, last_done;
     bool any_submit = false;
     int device = 0;
+    std::atomic<int> planners{0};  // jobs being planned on the host right now
 
     void worker_loop();
     void run_one(const std::shared_ptr<ServerJob> &sj);
@@ -1252,8 +1253,15 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
     try {
         CUDA_CHECK(cudaSetDevice(device));
         const auto t_plan = std::chrono::steady_clock::now();
-        // several jobs plan at once: each gets its share of the host threads
-        prepare(S, sj->job, *sj->result, std::max(1, host_threads() / std::max(1, (int)workers.size())));
+        // the jobs planning at the same time share the host threads
+        {
+            const int planning = ++planners;
+            struct Leave {
+                std::atomic<int> &n;
+                ~Leave() { --n; }
+            } leave{planners};
+            prepare(S, sj->job, *sj->result, std::max(1, host_threads() / planning));
+        }
         sj->plan_ms = ms_since(t_plan);
         bytes = (long long)S.ar.total;
         if (bytes > budget)
