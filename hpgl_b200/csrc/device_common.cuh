@@ -163,4 +163,48 @@ struct RouteGuess {
     }
 };
 
+// Sends a node's system to the FP64 re-solve (one lane).
+__device__ __forceinline__ void route(const DevJob &J, int node) {
+    J.routed[node] = 1;
+    atomicAdd(J.n_routed, 1);
+}
+
+// Job-level decision of the mixed path.  When most systems of a job are
+// routed (an ill-conditioned model over the whole grid), the FP32 attempts
+// are wasted and the re-solve is nearly the plain FP64 pass anyway.  The
+// warps therefore add up their attempts and routed attempts every 16
+// nodes; once at least ABANDON_MIN systems have been
+// attempted and more than ABANDON_FRACTION of them routed, the job is
+// abandoned: the mixed kernel stops, and the re-solve kernel runs the plain
+// FP64 pass over every node instead of the flagged ones (results of nodes
+// the mixed kernel already solved are recomputed, so every result is the
+// FP64 one).
+constexpr int ABANDON_MIN = 4096;
+constexpr float ABANDON_FRACTION = 0.6f;
+
+struct AttemptTally {
+    int att = 0, routed = 0, since = 0;
+    // after each node (outcome of mixed*_node, attempted or not); true once
+    // the job is abandoned
+    __device__ __forceinline__ bool step(const DevJob &J, bool attempted, int outcome, int lane) {
+        if (attempted && outcome >= 0) {
+            ++att;
+            routed += outcome;
+        }
+        if (++since < 16) return false;
+        since = 0;
+        int flag = 0;
+        if (lane == 0) {
+            if (att) {
+                const int a = atomicAdd(J.n_attempt, att) + att;
+                const int r = atomicAdd(J.n_attempt_routed, routed) + routed;
+                if (a >= ABANDON_MIN && (float)r > ABANDON_FRACTION * (float)a) atomicExch(J.abandon, 1);
+            }
+            flag = *reinterpret_cast<volatile int *>(J.abandon);
+        }
+        att = routed = 0;
+        return __shfl_sync(FULL_MASK, flag, 0) != 0;
+    }
+};
+
 }  // namespace hpgl_b200

@@ -74,7 +74,9 @@ struct Counters {
     int n_untouched;
     int n_routed;
     int err;
-    int pad;
+    int n_attempt;         // mixed path: systems attempted in FP32
+    int n_attempt_routed;  // and of those routed
+    int abandon;           // the job was abandoned to the plain FP64 pass
     unsigned long long n_fp64;
 };
 
@@ -318,7 +320,7 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     A.o_nb = take(n * (size_t)S.nmax_all * 4);
     A.o_nbcount = take(n * 4);
     A.o_untouched = take(n * 4);
-    A.o_routed = take(n * 4);
+    A.o_routed = take(n);  // per-node routed flags
     A.o_counters = take(sizeof(Counters));
     int max_cand = 1;
     bool any_clean = false;
@@ -490,8 +492,11 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     Counters *cnt = at<Counters>(S, A.o_counters);
     J.untouched = at<int>(S, A.o_untouched);
     J.n_untouched = &cnt->n_untouched;
-    J.routed = at<int>(S, A.o_routed);
+    J.routed = at<uint8_t>(S, A.o_routed);
     J.n_routed = &cnt->n_routed;
+    J.n_attempt = &cnt->n_attempt;
+    J.n_attempt_routed = &cnt->n_attempt_routed;
+    J.abandon = &cnt->abandon;
     J.n_fp64 = &cnt->n_fp64;
     J.err = &cnt->err;
     if (S.cok) {
@@ -530,6 +535,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
         const LaunchTuning tune64 = tuning_get(tuning_family(g.plan.nmax), HPGL_PRECISION_FP64);
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->search0, s));
         CUDA_CHECK(cudaMemsetAsync(J.nbcount, 0, (size_t)S.size * sizeof(int), s));
+        if (S.precision == HPGL_PRECISION_MIXED) CUDA_CHECK(cudaMemsetAsync(J.routed, 0, (size_t)S.size, s));
         launch_build_bits(J, g.dp, at<uint32_t>(S, g.o_bits), s);
         ++launches;
         if (S.cok) {
@@ -559,19 +565,22 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
             if (g.plan.nmax <= 32) launch_fused32(J, g.dp, S.precision, s, tune.blocks_per_sm);
             else launch_fused64(J, g.dp, S.precision, s, tune.blocks_per_sm);
         } else {
-            launch_solve(J, g.dp, S.precision, nullptr, nullptr, 0, s, tune.blocks_per_sm);
+            launch_solve(J, g.dp, S.precision, nullptr, s, tune.blocks_per_sm);
         }
         ++launches;
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top1, s));
         if (S.precision == HPGL_PRECISION_MIXED) {
-            launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, J.n_routed, (int)S.size, s, tune64.blocks_per_sm);
+            launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, s, tune64.blocks_per_sm);
             ++launches;
         }
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->resolve1, s));
         CUDA_CHECK(cudaGetLastError());
         if (after_group) after_group(g);
-        if (S.precision == HPGL_PRECISION_MIXED && gi + 1 < S.groups.size())
+        if (S.precision == HPGL_PRECISION_MIXED && gi + 1 < S.groups.size()) {
+            // the routed count and the job-level tally start over per group
             CUDA_CHECK(cudaMemsetAsync(&cnt->n_routed, 0, sizeof(int), s));
+            CUDA_CHECK(cudaMemsetAsync(&cnt->n_attempt, 0, 3 * sizeof(int), s));
+        }
     }
     if (S.per_category) {
         DevJob J = make_devjob(S, S.groups[0]);

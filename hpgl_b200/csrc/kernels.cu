@@ -297,15 +297,14 @@ void launch_search_cluster(const DevJob &J, const DevPlan &P, double *sk, int *s
     k_search_cluster<<<(unsigned)((n_warps * 32 + threads - 1) / threads), threads, 0, s>>>(J, P, sk, si, n_warps);
 }
 
-void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                  int n_list_max, cudaStream_t s, int blocks_per_sm) {
-    long long n_max = node_list ? (long long)n_list_max : J.size;
-    if (n_max <= 0) return;
+void launch_solve(const DevJob &J, const DevPlan &P, int precision, const uint8_t *routed, cudaStream_t s,
+                  int blocks_per_sm) {
+    if (J.size <= 0) return;
     if (P.nmax <= 32) {
-        launch_solve32(J, P, precision, node_list, n_list, n_max, s, blocks_per_sm);
+        launch_solve32(J, P, precision, routed, s, blocks_per_sm);
         return;
     }
-    if (precision == 0 || node_list) launch_solve64_exact(J, P, node_list, n_list, n_max, s, blocks_per_sm);
+    if (precision == 0 || routed) launch_solve64_exact(J, P, routed, s, blocks_per_sm);
     else launch_solve64_mixed(J, P, s, blocks_per_sm);
 }
 

@@ -101,9 +101,12 @@ struct DevJob {
     // untouched nodes (ordinary kriging failures keep the caller's content)
     int *untouched;
     int *n_untouched;
-    // mixed precision routing
-    int *routed;
+    // mixed precision routing; the job-level tally of attempts (AttemptTally)
+    uint8_t *routed;         // per node: routed to the FP64 re-solve
     int *n_routed;
+    int *n_attempt;
+    int *n_attempt_routed;
+    int *abandon;            // set: the re-solve runs the plain FP64 pass
     // counters
     unsigned long long *n_fp64;
     int *err;
@@ -151,10 +154,11 @@ void launch_build_bits(const DevJob &J, const DevPlan &P, uint32_t *bits, cudaSt
 void launch_search_template(const DevJob &J, const DevPlan &P, cudaStream_t s);
 void launch_search_cluster(const DevJob &J, const DevPlan &P, double *scratch_key, int *scratch_idx,
                            int n_warps, cudaStream_t s);
-// precision: 0 exact FP64, 1 FP32 + FP64 refinement (routes to `routed`).
-// node_list: optional list of nodes (routed re-solve); else every node.
-void launch_solve(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                  int n_list_max, cudaStream_t s, int blocks_per_sm = 0);
+// precision: 0 exact FP64, 1 FP32 + FP64 refinement (flags J.routed).
+// routed: optional per-node flags (the routed re-solve: the flagged nodes in
+// node order, every node once the job is abandoned); else every node.
+void launch_solve(const DevJob &J, const DevPlan &P, int precision, const uint8_t *routed, cudaStream_t s,
+                  int blocks_per_sm = 0);
 void launch_ik_argmax(const DevJob &J, cudaStream_t s);
 // cokriging.cu: colocated simple cokriging of every node (after the template search)
 void launch_cokriging(const DevJob &J, const DevPlan &P, cudaStream_t s);
@@ -210,12 +214,12 @@ void launch_sis_try64(const DevJob &J, const DevPlan *plans, const SgsState &G, 
 // solve32.cu: the mixed-precision kernel launch_solve32 runs for plan P
 const char *mixed32_kernel_name(const DevPlan &P);
 // solve32.cu: register-resident solves for max_neighbours <= 32
-void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                    long long n_max, cudaStream_t s, int blocks_per_sm);
+void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const uint8_t *routed, cudaStream_t s,
+                    int blocks_per_sm);
 // solve64.cu: solves for 33..64 neighbours (exact FP64; FP32 inverse + FP64
 // refinement, routing to `routed`)
-void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
-                          long long n_max, cudaStream_t s, int blocks_per_sm);
+void launch_solve64_exact(const DevJob &J, const DevPlan &P, const uint8_t *routed, cudaStream_t s,
+                          int blocks_per_sm);
 void launch_solve64_mixed(const DevJob &J, const DevPlan &P, cudaStream_t s, int blocks_per_sm);
 // Fused template search + solve of every node (the clusterizer search runs
 // first); precision 0 exact FP64, 1 mixed.

@@ -435,21 +435,37 @@ __device__ __forceinline__ bool exact32_node(const DevJob &J, const DevPlan &P, 
     return true;
 }
 
-__global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPlan P, const int *list, const int *n_list) {
+// routed: per-node flags of the mixed pass -- the flagged nodes are solved,
+// 32 flags read at a time and taken in node order (every node once the job
+// was abandoned); null: every node.
+__global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPlan P, const uint8_t *routed) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
-    const long long count = list ? (long long)*n_list : J.size;
     const long long stride = (long long)gridDim.x * WARPS32;
     unsigned long long solved = 0;
     long long it = (long long)blockIdx.x * WARPS32 + warp;
-    NodeFetch cur = fetch_node(J, P, it < count ? (list ? list[it] : (int)it) : -1, lane);
-    for (; it < count; it += stride) {
-        const long long nx = it + stride;
-        const NodeFetch next = fetch_node(J, P, nx < count ? (list ? list[nx] : (int)nx) : -1, lane);
-        solved += exact32_node(J, P, S, cur, lane);
-        __syncwarp();
-        cur = next;
+    if (routed && !*J.abandon) {
+        for (long long base = it * 32; base < J.size; base += stride * 32) {
+            const long long i = base + lane;
+            unsigned m = __ballot_sync(FULL_MASK, i < J.size && routed[i]);
+            while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1;
+                const NodeFetch f = fetch_node(J, P, (int)(base + k), lane);
+                solved += exact32_node(J, P, S, f, lane);
+                __syncwarp();
+            }
+        }
+    } else {
+        NodeFetch cur = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+        for (; it < J.size; it += stride) {
+            const long long nx = it + stride;
+            const NodeFetch next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
+            solved += exact32_node(J, P, S, cur, lane);
+            __syncwarp();
+            cur = next;
+        }
     }
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
@@ -559,7 +575,7 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
     const int node = cur.node;
     if (copy_informed(J, cur, lane)) return -1;
     if (skip && cur.n > 0) {
-        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        if (lane == 0) route(J, node);
         __syncwarp();
         return 1;
     }
@@ -623,10 +639,7 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
         __syncwarp();
     }
     if (__any_sync(FULL_MASK, low)) {
-        if (lane == 0) {
-            const int pos = atomicAdd(J.n_routed, 1);
-            J.routed[pos] = node;
-        }
+        if (lane == 0) route(J, node);
         __syncwarp();
         return 1;
     }
@@ -657,10 +670,7 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
         }
     }
     if (!converged) {
-        if (lane == 0) {
-            const int pos = atomicAdd(J.n_routed, 1);
-            J.routed[pos] = node;
-        }
+        if (lane == 0) route(J, node);
         __syncwarp();
         return 1;
     }
@@ -690,12 +700,15 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
     long long it = (long long)blockIdx.x * WARPS32 + warp;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
     RouteGuess guess;
+    AttemptTally tally;
     for (; it < J.size; it += stride) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
         const bool attempt = guess.attempt();
-        guess.record(attempt, mixed32_node(J, P, S, cur, lane, !attempt));
+        const int outcome = mixed32_node(J, P, S, cur, lane, !attempt);
+        guess.record(attempt, outcome);
         __syncwarp();
+        if (tally.step(J, attempt, outcome, lane)) break;
     }
 }
 
@@ -940,14 +953,13 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
 
 const char *mixed32_kernel_name(const DevPlan &) { return "k_solve_mixed32"; }
 
-void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const int *node_list, const int *n_list,
-                    long long n_max, cudaStream_t s, int blocks_per_sm) {
-    if (n_max <= 0) return;
+void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const uint8_t *routed, cudaStream_t s,
+                    int blocks_per_sm) {
     const int threads = WARPS32 * 32;
-    const long long units = (n_max + WARPS32 - 1) / WARPS32;
-    if (precision == 0 || node_list) {
+    const long long units = (J.size + WARPS32 - 1) / WARPS32;
+    if (precision == 0 || routed) {
         const long long g = persistent_grid((const void *)k_solve_exact32, threads, SMEM32, blocks_per_sm, units);
-        k_solve_exact32<<<(unsigned)g, threads, SMEM32, s>>>(J, P, node_list, n_list);
+        k_solve_exact32<<<(unsigned)g, threads, SMEM32, s>>>(J, P, routed);
     } else {
         const long long g = persistent_grid((const void *)k_solve_mixed32, threads, SMEM32, blocks_per_sm, units);
         k_solve_mixed32<<<(unsigned)g, threads, SMEM32, s>>>(J, P);

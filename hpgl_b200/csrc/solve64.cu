@@ -482,25 +482,40 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sgs_try64(DevJob J, DevP
     }
 }
 
-__global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, DevPlan P, const int *list,
-                                                                      const int *n_list) {
+// routed: per-node flags of the mixed pass -- the flagged nodes are solved,
+// 32 flags read at a time and taken in node order (every node once the job
+// was abandoned); null: every node.
+__global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, DevPlan P, const uint8_t *routed) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ int s_cs[N64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Exact64Smem &S = reinterpret_cast<Exact64Smem *>(dyn_smem)[warp];
-    const long long count = list ? (long long)*n_list : J.size;
     const long long stride = (long long)gridDim.x * WARPS64_BLOCK;
     unsigned long long solved = 0;
     long long it = (long long)blockIdx.x * WARPS64_BLOCK + warp;
-    NodeFetch cur = fetch_node(J, P, it < count ? (list ? list[it] : (int)it) : -1, lane);
-    for (; it < count; it += stride) {
-        const long long nx = it + stride;
-        const NodeFetch next = fetch_node(J, P, nx < count ? (list ? list[nx] : (int)nx) : -1, lane);
-        solved += exact64_node(J, P, S, s_cs, cur, lane);
-        __syncwarp();
-        cur = next;
+    if (routed && !*J.abandon) {
+        for (long long base = it * 32; base < J.size; base += stride * 32) {
+            const long long i = base + lane;
+            unsigned m = __ballot_sync(FULL_MASK, i < J.size && routed[i]);
+            while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1;
+                const NodeFetch f = fetch_node(J, P, (int)(base + k), lane);
+                solved += exact64_node(J, P, S, s_cs, f, lane);
+                __syncwarp();
+            }
+        }
+    } else {
+        NodeFetch cur = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
+        for (; it < J.size; it += stride) {
+            const long long nx = it + stride;
+            const NodeFetch next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
+            solved += exact64_node(J, P, S, s_cs, cur, lane);
+            __syncwarp();
+            cur = next;
+        }
     }
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
 }
@@ -608,7 +623,7 @@ __device__ __forceinline__ int mixed64_node(const DevJob &J, const DevPlan &P, M
     const int node = cur.node;
     if (copy_informed64(J, cur, lane)) return -1;
     if (skip && cur.n > 0) {
-        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        if (lane == 0) route(J, node);
         __syncwarp();
         return 1;
     }
@@ -693,7 +708,7 @@ __device__ __forceinline__ int mixed64_node(const DevJob &J, const DevPlan &P, M
         __syncwarp();
     }
     if (low) {
-        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        if (lane == 0) route(J, node);
         __syncwarp();
         return 1;
     }
@@ -739,7 +754,7 @@ __device__ __forceinline__ int mixed64_node(const DevJob &J, const DevPlan &P, M
         }
     }
     if (!converged) {
-        if (lane == 0) J.routed[atomicAdd(J.n_routed, 1)] = node;
+        if (lane == 0) route(J, node);
         __syncwarp();
         return 1;
     }
@@ -792,12 +807,15 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     long long it = blockIdx.x;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
     RouteGuess guess;
+    AttemptTally tally;
     for (; it < J.size; it += gridDim.x) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + gridDim.x < J.size ? (int)(it + gridDim.x) : -1, lane);
         const bool attempt = guess.attempt();
-        guess.record(attempt, mixed64_node(J, P, S, s_cs, cur, lane, !attempt));
+        const int outcome = mixed64_node(J, P, S, s_cs, cur, lane, !attempt);
+        guess.record(attempt, outcome);
         __syncwarp();
+        if (tally.step(J, attempt, outcome, lane)) break;
     }
 }
 
@@ -929,12 +947,11 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sis_try64(DevJob J, cons
 
 }  // namespace
 
-void launch_solve64_exact(const DevJob &J, const DevPlan &P, const int *node_list, const int *n_list,
-                          long long n_max, cudaStream_t s, int blocks_per_sm) {
-    if (n_max <= 0) return;
+void launch_solve64_exact(const DevJob &J, const DevPlan &P, const uint8_t *routed, cudaStream_t s,
+                          int blocks_per_sm) {
     const long long g = persistent_grid((const void *)k_solve_exact64, WARPS64_BLOCK * 32, SMEM64_EXACT,
-                                        blocks_per_sm, (n_max + WARPS64_BLOCK - 1) / WARPS64_BLOCK);
-    k_solve_exact64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, node_list, n_list);
+                                        blocks_per_sm, (J.size + WARPS64_BLOCK - 1) / WARPS64_BLOCK);
+    k_solve_exact64<<<(unsigned)g, WARPS64_BLOCK * 32, SMEM64_EXACT, s>>>(J, P, routed);
 }
 
 void launch_sgs_try64(const DevJob &J, const DevPlan &P, const SgsState &G, int cur, cudaStream_t s) {
