@@ -1297,7 +1297,11 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
         set_arena(S, (char *)arena);
         try {
             upload(S, s);
-            device_pass(S, s, nullptr, nullptr);
+            hpgl_b200_result_t &res = *sj->result;
+            const bool want_nb = res.nb_count || res.nb_index;
+            device_pass(S, s, nullptr, [&](const Group &g) {
+                if (want_nb) download_neighbours(S, g, res, s);
+            });
             Counters cnt = read_counters(S, s);
             download(S, *sj->result, cnt, s);
         } catch (...) {
