@@ -1251,9 +1251,51 @@ struct Server {
     int device = 0;
     std::atomic<int> planners{0};  // jobs being planned on the host right now
 
+    // Planned jobs waiting for admission.  Among those that fit (a free slot,
+    // room in the budget) the one with the least estimated device work goes
+    // first -- small jobs do not queue behind large ones, which keeps the
+    // median latency low when jobs arrive faster than the GPU finishes
+    // them -- except that a job waiting longer than AGE_MS goes before all
+    // younger ones (oldest first), so large jobs are not held back for good.
+    struct Waiter {
+        long long ticket;
+        double cost;
+        std::chrono::steady_clock::time_point since;
+        long long bytes;
+    };
+    static constexpr double AGE_MS = 2000.0;
+    std::vector<Waiter *> waiting;
+    bool first_to_admit(const Waiter &w) const {
+        const auto now = std::chrono::steady_clock::now();
+        auto aged = [&](const Waiter *x) {
+            return std::chrono::duration<double, std::milli>(now - x->since).count() >= AGE_MS;
+        };
+        for (const Waiter *o : waiting) {
+            if (o == &w || in_use + o->bytes > budget) continue;
+            const bool ao = aged(o), aw = aged(&w);
+            if (ao != aw) {
+                if (ao) return false;
+                continue;
+            }
+            if (ao ? (o->since < w.since || (o->since == w.since && o->ticket < w.ticket))
+                   : (o->cost < w.cost || (o->cost == w.cost && o->ticket < w.ticket)))
+                return false;
+        }
+        return true;
+    }
+
     void worker_loop();
     void run_one(const std::shared_ptr<ServerJob> &sj);
 };
+
+// Estimated device work of a planned job: its systems times the square of
+// the neighbour count (the solves' cost grows with N^2 to N^3, the searches
+// with N), per category group.
+static double job_cost(const JobState &S) {
+    double c = 0;
+    for (const auto &g : S.groups) c += (double)S.kriged * (double)g.plan.nmax * (double)g.plan.nmax;
+    return c;
+}
 
 void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
     JobState S;
@@ -1280,7 +1322,12 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
         const auto t_wait = std::chrono::steady_clock::now();
         {
             std::unique_lock<std::mutex> l(mu);
-            cv_admit.wait(l, [&] { return stopping || (!free_slots.empty() && in_use + bytes <= budget); });
+            Waiter w{sj->ticket, job_cost(S), t_wait, bytes};
+            waiting.push_back(&w);
+            cv_admit.wait(l, [&] {
+                return stopping || (!free_slots.empty() && in_use + bytes <= budget && first_to_admit(w));
+            });
+            waiting.erase(std::find(waiting.begin(), waiting.end(), &w));
             if (stopping) throw HpglError{HPGL_E_INTERNAL, "server stopped"};
             slot = free_slots.back();
             free_slots.pop_back();
@@ -1288,6 +1335,7 @@ void Server::run_one(const std::shared_ptr<ServerJob> &sj) {
             peak_bytes = std::max(peak_bytes, in_use);
             ++inflight;
             peak_inflight = std::max(peak_inflight, inflight);
+            cv_admit.notify_all();  // the next waiter may fit too
         }
         sj->wait_ms = ms_since(t_wait);
         const auto t_run = std::chrono::steady_clock::now();
