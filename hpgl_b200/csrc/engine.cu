@@ -439,9 +439,6 @@ static void upload_rest(JobState &S, cudaStream_t s) {
         d.my = P.my;
         d.mz = P.mz;
         d.max_candidates = std::max(1, P.max_candidates);
-        d.cbx = P.cand_box[0];
-        d.cby = P.cand_box[1];
-        d.cbz = P.cand_box[2];
     }
 }
 

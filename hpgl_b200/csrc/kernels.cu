@@ -210,12 +210,6 @@ __global__ void __launch_bounds__(CLUSTER_WARPS * 32) k_search_cluster(DevJob J,
             for (int j = cy - 1; j <= cy + 1; ++j)
                 for (int i = cx - 1; i <= cx + 1; ++i) {
                     if (i < 0 || j < 0 || k < 0 || i > P.mx || j > P.my || k > P.mz) continue;
-                    // a box whose cells (widened by one) all lie beyond the
-                    // candidate box holds no candidate that can pass
-                    if (floor(i * P.crx) - 1 - x > P.cbx || x - (ceil((i + 1) * P.crx) + 1) > P.cbx ||
-                        floor(j * P.cry) - 1 - y > P.cby || y - (ceil((j + 1) * P.cry) + 1) > P.cby ||
-                        floor(k * P.crz) - 1 - z > P.cbz || z - (ceil((k + 1) * P.crz) + 1) > P.cbz)
-                        continue;
                     const long long bi = ((long long)k * P.my + j) * P.mx + i;
                     const int s0 = P.bucket_start[bi], s1 = P.bucket_start[bi + 1];
                     for (int base = s0; base < s1; base += 32) {
@@ -227,12 +221,8 @@ __global__ void __launch_bounds__(CLUSTER_WARPS * 32) k_search_cluster(DevJob J,
                             cand = P.bucket_nodes[p];
                             int qx, qy, qz;
                             node_xyz(J, cand, qx, qy, qz);
-                            const int dx = qx - x, dy = qy - y, dz = qz - z;
-                            // beyond the candidate box the covariance cannot exceed the threshold
-                            if (abs(dx) <= P.cbx && abs(dy) <= P.cby && abs(dz) <= P.cbz) {
-                                key = cov_at(P, dx, dy, dz, J.err);
-                                keep = key > thr;
-                            }
+                            key = cov_at(P, qx - x, qy - y, qz - z, J.err);
+                            keep = key > thr;
                         }
                         const uint32_t bal = __ballot_sync(FULL_MASK, keep);
                         const int pos = n + __popc(bal & ((1u << lane) - 1));

@@ -36,9 +36,6 @@ struct DevPlan {
     double crx, cry, crz;
     int mx, my, mz;
     int max_candidates;
-    // clusterizer candidates farther than this box on any axis cannot pass
-    // the covariance filter (Plan::cand_box)
-    int cbx, cby, cbz;
 };
 
 // Division by a runtime-invariant divisor d >= 1 of any n < 2^32 with one

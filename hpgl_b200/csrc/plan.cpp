@@ -184,54 +184,6 @@ double CovModel::operator()(double vx, double vy, double vz) const {
     }
 }
 
-// The clusterizer keeps a candidate when its covariance exceeds C(0)/100
-// (sugarbox_indexed_neighbour_lookup.h:95-105).  Every model is C(0) =
-// sill - nugget below h = 1e-4 and a non-increasing function of the
-// transformed distance h = |t v| above, so C(v) > C(0)/100 needs h < h*,
-// where the model reaches C(0)/100 at h* (exponential a ln(100)/3, Gaussian
-// a sqrt(ln(100)/3), spherical a x* with 1 - 1.5 x* + 0.5 x*^3 = 0.01).  The
-// offsets with h <= h lie in the ellipsoid v = t^-1 u, |u| <= h, whose extent
-// along axis i is h |row i of t^-1|; with a relative margin of 1e-9 on h*
-// (far beyond the rounding of the model's own evaluation) and one more cell,
-// no offset outside the box can pass the test.  Where the model is not of
-// this form (C(0) <= 0, a negative range) the box covers everything.
-static void candidate_box(const CovModel &cov, int box[3]) {
-    const int all = 1 << 29;
-    box[0] = box[1] = box[2] = all;
-    const double c = cov.sill - cov.nugget, a = cov.range0;
-    if (!(c > 0) || !(a > 0)) return;
-    double xs;  // h* / a
-    if (cov.type == 1) {
-        xs = std::log(100.0) / 3;
-    } else if (cov.type == 2) {
-        xs = std::sqrt(std::log(100.0) / 3);
-    } else {
-        double lo = 0, hi = 1;  // 1 - 1.5x + 0.5x^3 falls from 1 to 0 on [0, 1]
-        for (int it = 0; it < 200; ++it) {
-            const double m = 0.5 * (lo + hi);
-            if (1 - 1.5 * m + 0.5 * m * m * m > 0.01) lo = m;
-            else hi = m;
-        }
-        xs = hi;
-    }
-    const double hs = a * xs * (1 + 1e-9) + 1e-9;
-    const double *t = cov.t;
-    const double det = t[0] * (t[4] * t[8] - t[5] * t[7]) - t[1] * (t[3] * t[8] - t[5] * t[6]) +
-                       t[2] * (t[3] * t[7] - t[4] * t[6]);
-    if (!(std::fabs(det) > 0)) return;
-    // rows of the inverse (adjugate / det)
-    const double inv[9] = {(t[4] * t[8] - t[5] * t[7]) / det, (t[2] * t[7] - t[1] * t[8]) / det,
-                           (t[1] * t[5] - t[2] * t[4]) / det, (t[5] * t[6] - t[3] * t[8]) / det,
-                           (t[0] * t[8] - t[2] * t[6]) / det, (t[2] * t[3] - t[0] * t[5]) / det,
-                           (t[3] * t[7] - t[4] * t[6]) / det, (t[1] * t[6] - t[0] * t[7]) / det,
-                           (t[0] * t[4] - t[1] * t[3]) / det};
-    for (int i = 0; i < 3; ++i) {
-        const double e = hs * std::sqrt(inv[3 * i] * inv[3 * i] + inv[3 * i + 1] * inv[3 * i + 1] +
-                                        inv[3 * i + 2] * inv[3 * i + 2]);
-        if (e < (double)all) box[i] = (int)std::floor(e) + 1;
-    }
-}
-
 void validate_params(const KrigingParams &p, int kind) {
     if (p.cov_type < 0 || p.cov_type > 2) throw std::invalid_argument("covariance type must be 0, 1 or 2");
     for (int i = 0; i < 3; ++i) {
@@ -380,7 +332,6 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     };
     validate_params(p, kind);
     CovModel cov(p);
-    candidate_box(cov, P.cand_box);
     P.kind = kind;
     P.nx = nx;
     P.ny = ny;

@@ -75,9 +75,6 @@ struct Plan {
     bool any_clean = false;
     int max_candidates = 0;               // largest candidate count of a clean neighbourhood
     long long informed = 0;               // informed nodes of the mask
-    // half-extents of a box outside which no offset's covariance exceeds
-    // C(0)/100: clusterizer candidates beyond it need no table read
-    int cand_box[3] = {0, 0, 0};
 
     // padded informed-bit rows for the template search
     int px = 0;      // x padding in cells, a multiple of 32
