@@ -109,44 +109,34 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
 // shared-memory bank at most twice per 32 doubles, the minimum.
 __device__ __forceinline__ int msw(int i, int j) { return j * 33 + (i ^ (j >> 2)); }
 
-// The full symmetric system into S.A (column k at k*33, msw): the n(n-1)/2
-// entries A(i,k) = C(x_i - x_k), i < k (my_kriging_weights.h:49-58,
-// 156-165), gathered 32 pairs at a time with 8 gathers in flight per lane,
-// each stored at (i,k) and (k,i); diagonal C(0); the identity beyond n.
+// The full symmetric system into S.A (column k at k*33, msw): the entries
+// A(i,k) = C(x_i - x_k) (my_kriging_weights.h:49-58, 156-165; the tables
+// are exactly symmetric, C(v) = C(-v) bit for bit, so either orientation
+// gives the reference's value); diagonal C(0); the identity beyond n.
+// Lane l takes the pairs (l, l+d mod 32), d = 1..16 (d = 16 on lanes 0-15
+// only): every off-diagonal pair once, all 16 gathers of a lane in flight
+// together, and the zero padding written by the same stores.
 __device__ __forceinline__ void build_full32(const DevJob &J, const DevPlan &P, SysSmem &S, int n, int lane) {
-    const int npairs = n * (n - 1) / 2;
-    for (int p0 = 0; p0 < npairs; p0 += 256) {
-        double v[8];
-        int ik[8];
+    const int4 a = S.nb[lane];
+    double v[16];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int p = p0 + 32 * e + lane;
-            ik[e] = -1;
-            v[e] = 0.0;
-            if (p < npairs) {
-                ik[e] = __ldg(g_pairs64.v + p);
-                const int4 a = S.nb[ik[e] & 0xff], b = S.nb[ik[e] >> 8];
-                v[e] = cov_lin(P, a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, J.err);
-            }
+    for (int d = 1; d <= 16; ++d) {
+        const int k = (lane + d) & 31;
+        v[d - 1] = 0.0;
+        if (lane < n && k < n && (d < 16 || lane < 16)) {
+            const int4 b = S.nb[k];
+            v[d - 1] = cov_lin(P, a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, J.err);
         }
+    }
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            if (ik[e] >= 0) {
-                const int i = ik[e] & 0xff, k = ik[e] >> 8;
-                S.A[msw(i, k)] = v[e];
-                S.A[msw(k, i)] = v[e];
-            }
+    for (int d = 1; d <= 16; ++d) {
+        const int k = (lane + d) & 31;
+        if (d < 16 || lane < 16) {
+            S.A[msw(lane, k)] = v[d - 1];
+            S.A[msw(k, lane)] = v[d - 1];
         }
     }
     S.A[msw(lane, lane)] = lane < n ? __ldg(P.table + P.center) : 1.0;
-    if (lane >= n) {
-        for (int c = 0; c < N32; ++c) {
-            if (c != lane) {
-                S.A[msw(lane, c)] = 0.0;
-                S.A[msw(c, lane)] = 0.0;
-            }
-        }
-    }
     __syncwarp();
 }
 
