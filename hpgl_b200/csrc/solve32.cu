@@ -33,7 +33,7 @@ constexpr int MIXED_MAX_CORR = 4;
 // columns of 34: NC * 34 for systems of at most NC neighbours).
 template <int NA>
 struct SysSmemN {
-    double A[NA];           // exact: in-place factor (column k at k*34); mixed: full system (LD 33)
+    double A[NA];           // exact: in-place factor (column k at k*34); mixed: full system (LD 32, msw)
     double vd[N32];         // double vector broadcast
     float vf[2][N32];       // float vector broadcast
     float row[2][N32];      // mixed: pivot row broadcast (double buffered)
@@ -102,14 +102,16 @@ __device__ __forceinline__ NodeData load_node(const DevJob &J, const DevPlan &P,
     return d;
 }
 
-// Position of A(i, j) in the mixed kernel's FP64 system: column j at j*33,
+// Position of A(i, j) in the mixed kernel's FP64 system: column j at j*32,
 // row i XOR-swizzled by j/4 within it.  A lane reading its row (the FP64
 // residuals, lane = row) and the lanes reading 8x4 tiles (the FP32 copy,
 // rows 8 (lane/8) .. +7, columns 4 (lane%8) .. +3) both hit every
-// shared-memory bank at most twice per 32 doubles, the minimum.
-__device__ __forceinline__ int msw(int i, int j) { return j * 33 + (i ^ (j >> 2)); }
+// shared-memory bank at most twice per 32 doubles, the minimum; the build's
+// stores along the cyclic diagonals (l, l+d) and (l+d, l) take 86
+// wavefronts a system against 62 at best (128 with a column stride of 33).
+__device__ __forceinline__ int msw(int i, int j) { return j * 32 + (i ^ (j >> 2)); }
 
-// The full symmetric system into S.A (column k at k*33, msw): the entries
+// The full symmetric system into S.A (column k at k*32, msw): the entries
 // A(i,k) = C(x_i - x_k) (my_kriging_weights.h:49-58, 156-165; the tables
 // are exactly symmetric, C(v) = C(-v) bit for bit, so either orientation
 // gives the reference's value); diagonal C(0); the identity beyond n.
