@@ -210,32 +210,35 @@ __device__ __forceinline__ double pair_cov64(const DevJob &J, const DevPlan &P, 
 }
 
 // Build: the n(n-1)/2 entries A(i, k) = C(x_i - x_k), i < k, of the upper
-// triangle into the skewed packed layout, in column order, 32 at a time
-// (pairs[p] = i | k << 8); lanes stay converged and the gathers of 8 pairs
-// are issued together.  Columns from n on are left as they are.
+// triangle into the skewed packed layout (my_kriging_weights.h:49-58; the
+// tables are exactly symmetric, C(v) = C(-v) bit for bit, so either
+// orientation gives the reference's value).  Lane l takes the pairs
+// (r, r + d mod 64) of its rows r = l, l + 32 for d = 1..31, and (l, l + 32):
+// every pair once, 63 a lane, 16 gathers in flight per trip.  Columns from n
+// on are left as they are.
 template <bool CORR>
 __device__ __forceinline__ void build_packed(const DevJob &J, const DevPlan &P, double *U, const int4 *nb,
-                                             const int *cs, const uint16_t *pairs, int n, int lane,
-                                             const double *sg) {
-    const int npairs = n * (n - 1) / 2;
-    for (int p0 = 0; p0 < npairs; p0 += 256) {
-        double v[8];
-        int dst[8];
+                                             const int *cs, int n, int lane, const double *sg) {
+    const int4 own[2] = {nb[lane], nb[lane + 32]};
+#pragma unroll 1
+    for (int d0 = 1; d0 <= 32; d0 += 8) {
+        double v[16];
+        int dst[16];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int p = p0 + 32 * e + lane;
+        for (int e = 0; e < 16; ++e) {
+            const int d = d0 + (e >> 1), h = e & 1;
+            const int r = lane + 32 * h, k = (r + d) & 63;
             dst[e] = -1;
             v[e] = 0.0;
-            if (p < npairs) {
-                const int ik = __ldg(pairs + p);
-                const int i = ik & 0xff, k = ik >> 8;
-                v[e] = pair_cov64(J, P, nb[i], nb[k]);
-                if (CORR) v[e] = __dmul_rn(v[e], __dmul_rn(sg[k], sg[i]));
-                dst[e] = cs[k] + i;
+            if (r < n && k < n && (d < 32 || h == 0)) {
+                v[e] = pair_cov64(J, P, own[h], nb[k]);
+                const int lo = r < k ? r : k, hi = r < k ? k : r;
+                if (CORR) v[e] = __dmul_rn(v[e], __dmul_rn(sg[hi], sg[lo]));
+                dst[e] = cs[hi] + lo;
             }
         }
 #pragma unroll
-        for (int e = 0; e < 8; ++e)
+        for (int e = 0; e < 16; ++e)
             if (dst[e] >= 0) U[dst[e]] = v[e];
     }
     __syncwarp();
@@ -246,12 +249,12 @@ __device__ __forceinline__ void build_packed(const DevJob &J, const DevPlan &P, 
 // (corellogramed_weights_3, my_kriging_weights.h:308-317; b is scaled by
 // the caller).
 template <bool CORR>
-__device__ int exact64_core(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs, const uint16_t *pairs,
+__device__ int exact64_core(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs,
                             int lane, const Node64 &d, const double *sg, double &w0_out, double &w1_out) {
     const int n = d.n;
     const bool ordinary = J.kind == 0;
     double *U = S.U;
-    build_packed<CORR>(J, P, U, S.nb, cs, pairs, n, lane, sg);
+    build_packed<CORR>(J, P, U, S.nb, cs, n, lane, sg);
     const int k0 = lane, k1 = lane + 32;  // the lane's columns in the factorisation
     const double a_diag = __ldg(P.table + P.center);  // A(k,k) = C(0), the table's centre
     // diagonal slots and pads of the lane's columns are zero until their step
@@ -417,13 +420,13 @@ __device__ int exact64_core(const DevJob &J, const DevPlan &P, Exact64Smem &S, c
     return status;
 }
 
-__device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs,
-                               const uint16_t *pairs, int node, int lane, const Node64 &d) {
+__device__ void exact64_system(const DevJob &J, const DevPlan &P, Exact64Smem &S, const int *cs, int node,
+                               int lane, const Node64 &d) {
     const int n = d.n;
     const bool ordinary = J.kind == 0;
     const int n0 = n < 32 ? n : 32;
     double w0, w1;
-    const int status = exact64_core<false>(J, P, S, cs, pairs, lane, d, nullptr, w0, w1);
+    const int status = exact64_core<false>(J, P, S, cs, lane, d, nullptr, w0, w1);
     double variance = -1.0;
     if (J.variance && status == ST_SUCCESS) {
         double v = P.c0;
@@ -445,7 +448,7 @@ __device__ __forceinline__ bool exact64_node(const DevJob &J, const DevPlan &P, 
         write_outputs64(J, P, cur.node, lane, d, ST_NO_NEIGHBOURS, 0.0, 0.0, -1.0);
         return false;
     }
-    exact64_system(J, P, S, cs, g_pairs64.v, cur.node, lane, d);
+    exact64_system(J, P, S, cs, cur.node, lane, d);
     return true;
 }
 
@@ -633,7 +636,7 @@ __device__ __forceinline__ int mixed64_node(const DevJob &J, const DevPlan &P, M
         return -1;
     }
     const int n = d.n;
-    build_packed<false>(J, P, S.U, S.nb, cs, g_pairs64.v, n, lane, nullptr);
+    build_packed<false>(J, P, S.U, S.nb, cs, n, lane, nullptr);
     // Rows lane and lane + 32 of the unit-diagonal system A / C(0),
     // identity beyond n.
     float2 m0[32], m1[32];
@@ -927,8 +930,8 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_sis_try64(DevJob J, cons
                 const Node64 d = sis_load64(J, P, S, node, list, cnt, k, sgc, lane);
                 double w0, w1;
                 const int status =
-                    J.sis_corr ? exact64_core<true>(J, P, S.e, s_cs, g_pairs64.v, lane, d, S.sg, w0, w1)
-                               : exact64_core<false>(J, P, S.e, s_cs, g_pairs64.v, lane, d, nullptr, w0, w1);
+                    J.sis_corr ? exact64_core<true>(J, P, S.e, s_cs, lane, d, S.sg, w0, w1)
+                               : exact64_core<false>(J, P, S.e, s_cs, lane, d, nullptr, w0, w1);
                 if (status == ST_SUCCESS) {
                     const double t0 = __dmul_rn(w0, (double)d.dv[0]), t1 = __dmul_rn(w1, (double)d.dv[1]);
                     prob = rows_dsum((double)mc, t0, t1, cnt);
