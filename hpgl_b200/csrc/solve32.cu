@@ -283,13 +283,13 @@ __device__ __forceinline__ int exact_core(const DevJob &J, const DevPlan &P, SM 
     double c[NC];
 #pragma unroll
     for (int i = 0; i < NC; ++i) {
-        // A(i, lane) = C(x_i - x_lane) for i <= lane (my_kriging_weights.h:53)
-        const int ix = __shfl_sync(FULL_MASK, d.ox, i), iy = __shfl_sync(FULL_MASK, d.oy, i);
-        const int iz = __shfl_sync(FULL_MASK, d.oz, i), il = __shfl_sync(FULL_MASK, d.lin, i);
+        // A(i, lane) = C(x_i - x_lane) for i <= lane (my_kriging_weights.h:53);
+        // neighbour i's offsets are one broadcast read of S.nb
+        const int4 q = S.nb[i];
         const double si = CORR ? __shfl_sync(FULL_MASK, sg, i) : 0.0;
         c[i] = 0.0;
         if (i <= lane && lane < n) {
-            c[i] = cov_lin(P, ix - d.ox, iy - d.oy, iz - d.oz, il - d.lin, J.err);
+            c[i] = cov_lin(P, q.x - d.ox, q.y - d.oy, q.z - d.oz, q.w - d.lin, J.err);
             if (CORR) c[i] = __dmul_rn(c[i], __dmul_rn(sg, si));
         }
     }
