@@ -29,7 +29,9 @@ Metric: kriged nodes/s.
 ``--workload sgs``: sequential Gaussian and indicator simulation
 (hpgl_b200/bench_sim.py); ``--workload cokriging``: colocated simple
 cokriging, Markov models I and II (hpgl_b200/bench_cok.py); ``--workload
-configs``: every kriging configuration, mixed and FP64 (hpgl_b200/bench_configs.py).
+configs``: every kriging configuration, mixed and FP64 (hpgl_b200/bench_configs.py);
+``--workload serve_jobs``: the serving stream's jobs each alone
+(hpgl_b200/bench_serve_jobs.py; ``--job``, ``--crop`` for profiling).
 
 Multi-GPU: the path has no exchange step; N ranks (torchrun, one per GPU)
 each krige their own copy of the job ("replicas only", weak scaling).
@@ -188,12 +190,16 @@ def main():
     ap.add_argument("--serve-rates", default="5,20,50,100,200", help="arrival rates (jobs/s) of the serving sweep")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same workload on another grid (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch setting (profiling runs)")
-    ap.add_argument("--workload", default="krige", choices=["krige", "inc_io", "variogram", "sgs", "cokriging", "configs"],
+    ap.add_argument("--job", default=None, help="serve_jobs: keep the stream's job of this name")
+    ap.add_argument("--crop", default=None, help="serve_jobs: NXxNYxNZ, cut the job's cube (profiling runs)")
+    ap.add_argument("--workload", default="krige",
+                    choices=["krige", "inc_io", "variogram", "sgs", "cokriging", "configs", "serve_jobs"],
                     help="inc_io: INC property file read/write (hpgl_b200/bench_io.py); variogram: experimental "
                          "variograms (hpgl_b200/bench_variogram.py); sgs: sequential Gaussian and indicator "
                          "simulation (hpgl_b200/bench_sim.py); cokriging: colocated simple cokriging "
                          "(hpgl_b200/bench_cok.py); configs: every kriging configuration "
-                         "(hpgl_b200/bench_configs.py); one GPU")
+                         "(hpgl_b200/bench_configs.py); serve_jobs: the serving stream's jobs each alone "
+                         "(hpgl_b200/bench_serve_jobs.py); one GPU")
     args = ap.parse_args()
     if args.workload == "inc_io":
         from hpgl_b200 import bench_io
@@ -210,6 +216,9 @@ def main():
     if args.workload == "configs":
         from hpgl_b200 import bench_configs
         return bench_configs.run(args, ROOT)
+    if args.workload == "serve_jobs":
+        from hpgl_b200 import bench_serve_jobs
+        return bench_serve_jobs.run(args, ROOT)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)
