@@ -28,7 +28,7 @@ CXX_FLAGS = ["-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wno-u
              "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include"]
 
 SOURCES_CU = ["kernels.cu", "solve32.cu", "solve64.cu", "cokriging.cu", "engine.cu", "sk_weights.cu", "textio.cu", "variogram.cu", "peak.cu"]
-SOURCES_CXX = ["plan.cpp", "api.cpp", "sgs_host.cpp"]
+SOURCES_CXX = ["plan.cpp", "api.cpp", "sgs_host.cpp", "task_pool.cpp"]
 
 
 def _run(cmd, log=None):

@@ -23,6 +23,7 @@
 
 #include "engine.h"
 #include "sgs_host.h"
+#include "task_pool.h"
 #include "kernels.cuh"
 
 namespace hpgl_b200 {
@@ -290,12 +291,8 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
         S.sk_mean = job.sk_automatic_mean ? informed_mean(job.values, job.mask, S.size) : job.sk_mean;
     S.want_variance = res.variance != nullptr || (job.sequential && cont);
     S.want_weights = res.weights != nullptr;
-    S.kriged = 0;
-    if (cont) {
-        for (long long i = 0; i < S.size; ++i) S.kriged += job.mask[i] == 0;
-    } else {
-        S.kriged = S.size;
-    }
+    // the plan counted the informed cells (every plan of the job reads the same mask)
+    S.kriged = cont ? S.size - S.groups[0].plan.informed : S.size;
 
     // arena layout
     const size_t n = (size_t)S.size, slots = n * S.status_stride;
@@ -613,22 +610,11 @@ static Counters read_counters(const JobState &S, cudaStream_t s) {
     return c;
 }
 
-// memcpy on up to host_threads() threads, at least 4 MiB each.
+// memcpy on up to host_threads() pool threads, at least 4 MiB each.
 static void parallel_copy(void *dst, const void *src, size_t bytes) {
-    const size_t grain = 4u << 20;
-    const int threads = (int)std::max<size_t>(1, std::min<size_t>((size_t)host_threads(), bytes / grain));
-    if (threads == 1) {
-        memcpy(dst, src, bytes);
-        return;
-    }
-    const size_t chunk = (bytes + threads - 1) / threads;
-    std::vector<std::thread> pool;
-    for (int t = 0; t < threads; ++t) {
-        const size_t lo = (size_t)t * chunk, hi = std::min(bytes, lo + chunk);
-        if (lo >= hi) break;
-        pool.emplace_back([=] { memcpy((char *)dst + lo, (const char *)src + lo, hi - lo); });
-    }
-    for (auto &th : pool) th.join();
+    pool_for((long long)bytes, host_threads(), [=](long long lo, long long hi) {
+        memcpy((char *)dst + lo, (const char *)src + lo, (size_t)(hi - lo));
+    }, 4LL << 20);
 }
 
 // staging: pinned host memory of at least the main outputs' size (the

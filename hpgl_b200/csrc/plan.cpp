@@ -16,15 +16,13 @@
 #include <thread>
 
 #include "introsort.h"
+#include "task_pool.h"
 
 namespace hpgl_b200 {
 
 
 
 static std::atomic<int> g_threads{0};
-
-template <typename F>
-static void parallel_for(long long n, int threads, F f, long long grain = 4096);
 
 int host_threads() {
     int n = g_threads.load();
@@ -35,23 +33,11 @@ int host_threads() {
 
 void set_host_threads(int n) { g_threads.store(n > 0 ? n : 0); }
 
-// f(lo, hi) over [0, n) split across up to `threads` threads, at least
-// `grain` items per thread.
+// f(lo, hi) over [0, n) split across up to `threads` threads of the pool, at
+// least `grain` items per thread.
 template <typename F>
-static void parallel_for(long long n, int threads, F f, long long grain) {
-    threads = (int)std::max<long long>(1, std::min<long long>(threads, n / grain + 1));
-    if (threads == 1) {
-        f(0LL, n);
-        return;
-    }
-    std::vector<std::thread> pool;
-    long long chunk = (n + threads - 1) / threads;
-    for (int t = 0; t < threads; ++t) {
-        long long lo = t * chunk, hi = std::min(n, lo + chunk);
-        if (lo >= hi) break;
-        pool.emplace_back([=] { f(lo, hi); });
-    }
-    for (auto &th : pool) th.join();
+static void parallel_for(long long n, int threads, F f, long long grain = 4096) {
+    pool_for(n, threads, f, grain);
 }
 
 // C(v) over the box |v_i| <= r_i into out[((z+rz)*(2ry+1) + y+ry)*(2rx+1) + x+rx],
@@ -86,11 +72,10 @@ static void fill_symmetric(std::vector<double> &out, int rx, int ry, int rz, int
 constexpr int SORT_SPAWN_MIN = 4096;
 
 // The reference's std::sort permutation (introsort.h) with the independent
-// right-hand sub-ranges of large partitions sorted on other threads: each
+// right-hand sub-ranges of large partitions sorted as pool tasks: each
 // sub-range's processing touches only its own elements, so the result is
-// the sequential algorithm's, element for element.
-static void sort_subrange(SortArr a, int lo, int hi, int depth, std::atomic<int> &spare,
-                          std::vector<std::thread> &spawned, std::mutex &mu) {
+// the sequential algorithm's, element for element, whatever runs where.
+static void sort_subrange(SortArr a, int lo, int hi, int depth, TaskGroup &g) {
     while (hi - lo > 16) {
         if (depth == 0) {
             sort_heapsort(a, lo, hi);
@@ -100,13 +85,10 @@ static void sort_subrange(SortArr a, int lo, int hi, int depth, std::atomic<int>
         const int mid = lo + (hi - lo) / 2;
         sort_median_to_first(a, lo, lo + 1, mid, hi - 1);
         const int cut = sort_partition(a, lo + 1, hi, lo);
-        if (hi - cut > SORT_SPAWN_MIN && spare.fetch_sub(1) > 0) {
-            std::lock_guard<std::mutex> l(mu);
-            spawned.emplace_back([=, &spare, &spawned, &mu] { sort_subrange(a, cut, hi, depth, spare, spawned, mu); });
-        } else {
-            if (hi - cut > SORT_SPAWN_MIN) spare.fetch_add(1);
-            sort_subrange(a, cut, hi, depth, spare, spawned, mu);
-        }
+        if (hi - cut > SORT_SPAWN_MIN)
+            task_submit(g, [a, cut, hi, depth, &g] { sort_subrange(a, cut, hi, depth, g); });
+        else
+            sort_subrange(a, cut, hi, depth, g);
         hi = cut;
     }
 }
@@ -115,20 +97,16 @@ static void parallel_reference_sort(std::vector<double> &key, std::vector<int> &
     const int n = (int)key.size();
     if (n <= 1) return;
     SortArr a{key.data(), idx.data()};
-    std::atomic<int> spare(threads - 1);
-    std::vector<std::thread> spawned;
-    std::mutex mu;
-    sort_subrange(a, 0, n, 2 * sort_floor_log2(n), spare, spawned, mu);
-    while (true) {
-        std::thread t;
-        {
-            std::lock_guard<std::mutex> l(mu);
-            if (spawned.empty()) break;
-            t = std::move(spawned.back());
-            spawned.pop_back();
-        }
-        t.join();
+    if (threads > 1) task_pool_reserve(threads - 1);
+    TaskGroup g;
+    std::exception_ptr own;
+    try {
+        sort_subrange(a, 0, n, 2 * sort_floor_log2(n), g);
+    } catch (...) {
+        own = std::current_exception();
     }
+    task_wait(g);
+    if (own) std::rethrow_exception(own);
     if (n > 16) {
         sort_insertion(a, 0, 16);
         for (int i = 16; i < n; ++i) sort_linear_insert(a, i);
@@ -403,22 +381,21 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
             for (int a = 0; a < 3; ++a) P.ext[a] = std::max(P.ext[a], ez[3 * zi + a]);
         }
     }
+    lap("keys");
     // Every collected key is above the threshold, so the template keeps all
     // of them and the clusterizer's limit (|template| / 250) is known before
-    // the sort: the buckets are built on their own thread meanwhile.
+    // the sort: the buckets are built as a pool task meanwhile.
     const int bucket_threads = std::max(1, threads / 4);
-    std::exception_ptr bucket_error;
-    std::thread bucket_thread([&] {
-        try {
-            build_buckets(P, nx, ny, nz, p, mask, (long long)(keys.size() / 250), bucket_threads);
-        } catch (...) {
-            bucket_error = std::current_exception();
-        }
-    });
+    TaskGroup bucket_task;
+    task_pool_reserve(1);
+    task_submit(bucket_task, [&] { build_buckets(P, nx, ny, nz, p, mask, (long long)(keys.size() / 250), bucket_threads); });
     try {
         parallel_reference_sort(keys, order, threads);
     } catch (...) {
-        bucket_thread.join();
+        try {
+            task_wait(bucket_task);
+        } catch (...) {
+        }
         throw;
     }
     lap("sort");
@@ -451,8 +428,7 @@ void build_plan(Plan &P, int kind, int nx, int ny, int nz, const KrigingParams &
     }
 
     lap("template");
-    bucket_thread.join();
-    if (bucket_error) std::rethrow_exception(bucket_error);
+    task_wait(bucket_task);
     if ((long long)(P.tmpl.size() / 250) != P.limit)
         build_buckets(P, nx, ny, nz, p, mask, (long long)(P.tmpl.size() / 250), threads);
     lap("buckets");

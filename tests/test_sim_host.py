@@ -23,7 +23,8 @@ def shc(tmp_path_factory):
     out = str(tmp_path_factory.mktemp("shc") / "sim_host_check.so")
     subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-pthread", "-o", out,
                     "-I", os.path.join(ROOT, "include"), os.path.join(HERE, "cpp", "sim_host_check.cpp"),
-                    os.path.join(SRC, "sgs_host.cpp"), os.path.join(SRC, "plan.cpp")], check=True,
+                    os.path.join(SRC, "sgs_host.cpp"), os.path.join(SRC, "plan.cpp"),
+                    os.path.join(SRC, "task_pool.cpp")], check=True,
                    capture_output=True)
     lib = C.CDLL(out)
     lib.shc_path.restype = C.c_longlong
