@@ -339,7 +339,13 @@ static void prepare(JobState &S, const hpgl_b200_job_t &job, const hpgl_b200_res
     }
     A.cluster_warps = 0;
     if (any_clean) {
-        A.cluster_warps = std::min<long long>((long long)sm_count_host() * 32, (S.size + 31) / 32 * 32);
+        // 64 warps a SM (the kernel's 16 blocks of 4: the search waits on
+        // memory, and more warps hide more of it), fewer where the candidate
+        // scratch (12 bytes a candidate a warp) would pass 4 GiB
+        const long long sms = sm_count_host();
+        const long long by_scratch = (4LL << 30) / std::max<long long>(1, (long long)max_cand * 12);
+        const long long warps = std::min(sms * 64, std::max(sms * 8, by_scratch));
+        A.cluster_warps = std::min<long long>(warps, (S.size + 31) / 32 * 32);
         A.o_skey = take((size_t)A.cluster_warps * max_cand * 8);
         A.o_sidx = take((size_t)A.cluster_warps * max_cand * 4);
     } else {

@@ -186,7 +186,8 @@ __device__ bool warp_reference_sort_prefix(SortArr &a, int n, int k, int lane, S
 // the list.
 constexpr int CLUSTER_WARPS = 4;
 
-__global__ void __launch_bounds__(CLUSTER_WARPS * 32) k_search_cluster(DevJob J, DevPlan P, double *scratch_key,
+// 16 blocks a SM (32 registers): the engine launches 64 warps a SM
+__global__ void __launch_bounds__(CLUSTER_WARPS * 32, 16) k_search_cluster(DevJob J, DevPlan P, double *scratch_key,
                                                                       int *scratch_idx, int n_warps_total) {
     __shared__ SortFrame s_stack[CLUSTER_WARPS][SORT_STACK];
     __shared__ int s_lbuf[CLUSTER_WARPS][32], s_rbuf[CLUSTER_WARPS][32];
