@@ -140,17 +140,22 @@ struct RefineGate {
 // attempt and then the FP64 re-solve, so where most systems are routed
 // (ill-conditioned models, clustered data) attempting loses to the FP64
 // path alone.  A warp keeps an average of its recent attempts' outcomes
-// (weight 1/4 for the newest); below 1/2 it stops attempting and routes its
+// (weight 1/4 for the newest); below `keep` it stops attempting and routes its
 // systems straight to the FP64 re-solve, attempting every 8th again to
 // notice when its nodes become well conditioned.  The warp's node sequence
 // is fixed by the launch, so the choice is the same on every run; routed
 // systems get the FP64 path's results, which the mixed results match
 // within their tolerance either way.
+// A kernel passes the success share below which attempting stops paying:
+// an attempt costs about c of an FP64 solve and saves one when it succeeds,
+// so it pays while the share of successes exceeds c.
 struct RouteGuess {
     float ok = 1.f;
     int skipped = 0;
+    float keep;  // attempt while the recent success share is at least this
+    __device__ explicit RouteGuess(float keep_) : keep(keep_) {}
     __device__ __forceinline__ bool attempt() {
-        if (ok >= 0.5f || skipped >= 7) {
+        if (ok >= keep || skipped >= 7) {
             skipped = 0;
             return true;
         }
@@ -174,16 +179,26 @@ __device__ __forceinline__ void route(const DevJob &J, int node) {
 // are wasted and the re-solve is nearly the plain FP64 pass anyway.  The
 // warps therefore add up their attempts and routed attempts every 16
 // nodes; once at least ABANDON_MIN systems have been
-// attempted and more than ABANDON_FRACTION of them routed, the job is
+// attempted and more than the kernel's `fraction` of them routed, the job is
 // abandoned: the mixed kernel stops, and the re-solve kernel runs the plain
 // FP64 pass over every node instead of the flagged ones (results of nodes
 // the mixed kernel already solved are recomputed, so every result is the
 // FP64 one).
+//
+// The break-even points, measured: a 32-row FP32 attempt costs about 0.42 of
+// the exact 32-row solve (23.2 vs 54.8 ms over the SK 256x256x64 job), so
+// attempts pay above 42 % successes (keep 0.5, abandon above 60 % routed);
+// a 64-row attempt costs about 0.82 of the exact 64-row solve (the median
+// over serving jobs of 38-60 neighbours with nothing routed), so they pay
+// only above about 82 % successes (keep 0.85, abandon above 15 % routed).
 constexpr int ABANDON_MIN = 4096;
-constexpr float ABANDON_FRACTION = 0.6f;
+constexpr float ROUTE_KEEP32 = 0.5f, ABANDON_FRACTION32 = 0.6f;
+constexpr float ROUTE_KEEP64 = 0.85f, ABANDON_FRACTION64 = 0.15f;
 
 struct AttemptTally {
     int att = 0, routed = 0, since = 0;
+    float fraction;
+    __device__ explicit AttemptTally(float fraction_) : fraction(fraction_) {}
     // after each node (outcome of mixed*_node, attempted or not); true once
     // the job is abandoned
     __device__ __forceinline__ bool step(const DevJob &J, bool attempted, int outcome, int lane) {
@@ -198,7 +213,7 @@ struct AttemptTally {
             if (att) {
                 const int a = atomicAdd(J.n_attempt, att) + att;
                 const int r = atomicAdd(J.n_attempt_routed, routed) + routed;
-                if (a >= ABANDON_MIN && (float)r > ABANDON_FRACTION * (float)a) atomicExch(J.abandon, 1);
+                if (a >= ABANDON_MIN && (float)r > fraction * (float)a) atomicExch(J.abandon, 1);
             }
             flag = *reinterpret_cast<volatile int *>(J.abandon);
         }

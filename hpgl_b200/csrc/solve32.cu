@@ -691,8 +691,8 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
     const long long stride = (long long)gridDim.x * WARPS32;
     long long it = (long long)blockIdx.x * WARPS32 + warp;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
-    RouteGuess guess;
-    AttemptTally tally;
+    RouteGuess guess(ROUTE_KEEP32);
+    AttemptTally tally(ABANDON_FRACTION32);
     for (; it < J.size; it += stride) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);

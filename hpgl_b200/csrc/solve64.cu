@@ -809,8 +809,8 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     Mixed64Smem &S = *reinterpret_cast<Mixed64Smem *>(dyn_smem);
     long long it = blockIdx.x;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
-    RouteGuess guess;
-    AttemptTally tally;
+    RouteGuess guess(ROUTE_KEEP64);
+    AttemptTally tally(ABANDON_FRACTION64);
     for (; it < J.size; it += gridDim.x) {
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + gridDim.x < J.size ? (int)(it + gridDim.x) : -1, lane);
