@@ -4,8 +4,9 @@ synchronise the device and stall the caller's other GPU work, and a host
 that reserved the GPU's memory for its own pool leaves nothing to allocate).
 It must give the same weights as hpgl_simple_kriging_weights, which
 allocates its scratch -- bit for bit, the two run the same kernel on the same
-inputs -- on consecutive calls that reuse its fixed scratch array, and reject
-neighbour counts above its stated maximum.
+inputs -- on consecutive calls that reuse its fixed scratch array, reject
+neighbour counts above its stated maximum, and leave the device's free memory
+unchanged (no allocation).
 
 This file is named to be collected last."""
 
@@ -71,3 +72,21 @@ def test_static_entry_rejects_above_maximum(native_lib):
     with pytest.raises(N.HpglError) as e:
         N.sk_weights(c, pts[:, 0], pts[:, 1], pts[:, 2], p, entry=STATIC)
     assert e.value.code == N.HPGL_E_CAPACITY
+
+
+@pytest.mark.gpu
+def test_static_entry_does_not_allocate(native_lib):
+    # the device's free memory is unchanged across static calls once the
+    # first call has loaded the kernel (lazy module loading) and the context
+    import torch
+    rng = np.random.default_rng(14)
+    c, pts, p = _case(rng, STATIC_MAX)
+    N.sk_weights(c, pts[:, 0], pts[:, 1], pts[:, 2], p, entry=STATIC)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for n in (1, 64, STATIC_MAX, 5):
+        c, pts, p = _case(rng, n)
+        N.sk_weights(c, pts[:, 0], pts[:, 1], pts[:, 2], p, entry=STATIC)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
