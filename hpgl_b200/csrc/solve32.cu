@@ -560,6 +560,12 @@ __device__ __forceinline__ double residual_corrected_variance(const SM &S, doubl
 // do not qualify are appended to J.routed.  skip: a system is appended to
 // J.routed at once, without the FP32 attempt.  Returns -1 when the node
 // needs no system, 0 when it was solved here, 1 when routed.
+// STEPS: the sweep's pivots, at least the job's largest neighbour count (a
+// multiple of 8): rows from n on are identity padding, decoupled from the
+// live block, with zero right-hand sides, so their solutions stay zero
+// whether or not their pivots are swept; a job of at most 24 neighbours
+// sweeps 24 pivots, and the steps stay fully unrolled.
+template <int STEPS = N32>
 __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, SysSmem &S, const NodeFetch &cur,
                                             int lane, bool skip = false) {
     const bool ordinary = J.kind == 0;
@@ -598,7 +604,7 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
     // products subtract the 2 v (apply_inverse).
     bool low = false;
 #pragma unroll
-    for (int p = 0; p < N32; ++p) {
+    for (int p = 0; p < STEPS; ++p) {
         float *rb = S.row[p & 1];
         const int rgp = p >> 3, rp = p & 7, cgp = p >> 2, cp = p & 3;
         const bool prow = rg == rgp;
@@ -684,7 +690,8 @@ __device__ __forceinline__ int mixed32_node(const DevJob &J, const DevPlan &P, S
     return 0;
 }
 
-__global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPlan P) {
+template <int STEPS>
+__device__ __forceinline__ void mixed32_warps(const DevJob &J, const DevPlan &P) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
@@ -697,11 +704,20 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPla
         const NodeFetch cur = next;
         next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
         const bool attempt = guess.attempt();
-        const int outcome = mixed32_node(J, P, S, cur, lane, !attempt);
+        const int outcome = mixed32_node<STEPS>(J, P, S, cur, lane, !attempt);
         guess.record(attempt, outcome);
         __syncwarp();
         if (tally.step(J, attempt, outcome, lane)) break;
     }
+}
+
+__global__ void __launch_bounds__(WARPS32 * 32) k_solve_mixed32(DevJob J, DevPlan P) { mixed32_warps<N32>(J, P); }
+
+// jobs of at most 16 or 24 neighbours: the sweep stops there (held to 4
+// blocks a SM, the 128 registers the full sweep compiles to by itself)
+template <int STEPS>
+__global__ void __launch_bounds__(WARPS32 * 32, 4) k_solve_mixed32_short(DevJob J, DevPlan P) {
+    mixed32_warps<STEPS>(J, P);
 }
 
 // Fused search + solve: each warp takes 32-node x-segments, runs the template
@@ -943,7 +959,7 @@ void launch_fused32(const DevJob &J, const DevPlan &P, int precision, cudaStream
     }
 }
 
-const char *mixed32_kernel_name(const DevPlan &) { return "k_solve_mixed32"; }
+const char *mixed32_kernel_name(const DevPlan &P) { return P.nmax <= 24 ? "k_solve_mixed32_short" : "k_solve_mixed32"; }
 
 void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const uint8_t *routed, cudaStream_t s,
                     int blocks_per_sm) {
@@ -953,8 +969,14 @@ void launch_solve32(const DevJob &J, const DevPlan &P, int precision, const uint
         const long long g = persistent_grid((const void *)k_solve_exact32, threads, SMEM32, blocks_per_sm, units);
         k_solve_exact32<<<(unsigned)g, threads, SMEM32, s>>>(J, P, routed);
     } else {
-        const long long g = persistent_grid((const void *)k_solve_mixed32, threads, SMEM32, blocks_per_sm, units);
-        k_solve_mixed32<<<(unsigned)g, threads, SMEM32, s>>>(J, P);
+        // the sweep's length: the job's largest neighbour count rounded up to 8
+        const int steps = P.nmax <= 16 ? 16 : (P.nmax <= 24 ? 24 : 32);
+        const void *k = steps == 16 ? (const void *)k_solve_mixed32_short<16>
+                                    : (steps == 24 ? (const void *)k_solve_mixed32_short<24> : (const void *)k_solve_mixed32);
+        const long long g = persistent_grid(k, threads, SMEM32, blocks_per_sm, units);
+        if (steps == 16) k_solve_mixed32_short<16><<<(unsigned)g, threads, SMEM32, s>>>(J, P);
+        else if (steps == 24) k_solve_mixed32_short<24><<<(unsigned)g, threads, SMEM32, s>>>(J, P);
+        else k_solve_mixed32<<<(unsigned)g, threads, SMEM32, s>>>(J, P);
     }
 }
 
