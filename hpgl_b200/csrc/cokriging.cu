@@ -89,15 +89,58 @@ __device__ void cok_node(const DevJob &J, const DevPlan &P, CokSmem &S, int node
             S.nb[r] = o;
         }
         __syncwarp();
-        // build_system (simple_cokriging_markI.cpp:19-54)
-        const int npairs = n * (n - 1) / 2;
-        for (int p = lane; p < npairs; p += 32) {
-            const int ik = __ldg(g_pairs64.v + p);
-            const int i = ik & 0xff, k = ik >> 8;
-            const int4 a = S.nb[i], c = S.nb[k];
-            const double v = cov_lin(P, a.x - c.x, a.y - c.y, a.z - c.z, a.w - c.w, J.err);
-            S.A[i * LD + k] = v;
-            S.A[k * LD + i] = v;
+        // build_system (simple_cokriging_markI.cpp:19-54): A(i,k) = C(x_i - x_k)
+        // for i != k < n; the table is exactly symmetric (C(v) = C(-v) bit for
+        // bit), so either orientation gives the reference's value.  Pairs
+        // (r, r + d) along cyclic diagonals, all of a lane's gathers of a trip
+        // in flight: for n <= 32, lane l takes (l, l+d mod 32), d = 1..16 (d = 16
+        // on lanes 0-15 only); above, the pairs of its rows l and l+32 with
+        // d = 1..31 mod 64 and (l, l+32).
+        if (n <= 32) {
+            const int4 a = S.nb[lane];
+            double v[16];
+#pragma unroll
+            for (int d = 1; d <= 16; ++d) {
+                const int k = (lane + d) & 31;
+                v[d - 1] = 0.0;
+                if (lane < n && k < n && (d < 16 || lane < 16)) {
+                    const int4 c = S.nb[k];
+                    v[d - 1] = cov_lin(P, a.x - c.x, a.y - c.y, a.z - c.z, a.w - c.w, J.err);
+                }
+            }
+#pragma unroll
+            for (int d = 1; d <= 16; ++d) {
+                const int k = (lane + d) & 31;
+                if (lane < n && k < n && (d < 16 || lane < 16)) {
+                    S.A[lane * LD + k] = v[d - 1];
+                    S.A[k * LD + lane] = v[d - 1];
+                }
+            }
+        } else {
+            const int4 own[2] = {S.nb[lane], S.nb[lane + 32]};
+#pragma unroll 1
+            for (int d0 = 1; d0 <= 32; d0 += 8) {
+                double v[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const int d = d0 + (e >> 1), h = e & 1;
+                    const int r = lane + 32 * h, k = (r + d) & 63;
+                    v[e] = 0.0;
+                    if (r < n && k < n && (d < 32 || h == 0)) {
+                        const int4 c = S.nb[k];
+                        v[e] = cov_lin(P, own[h].x - c.x, own[h].y - c.y, own[h].z - c.z, own[h].w - c.w, J.err);
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const int d = d0 + (e >> 1), h = e & 1;
+                    const int r = lane + 32 * h, k = (r + d) & 63;
+                    if (r < n && k < n && (d < 32 || h == 0)) {
+                        S.A[r * LD + k] = v[e];
+                        S.A[k * LD + r] = v[e];
+                    }
+                }
+            }
         }
         const double c0 = __ldg(P.table + P.center);
 #pragma unroll

@@ -99,19 +99,6 @@ __device__ __forceinline__ NodeFetch fetch_node(const DevJob &J, const DevPlan &
     return f;
 }
 
-// The (row, column) pairs i < k of an upper triangle of up to 64 rows, in
-// column order (i | k << 8): the pairs of an n-row system are the first
-// n(n-1)/2 entries.  Builds walk this list 32 pairs at a time so that every
-// lane gathers the same number of covariances.
-struct PairTable64 {
-    uint16_t v[64 * 63 / 2];
-    constexpr PairTable64() : v() {
-        for (int k = 1, p = 0; k < 64; ++k)
-            for (int i = 0; i < k; ++i) v[p++] = (uint16_t)(i | k << 8);
-    }
-};
-static __device__ const PairTable64 g_pairs64;
-
 // Acceptance of an iterative refinement x <- x + d.  After a correction d_k
 // the remaining error is about rho_k |d_k|, with the contraction rho_k =
 // |d_k| / |d_{k-1}| (for the first correction |d_0| / |x|, the error it
