@@ -81,6 +81,7 @@ struct Counters {
     int n_attempt;         // mixed path: systems attempted in FP32
     int n_attempt_routed;  // and of those routed
     int abandon;           // the job was abandoned to the plain FP64 pass
+    int seg_next;          // template search: the next segment (reset per launch)
     unsigned long long n_fp64;
 };
 
@@ -509,6 +510,7 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.n_attempt = &cnt->n_attempt;
     J.n_attempt_routed = &cnt->n_attempt_routed;
     J.abandon = &cnt->abandon;
+    J.seg_next = &cnt->seg_next;
     J.n_fp64 = &cnt->n_fp64;
     J.err = &cnt->err;
     if (S.cok) {
@@ -552,6 +554,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
         ++launches;
         if (S.cok) {
             // template search, then the cokriging systems (FP64, reference order)
+            CUDA_CHECK(cudaMemsetAsync(J.seg_next, 0, sizeof(int), s));
             launch_search_template(J, g.dp, s);
             if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top0, s));
             launch_cokriging(J, g.dp, s);
@@ -565,6 +568,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
             continue;
         }
         if (tune.schedule == SCHED_SPLIT) {
+            CUDA_CHECK(cudaMemsetAsync(J.seg_next, 0, sizeof(int), s));
             launch_search_template(J, g.dp, s);
             ++launches;
         }

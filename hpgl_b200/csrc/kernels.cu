@@ -39,14 +39,20 @@ __global__ void k_build_bits(DevJob J, DevPlan P, uint32_t *bits) {
 
 // ---------------------------------------------------------------------------
 // Template search: one warp per 32-node x-segment (template_segment in
-// search_common.cuh), persistent over the segments.
+// search_common.cuh), persistent: each warp takes the next segment from a
+// counter, so warps whose segments end early (dense regions) take more and
+// none waits on a fixed share at the end.
 __global__ void __launch_bounds__(256) k_search_template(DevJob J, DevPlan P) {
     __shared__ int delta_sm[8][32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long total = (long long)P.nseg * J.ny * J.nz;
-    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long segi = (long long)blockIdx.x * (blockDim.x >> 5) + wib; segi < total; segi += nwarps)
+    while (true) {
+        int segi = 0;
+        if (lane == 0) segi = atomicAdd(J.seg_next, 1);
+        segi = __shfl_sync(FULL_MASK, segi, 0);
+        if (segi >= total) break;
         template_segment(J, P, segi, lane, delta_sm[wib]);
+    }
 }
 
 // ---------------------------------------------------------------------------
