@@ -82,6 +82,7 @@ struct Counters {
     int n_attempt_routed;  // and of those routed
     int abandon;           // the job was abandoned to the plain FP64 pass
     int seg_next;          // template search: the next segment (reset per launch)
+    int node_next;         // clusterizer search: the next chunk of nodes (reset per launch)
     unsigned long long n_fp64;
 };
 
@@ -511,6 +512,7 @@ static DevJob make_devjob(const JobState &S, const Group &g) {
     J.n_attempt_routed = &cnt->n_attempt_routed;
     J.abandon = &cnt->abandon;
     J.seg_next = &cnt->seg_next;
+    J.node_next = &cnt->node_next;
     J.n_fp64 = &cnt->n_fp64;
     J.err = &cnt->err;
     if (S.cok) {
@@ -573,6 +575,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
             ++launches;
         }
         if (g.plan.any_clean) {
+            CUDA_CHECK(cudaMemsetAsync(J.node_next, 0, sizeof(int), s));
             launch_search_cluster(J, g.dp, at<double>(S, A.o_skey), at<int>(S, A.o_sidx), (int)A.cluster_warps, s);
             ++launches;
         }

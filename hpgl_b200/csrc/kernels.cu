@@ -191,6 +191,7 @@ __device__ bool warp_reference_sort_prefix(SortArr &a, int n, int k, int lane, S
 // std::sort does — as far as the first max_neighbours positions, which become
 // the list.
 constexpr int CLUSTER_WARPS = 4;
+constexpr int CLUSTER_CHUNK = 16;  // nodes a warp takes from the counter at a time
 
 // 16 blocks a SM (32 registers): the engine launches 64 warps a SM
 __global__ void __launch_bounds__(CLUSTER_WARPS * 32, 16) k_search_cluster(DevJob J, DevPlan P, double *scratch_key,
@@ -205,57 +206,66 @@ __global__ void __launch_bounds__(CLUSTER_WARPS * 32, 16) k_search_cluster(DevJo
     double *keys = scratch_key + (long long)gw * cap;
     int *idxs = scratch_idx + (long long)gw * cap;
     const double thr = P.c0 / 100;
-    for (long long node_l = gw; node_l < J.size; node_l += n_warps_total) {
-        const int node = (int)node_l;
-        if (!node_needs_kriging(J, node)) continue;
-        int x, y, z;
-        node_xyz(J, node, x, y, z);
-        if (!node_clean(P, x, y, z)) continue;
-        const int cx = (int)(x / P.crx), cy = (int)(y / P.cry), cz = (int)(z / P.crz);
-        int n = 0;
-        for (int k = cz - 1; k <= cz + 1; ++k)
-            for (int j = cy - 1; j <= cy + 1; ++j)
-                for (int i = cx - 1; i <= cx + 1; ++i) {
-                    if (i < 0 || j < 0 || k < 0 || i > P.mx || j > P.my || k > P.mz) continue;
-                    const long long bi = ((long long)k * P.my + j) * P.mx + i;
-                    const int s0 = P.bucket_start[bi], s1 = P.bucket_start[bi + 1];
-                    for (int base = s0; base < s1; base += 32) {
-                        const int p = base + lane;
-                        bool keep = false;
-                        double key = 0;
-                        int cand = 0;
-                        if (p < s1) {
-                            cand = P.bucket_nodes[p];
-                            int qx, qy, qz;
-                            node_xyz(J, cand, qx, qy, qz);
-                            key = cov_at(P, qx - x, qy - y, qz - z, J.err);
-                            keep = key > thr;
-                        }
-                        const uint32_t bal = __ballot_sync(FULL_MASK, keep);
-                        const int pos = n + __popc(bal & ((1u << lane) - 1));
-                        if (keep) {
-                            if (pos < cap) {
-                                keys[pos] = key;
-                                idxs[pos] = cand;
-                            } else {
-                                atomicOr(J.err, DERR_CAND_CAPACITY);
+    // warps take CLUSTER_CHUNK consecutive nodes at a time from a counter:
+    // clusterizer-path nodes sit in sparse regions, so a fixed share would
+    // leave some warps most of them
+    while (true) {
+        int chunk = 0;
+        if (lane == 0) chunk = atomicAdd(J.node_next, CLUSTER_CHUNK);
+        chunk = __shfl_sync(FULL_MASK, chunk, 0);
+        if (chunk >= J.size) break;
+        const int chunk_end = (int)min((long long)chunk + CLUSTER_CHUNK, (long long)J.size);
+        for (int node = chunk; node < chunk_end; ++node) {
+            if (!node_needs_kriging(J, node)) continue;
+            int x, y, z;
+            node_xyz(J, node, x, y, z);
+            if (!node_clean(P, x, y, z)) continue;
+            const int cx = (int)(x / P.crx), cy = (int)(y / P.cry), cz = (int)(z / P.crz);
+            int n = 0;
+            for (int k = cz - 1; k <= cz + 1; ++k)
+                for (int j = cy - 1; j <= cy + 1; ++j)
+                    for (int i = cx - 1; i <= cx + 1; ++i) {
+                        if (i < 0 || j < 0 || k < 0 || i > P.mx || j > P.my || k > P.mz) continue;
+                        const long long bi = ((long long)k * P.my + j) * P.mx + i;
+                        const int s0 = P.bucket_start[bi], s1 = P.bucket_start[bi + 1];
+                        for (int base = s0; base < s1; base += 32) {
+                            const int p = base + lane;
+                            bool keep = false;
+                            double key = 0;
+                            int cand = 0;
+                            if (p < s1) {
+                                cand = P.bucket_nodes[p];
+                                int qx, qy, qz;
+                                node_xyz(J, cand, qx, qy, qz);
+                                key = cov_at(P, qx - x, qy - y, qz - z, J.err);
+                                keep = key > thr;
                             }
+                            const uint32_t bal = __ballot_sync(FULL_MASK, keep);
+                            const int pos = n + __popc(bal & ((1u << lane) - 1));
+                            if (keep) {
+                                if (pos < cap) {
+                                    keys[pos] = key;
+                                    idxs[pos] = cand;
+                                } else {
+                                    atomicOr(J.err, DERR_CAND_CAPACITY);
+                                }
+                            }
+                            n += __popc(bal);
                         }
-                        n += __popc(bal);
                     }
-                }
-        if (n > cap) n = cap;
-        __syncwarp();
-        {
-            // only the first max_neighbours positions of the reference's sort are used
-            SortArr a{keys, idxs};
-            if (!warp_reference_sort_prefix(a, n, P.nmax, lane, s_stack[wib], s_lbuf[wib], s_rbuf[wib]) && lane == 0)
-                atomicOr(J.err, DERR_SORT_STACK);
+            if (n > cap) n = cap;
+            __syncwarp();
+            {
+                // only the first max_neighbours positions of the reference's sort are used
+                SortArr a{keys, idxs};
+                if (!warp_reference_sort_prefix(a, n, P.nmax, lane, s_stack[wib], s_lbuf[wib], s_rbuf[wib]) && lane == 0)
+                    atomicOr(J.err, DERR_SORT_STACK);
+            }
+            const int cnt = n < P.nmax ? n : P.nmax;
+            for (int i = lane; i < cnt; i += 32) J.nb[(long long)node * P.nmax + i] = idxs[i];
+            if (lane == 0) J.nbcount[node] = cnt;
+            __syncwarp();
         }
-        const int cnt = n < P.nmax ? n : P.nmax;
-        for (int i = lane; i < cnt; i += 32) J.nb[(long long)node * P.nmax + i] = idxs[i];
-        if (lane == 0) J.nbcount[node] = cnt;
-        __syncwarp();
     }
 }
 

@@ -108,6 +108,7 @@ struct DevJob {
     int *n_attempt_routed;
     int *abandon;            // set: the re-solve runs the plain FP64 pass
     int *seg_next;           // template search: the next 32-node segment to take
+    int *node_next;          // clusterizer search: the next chunk of nodes to take
     // counters
     unsigned long long *n_fp64;
     int *err;
