@@ -129,10 +129,11 @@ struct RefineGate {
 // path alone.  A warp keeps an average of its recent attempts' outcomes
 // (weight 1/4 for the newest); below `keep` it stops attempting and routes its
 // systems straight to the FP64 re-solve, attempting every 8th again to
-// notice when its nodes become well conditioned.  The warp's node sequence
-// is fixed by the launch, so the choice is the same on every run; routed
-// systems get the FP64 path's results, which the mixed results match
-// within their tolerance either way.
+// notice when its nodes become well conditioned.  A kernel that hands out
+// its nodes dynamically restarts the guess with every chunk of consecutive
+// nodes, so the choice depends on the chunk's nodes only and is the same on
+// every run; routed systems get the FP64 path's results, which the mixed
+// results match within their tolerance either way.
 // A kernel passes the success share below which attempting stops paying:
 // an attempt costs about c of an FP64 solve and saves one when it succeeds,
 // so it pays while the share of successes exceeds c.

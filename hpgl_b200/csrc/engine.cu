@@ -584,6 +584,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
             if (g.plan.nmax <= 32) launch_fused32(J, g.dp, S.precision, s, tune.blocks_per_sm);
             else launch_fused64(J, g.dp, S.precision, s, tune.blocks_per_sm);
         } else {
+            CUDA_CHECK(cudaMemsetAsync(J.node_next, 0, sizeof(int), s));  // the mixed kernel's chunk counter
             launch_solve(J, g.dp, S.precision, nullptr, s, tune.blocks_per_sm);
         }
         ++launches;

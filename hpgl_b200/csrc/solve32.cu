@@ -26,6 +26,7 @@ namespace {
 
 constexpr int N32 = 32;
 constexpr int WARPS32 = 4;
+constexpr int MIXED_CHUNK = 32;  // nodes a mixed-kernel warp takes from the counter at a time
 constexpr float MIXED_PIVOT_MIN = 1e-3f;  // on the unit-diagonal scaled system
 constexpr int MIXED_MAX_CORR = 4;
 
@@ -695,19 +696,37 @@ __device__ __forceinline__ void mixed32_warps(const DevJob &J, const DevPlan &P)
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SysSmem &S = reinterpret_cast<SysSmem *>(dyn_smem)[warp];
-    const long long stride = (long long)gridDim.x * WARPS32;
-    long long it = (long long)blockIdx.x * WARPS32 + warp;
+    // Warps take MIXED_CHUNK consecutive nodes at a time from a per-job
+    // counter (the next chunk is taken while the current chunk's last node is
+    // solved), so none waits on a fixed share at the end.  The routing guess
+    // starts afresh with every chunk: its choices depend on the chunk's nodes
+    // only, whichever warp takes it.
+    int chunk = 0;
+    if (lane == 0) chunk = atomicAdd(J.node_next, MIXED_CHUNK);
+    chunk = __shfl_sync(FULL_MASK, chunk, 0);
+    long long it = chunk;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
     RouteGuess guess(ROUTE_KEEP32);
     AttemptTally tally(ABANDON_FRACTION32);
-    for (; it < J.size; it += stride) {
+    while (it < J.size) {
         const NodeFetch cur = next;
-        next = fetch_node(J, P, it + stride < J.size ? (int)(it + stride) : -1, lane);
+        if (it == chunk) guess = RouteGuess(ROUTE_KEEP32);
+        long long nit = it + 1;
+        int nchunk = chunk;
+        if (nit == (long long)chunk + MIXED_CHUNK) {
+            int c = 0;
+            if (lane == 0) c = atomicAdd(J.node_next, MIXED_CHUNK);
+            nchunk = __shfl_sync(FULL_MASK, c, 0);
+            nit = nchunk;
+        }
+        next = fetch_node(J, P, nit < J.size ? (int)nit : -1, lane);
         const bool attempt = guess.attempt();
         const int outcome = mixed32_node<STEPS>(J, P, S, cur, lane, !attempt);
         guess.record(attempt, outcome);
         __syncwarp();
         if (tally.step(J, attempt, outcome, lane)) break;
+        it = nit;
+        chunk = nchunk;
     }
 }
 
