@@ -590,6 +590,7 @@ static void device_pass(JobState &S, cudaStream_t s, PassTiming *pt,
         ++launches;
         if (pt && gi == 0) CUDA_CHECK(cudaEventRecord(pt->top1, s));
         if (S.precision == HPGL_PRECISION_MIXED) {
+            CUDA_CHECK(cudaMemsetAsync(J.node_next, 0, sizeof(int), s));  // an abandoned job's full FP64 pass
             launch_solve(J, g.dp, HPGL_PRECISION_FP64, J.routed, s, tune64.blocks_per_sm);
             ++launches;
         }

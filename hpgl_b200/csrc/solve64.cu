@@ -25,6 +25,15 @@ constexpr int N64 = 64;
 
 constexpr int WARPS64_BLOCK = 1;
 
+// Nodes a 64-row solve warp takes from the per-job counter at a time, and the
+// taking itself (lane 0's atomic, broadcast).
+constexpr int CHUNK64 = 16;
+__device__ __forceinline__ int take_chunk64(const DevJob &J, int lane) {
+    int c = 0;
+    if (lane == 0) c = atomicAdd(J.node_next, CHUNK64);
+    return __shfl_sync(FULL_MASK, c, 0);
+}
+
 // The factor lives in shared memory as a skewed packed upper triangle:
 // column k starts at col_start(k), holds rows 0..k (padded to an even count)
 // and col_start(k) = 2k (mod 16) doubles, so when every lane reads a 16-byte
@@ -511,13 +520,25 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, 
             }
         }
     } else {
+        // warps take CHUNK64 consecutive nodes at a time from a per-job
+        // counter (the next chunk taken while the current one's last node is
+        // solved), so none waits on a fixed share at the end
+        int chunk = take_chunk64(J, lane);
+        it = chunk;
         NodeFetch cur = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
-        for (; it < J.size; it += stride) {
-            const long long nx = it + stride;
+        while (it < J.size) {
+            long long nx = it + 1;
+            int nchunk = chunk;
+            if (nx == (long long)chunk + CHUNK64) {
+                nchunk = take_chunk64(J, lane);
+                nx = nchunk;
+            }
             const NodeFetch next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
             solved += exact64_node(J, P, S, s_cs, cur, lane);
             __syncwarp();
             cur = next;
+            it = nx;
+            chunk = nchunk;
         }
     }
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);
@@ -807,18 +828,31 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Mixed64Smem &S = *reinterpret_cast<Mixed64Smem *>(dyn_smem);
-    long long it = blockIdx.x;
+    // chunks of CHUNK64 nodes from the per-job counter, as the exact kernel;
+    // the routing guess restarts with each chunk, so its choices depend on
+    // the chunk's nodes only
+    int chunk = take_chunk64(J, lane);
+    long long it = chunk;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
     RouteGuess guess(ROUTE_KEEP64);
     AttemptTally tally(ABANDON_FRACTION64);
-    for (; it < J.size; it += gridDim.x) {
+    while (it < J.size) {
         const NodeFetch cur = next;
-        next = fetch_node(J, P, it + gridDim.x < J.size ? (int)(it + gridDim.x) : -1, lane);
+        if (it == chunk) guess = RouteGuess(ROUTE_KEEP64);
+        long long nx = it + 1;
+        int nchunk = chunk;
+        if (nx == (long long)chunk + CHUNK64) {
+            nchunk = take_chunk64(J, lane);
+            nx = nchunk;
+        }
+        next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
         const bool attempt = guess.attempt();
         const int outcome = mixed64_node(J, P, S, s_cs, cur, lane, !attempt);
         guess.record(attempt, outcome);
         __syncwarp();
         if (tally.step(J, attempt, outcome, lane)) break;
+        it = nx;
+        chunk = nchunk;
     }
 }
 
