@@ -156,6 +156,14 @@ struct RouteGuess {
     }
 };
 
+// Nodes a solve warp takes from the per-job counter at a time: up to `cap`,
+// fewer on small jobs so that every warp of the grid still gets about 8
+// chunks (the size depends only on the job and the launch).
+__device__ __forceinline__ int chunk_nodes(const DevJob &J, int cap, int warps_per_block) {
+    const long long c = J.size / ((long long)gridDim.x * warps_per_block * 8);
+    return (int)(c < 1 ? 1 : (c > cap ? cap : c));
+}
+
 // Sends a node's system to the FP64 re-solve (one lane).
 __device__ __forceinline__ void route(const DevJob &J, int node) {
     J.routed[node] = 1;

@@ -26,7 +26,7 @@ namespace {
 
 constexpr int N32 = 32;
 constexpr int WARPS32 = 4;
-constexpr int MIXED_CHUNK = 32;  // nodes a mixed-kernel warp takes from the counter at a time
+constexpr int MIXED_CHUNK = 32;  // at most this many nodes a warp takes from the counter at a time
 constexpr float MIXED_PIVOT_MIN = 1e-3f;  // on the unit-diagonal scaled system
 constexpr int MIXED_MAX_CORR = 4;
 
@@ -451,13 +451,29 @@ __global__ void __launch_bounds__(WARPS32 * 32) k_solve_exact32(DevJob J, DevPla
             }
         }
     } else {
+        // warps take up to MIXED_CHUNK consecutive nodes at a time from the per-job
+        // counter, as the mixed kernel
+        const int csize = chunk_nodes(J, MIXED_CHUNK, WARPS32);
+        int chunk = 0;
+        if (lane == 0) chunk = atomicAdd(J.node_next, csize);
+        chunk = __shfl_sync(FULL_MASK, chunk, 0);
+        it = chunk;
         NodeFetch cur = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
-        for (; it < J.size; it += stride) {
-            const long long nx = it + stride;
+        while (it < J.size) {
+            long long nx = it + 1;
+            int nchunk = chunk;
+            if (nx == (long long)chunk + csize) {
+                int c = 0;
+                if (lane == 0) c = atomicAdd(J.node_next, csize);
+                nchunk = __shfl_sync(FULL_MASK, c, 0);
+                nx = nchunk;
+            }
             const NodeFetch next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
             solved += exact32_node(J, P, S, cur, lane);
             __syncwarp();
             cur = next;
+            it = nx;
+            chunk = nchunk;
         }
     }
     if (lane == 0 && solved) atomicAdd(J.n_fp64, solved);

@@ -25,12 +25,12 @@ constexpr int N64 = 64;
 
 constexpr int WARPS64_BLOCK = 1;
 
-// Nodes a 64-row solve warp takes from the per-job counter at a time, and the
+// At most this many nodes a 64-row solve warp takes from the per-job counter at a time, and the
 // taking itself (lane 0's atomic, broadcast).
 constexpr int CHUNK64 = 16;
-__device__ __forceinline__ int take_chunk64(const DevJob &J, int lane) {
+__device__ __forceinline__ int take_chunk64(const DevJob &J, int lane, int csize) {
     int c = 0;
-    if (lane == 0) c = atomicAdd(J.node_next, CHUNK64);
+    if (lane == 0) c = atomicAdd(J.node_next, csize);
     return __shfl_sync(FULL_MASK, c, 0);
 }
 
@@ -520,17 +520,18 @@ __global__ void __launch_bounds__(WARPS64_BLOCK * 32) k_solve_exact64(DevJob J, 
             }
         }
     } else {
-        // warps take CHUNK64 consecutive nodes at a time from a per-job
+        // warps take up to CHUNK64 consecutive nodes at a time from a per-job
         // counter (the next chunk taken while the current one's last node is
         // solved), so none waits on a fixed share at the end
-        int chunk = take_chunk64(J, lane);
+        const int csize = chunk_nodes(J, CHUNK64, WARPS64_BLOCK);
+        int chunk = take_chunk64(J, lane, csize);
         it = chunk;
         NodeFetch cur = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
         while (it < J.size) {
             long long nx = it + 1;
             int nchunk = chunk;
-            if (nx == (long long)chunk + CHUNK64) {
-                nchunk = take_chunk64(J, lane);
+            if (nx == (long long)chunk + csize) {
+                nchunk = take_chunk64(J, lane, csize);
                 nx = nchunk;
             }
             const NodeFetch next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
@@ -828,10 +829,11 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
     for (int k = threadIdx.x; k < N64; k += blockDim.x) s_cs[k] = col_start_c(k);
     __syncthreads();
     Mixed64Smem &S = *reinterpret_cast<Mixed64Smem *>(dyn_smem);
-    // chunks of CHUNK64 nodes from the per-job counter, as the exact kernel;
+    // chunks of up to CHUNK64 nodes from the per-job counter, as the exact kernel;
     // the routing guess restarts with each chunk, so its choices depend on
     // the chunk's nodes only
-    int chunk = take_chunk64(J, lane);
+    const int csize = chunk_nodes(J, CHUNK64, 1);
+    int chunk = take_chunk64(J, lane, csize);
     long long it = chunk;
     NodeFetch next = fetch_node(J, P, it < J.size ? (int)it : -1, lane);
     RouteGuess guess(ROUTE_KEEP64);
@@ -841,8 +843,8 @@ __global__ void __launch_bounds__(32) k_solve_mixed64(DevJob J, DevPlan P) {
         if (it == chunk) guess = RouteGuess(ROUTE_KEEP64);
         long long nx = it + 1;
         int nchunk = chunk;
-        if (nx == (long long)chunk + CHUNK64) {
-            nchunk = take_chunk64(J, lane);
+        if (nx == (long long)chunk + csize) {
+            nchunk = take_chunk64(J, lane, csize);
             nx = nchunk;
         }
         next = fetch_node(J, P, nx < J.size ? (int)nx : -1, lane);
